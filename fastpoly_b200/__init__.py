@@ -1,0 +1,296 @@
+"""fastpoly_b200 - the fastpoly NTT hot path on one B200.
+
+Python mirror of the reference's polynomial API (``fpx::poly::conv / inv / log /
+exp / sqrt / pow / divmod / div / mod`` and ``NttPlan<M>::forward / inverse``;
+include/fastpoly/poly.hpp, detail/poly/*.hpp, ntt.hpp) over the C ABI in
+``include/fpx_b200.h``, implemented by the in-tree CUDA library
+``fastpoly_b200/libfpx_b200.so``.  There is no CPU fallback: if the library is
+missing or no GPU is present, constructing a ``Context`` raises.
+
+Arrays are canonical residues (numpy ``uint32``) unless ``repr=MONTGOMERY``
+selects the reference's Montgomery limbs.  Errors mirror the reference's
+exceptions: ``DomainError`` (fpx::poly::domain_error), ``NttSizeError``
+(fpx::ntt_size_error), ``LengthError`` (std::length_error).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libfpx_b200.so")
+
+OK, EDOMAIN, ESIZE, ELENGTH, ENOMEM, ETIMEDOUT, ECUDA, EINVAL, EUNSUPPORTED = range(9)
+CANONICAL, MONTGOMERY = 0, 1
+SIZE_MAX = 2**64 - 1
+
+
+class FpxError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"[fpx status {code}] {msg}")
+        self.code = code
+
+
+class DomainError(FpxError):
+    """fpx::poly::domain_error (include/fastpoly/detail/poly/base.hpp:26-30)."""
+
+
+class NttSizeError(FpxError):
+    """fpx::ntt_size_error (include/fastpoly/ntt.hpp:59-70)."""
+
+
+class LengthError(FpxError):
+    """std::length_error from conv (convolution.hpp:20-21)."""
+
+
+_ERRORS = {EDOMAIN: DomainError, ESIZE: NttSizeError, ELENGTH: LengthError}
+
+_u32p = C.POINTER(C.c_uint32)
+_szp = C.POINTER(C.c_size_t)
+_lib = None
+
+
+def load_library(path: str = LIB_PATH):
+    """Loads the CUDA library (fails loudly when it is missing)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise ImportError(f"fastpoly_b200 CUDA library not built: {path} (run python -m fastpoly_b200.build)")
+    L = C.CDLL(path)
+    vp, u32, sz, u64, i32 = C.c_void_p, C.c_uint32, C.c_size_t, C.c_uint64, C.c_int
+    L.fpx_ctx_create.argtypes = [i32, sz, C.POINTER(vp)]
+    L.fpx_ctx_destroy.argtypes = [vp]
+    L.fpx_ctx_set_stream.argtypes = [vp, vp]
+    L.fpx_ctx_stream.argtypes = [vp]
+    L.fpx_ctx_stream.restype = vp
+    L.fpx_ctx_synchronize.argtypes = [vp]
+    L.fpx_last_error_message.argtypes = [vp]
+    L.fpx_last_error_message.restype = C.c_char_p
+    L.fpx_pool_stats.argtypes = [vp, vp]
+    L.fpx_release_pool.argtypes = [vp]
+    L.fpx_ntt_max_log.argtypes = [u32]
+    L.fpx_profile.argtypes = [vp, i32]
+    L.fpx_profile_report.argtypes = [vp, C.c_char_p, sz, _szp]
+    L.fpx_launch_count.argtypes = [vp]
+    L.fpx_launch_count.restype = u64
+    for f in ("fpx_ntt_forward", "fpx_ntt_inverse"):
+        getattr(L, f).argtypes = [vp, u32, _u32p, u32, i32]
+    for f in ("fpx_ntt_forward_device", "fpx_ntt_inverse_device"):
+        getattr(L, f).argtypes = [vp, u32, vp, u32]
+    L.fpx_conv.argtypes = [vp, u32, _u32p, sz, _u32p, sz, sz, _u32p, _szp, i32]
+    L.fpx_conv_device.argtypes = [vp, u32, vp, sz, vp, sz, sz, vp, _szp]
+    for f in ("fpx_inv", "fpx_log", "fpx_exp", "fpx_sqrt"):
+        getattr(L, f).argtypes = [vp, u32, _u32p, sz, sz, _u32p, i32]
+    for f in ("fpx_inv_device", "fpx_log_device", "fpx_exp_device", "fpx_sqrt_device"):
+        getattr(L, f).argtypes = [vp, u32, vp, sz, sz, vp]
+    L.fpx_pow.argtypes = [vp, u32, _u32p, sz, u64, sz, _u32p, i32]
+    L.fpx_pow_device.argtypes = [vp, u32, vp, sz, u64, sz, vp]
+    L.fpx_divmod.argtypes = [vp, u32, _u32p, sz, _u32p, sz, _u32p, _szp, _u32p, _szp, i32]
+    L.fpx_div.argtypes = [vp, u32, _u32p, sz, _u32p, sz, _u32p, _szp, i32]
+    L.fpx_mod.argtypes = [vp, u32, _u32p, sz, _u32p, sz, _u32p, _szp, i32]
+    _lib = L
+    return L
+
+
+class PoolStats(C.Structure):
+    _fields_ = [("cached_bytes", C.c_size_t), ("cached_blocks", C.c_size_t), ("in_use_bytes", C.c_size_t),
+                ("system_allocations", C.c_size_t), ("cache_hits", C.c_size_t), ("limit_bytes", C.c_size_t)]
+
+
+def _arr(a) -> np.ndarray:
+    return np.ascontiguousarray(np.asarray(a, dtype=np.uint32))
+
+
+def _ptr(a: np.ndarray):
+    return a.ctypes.data_as(_u32p) if a.size else None
+
+
+def _dptr(t) -> int:
+    """Device pointer of a torch tensor (or an int address)."""
+    return t if isinstance(t, int) else t.data_ptr()
+
+
+class Context:
+    """One device, one stream, one device-memory pool and plan cache (fpx_ctx)."""
+
+    def __init__(self, device: int = 0, pool_limit_bytes: int = 0):
+        self._L = load_library()
+        h = C.c_void_p()
+        rc = self._L.fpx_ctx_create(device, pool_limit_bytes, C.byref(h))
+        if rc != OK:
+            raise FpxError(rc, f"fpx_ctx_create(device={device}) failed")
+        self._h = h
+        self.device = device
+
+    # -- plumbing --------------------------------------------------------------
+    def close(self):
+        if getattr(self, "_h", None):
+            self._L.fpx_ctx_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc: int, what: str):
+        if rc != OK:
+            msg = (self._L.fpx_last_error_message(self._h) or b"").decode()
+            raise _ERRORS.get(rc, FpxError)(rc, f"{what}: {msg}")
+
+    @property
+    def handle(self):
+        return self._h
+
+    def set_stream(self, stream=None):
+        """Queue device-pointer work on a cudaStream_t (int handle or torch stream)."""
+        s = getattr(stream, "cuda_stream", stream)
+        self._check(self._L.fpx_ctx_set_stream(self._h, s), "set_stream")
+
+    @property
+    def stream(self) -> int:
+        return self._L.fpx_ctx_stream(self._h) or 0
+
+    def synchronize(self):
+        self._check(self._L.fpx_ctx_synchronize(self._h), "synchronize")
+
+    def pool_stats(self) -> dict:
+        st = PoolStats()
+        self._check(self._L.fpx_pool_stats(self._h, C.byref(st)), "pool_stats")
+        return {k: getattr(st, k) for k, _ in PoolStats._fields_}
+
+    def profile(self, enable: bool = True):
+        """Start (and clear) or stop per-kernel CUDA-event timing on the context's stream."""
+        self._check(self._L.fpx_profile(self._h, 1 if enable else 0), "profile")
+
+    def profile_report(self) -> dict:
+        """{kernel: (launches, total_ms)} for the launches recorded since profile(True)."""
+        import json
+        need = C.c_size_t(0)
+        self._check(self._L.fpx_profile_report(self._h, None, 0, C.byref(need)), "profile_report")
+        buf = C.create_string_buffer(need.value + 16)
+        self._check(self._L.fpx_profile_report(self._h, buf, len(buf), C.byref(need)), "profile_report")
+        return {k: (int(v[0]), float(v[1])) for k, v in json.loads(buf.value.decode()).items()}
+
+    def launch_count(self) -> int:
+        return int(self._L.fpx_launch_count(self._h))
+
+    def release_pool(self):
+        self._check(self._L.fpx_release_pool(self._h), "release_pool")
+
+    # -- transforms (NttPlan<M>::forward / inverse) ------------------------------
+    def ntt_forward(self, p: int, x, repr: int = CANONICAL) -> np.ndarray:
+        x = _arr(x).copy()
+        self._check(self._L.fpx_ntt_forward(self._h, p, _ptr(x), x.size, repr), "ntt_forward")
+        return x
+
+    def ntt_inverse(self, p: int, x, repr: int = CANONICAL) -> np.ndarray:
+        x = _arr(x).copy()
+        self._check(self._L.fpx_ntt_inverse(self._h, p, _ptr(x), x.size, repr), "ntt_inverse")
+        return x
+
+    def ntt_forward_device(self, p: int, d_x, n: int):
+        self._check(self._L.fpx_ntt_forward_device(self._h, p, _dptr(d_x), n), "ntt_forward_device")
+
+    def ntt_inverse_device(self, p: int, d_x, n: int):
+        self._check(self._L.fpx_ntt_inverse_device(self._h, p, _dptr(d_x), n), "ntt_inverse_device")
+
+    # -- fpx::poly ---------------------------------------------------------------
+    def conv(self, p: int, a, b, n: int | None = None, repr: int = CANONICAL, out: np.ndarray | None = None):
+        """fpx::poly::conv(a, b[, n]); `out` may be a preallocated (e.g. pinned) uint32 array."""
+        a, b = _arr(a), _arr(b)
+        lim = SIZE_MAX if n is None else n
+        cap = min(a.size + b.size - 1, lim) if a.size and b.size and lim else 0
+        if out is None:
+            out = np.empty(max(cap, 1), dtype=np.uint32)
+        elif out.dtype != np.uint32 or not out.flags.c_contiguous or out.size < cap:
+            raise ValueError("out must be a contiguous uint32 array with room for the product")
+        got = C.c_size_t(0)
+        pb = _ptr(a) if b is a else _ptr(b)
+        self._check(self._L.fpx_conv(self._h, p, _ptr(a), a.size, pb, b.size, C.c_size_t(lim), _ptr(out),
+                                     C.byref(got), repr), "conv")
+        return out[: got.value]
+
+    def conv_device(self, p: int, d_a, la: int, d_b, lb: int, n: int | None, d_out) -> int:
+        got = C.c_size_t(0)
+        lim = SIZE_MAX if n is None else n
+        self._check(self._L.fpx_conv_device(self._h, p, _dptr(d_a), la, _dptr(d_b), lb, C.c_size_t(lim),
+                                            _dptr(d_out), C.byref(got)), "conv_device")
+        return got.value
+
+    def _series(self, fn, what, p, a, n, repr):
+        a = _arr(a)
+        out = np.empty(max(n, 1), dtype=np.uint32)
+        self._check(fn(self._h, p, _ptr(a), a.size, n, _ptr(out), repr), what)
+        return out[:n]
+
+    def inv(self, p, a, n, repr=CANONICAL):
+        return self._series(self._L.fpx_inv, "inv", p, a, n, repr)
+
+    def log(self, p, a, n, repr=CANONICAL):
+        return self._series(self._L.fpx_log, "log", p, a, n, repr)
+
+    def exp(self, p, a, n, repr=CANONICAL):
+        return self._series(self._L.fpx_exp, "exp", p, a, n, repr)
+
+    def sqrt(self, p, a, n, repr=CANONICAL):
+        return self._series(self._L.fpx_sqrt, "sqrt", p, a, n, repr)
+
+    def pow(self, p, a, k, n, repr=CANONICAL):
+        a = _arr(a)
+        out = np.empty(max(n, 1), dtype=np.uint32)
+        self._check(self._L.fpx_pow(self._h, p, _ptr(a), a.size, C.c_uint64(k), n, _ptr(out), repr), "pow")
+        return out[:n]
+
+    def _series_dev(self, fn, what, p, d_a, la, n, d_out):
+        self._check(fn(self._h, p, _dptr(d_a), la, n, _dptr(d_out)), what)
+
+    def inv_device(self, p, d_a, la, n, d_out):
+        self._series_dev(self._L.fpx_inv_device, "inv_device", p, d_a, la, n, d_out)
+
+    def log_device(self, p, d_a, la, n, d_out):
+        self._series_dev(self._L.fpx_log_device, "log_device", p, d_a, la, n, d_out)
+
+    def exp_device(self, p, d_a, la, n, d_out):
+        self._series_dev(self._L.fpx_exp_device, "exp_device", p, d_a, la, n, d_out)
+
+    def sqrt_device(self, p, d_a, la, n, d_out):
+        self._series_dev(self._L.fpx_sqrt_device, "sqrt_device", p, d_a, la, n, d_out)
+
+    def pow_device(self, p, d_a, la, k, n, d_out):
+        self._check(self._L.fpx_pow_device(self._h, p, _dptr(d_a), la, C.c_uint64(k), n, _dptr(d_out)), "pow_device")
+
+    def divmod(self, p, a, b, repr=CANONICAL):
+        a, b = _arr(a), _arr(b)
+        q = np.empty(max(a.size, 1), dtype=np.uint32)
+        r = np.empty(max(b.size, 1), dtype=np.uint32)
+        lq, lr = C.c_size_t(0), C.c_size_t(0)
+        self._check(self._L.fpx_divmod(self._h, p, _ptr(a), a.size, _ptr(b), b.size, _ptr(q), C.byref(lq), _ptr(r),
+                                       C.byref(lr), repr), "divmod")
+        return q[: lq.value], r[: lr.value]
+
+    def div(self, p, a, b, repr=CANONICAL):
+        a, b = _arr(a), _arr(b)
+        q = np.empty(max(a.size, 1), dtype=np.uint32)
+        lq = C.c_size_t(0)
+        self._check(self._L.fpx_div(self._h, p, _ptr(a), a.size, _ptr(b), b.size, _ptr(q), C.byref(lq), repr), "div")
+        return q[: lq.value]
+
+    def mod(self, p, a, b, repr=CANONICAL):
+        a, b = _arr(a), _arr(b)
+        r = np.empty(max(b.size, 1), dtype=np.uint32)
+        lr = C.c_size_t(0)
+        self._check(self._L.fpx_mod(self._h, p, _ptr(a), a.size, _ptr(b), b.size, _ptr(r), C.byref(lr), repr), "mod")
+        return r[: lr.value]
+
+
+def ntt_max_log(p: int) -> int:
+    return load_library().fpx_ntt_max_log(p)
+
+
+__all__ = ["Context", "DomainError", "NttSizeError", "LengthError", "FpxError", "CANONICAL", "MONTGOMERY",
+           "load_library", "ntt_max_log", "LIB_PATH"]

@@ -1,0 +1,75 @@
+"""Builds the in-tree CUDA library fastpoly_b200/libfpx_b200.so for sm_100a.
+
+    python -m fastpoly_b200.build [--force]
+
+nvcc compiles the kernels (-gencode arch=compute_100a,code=sm_100a -lineinfo),
+g++ the C++20 host engine and the C ABI, linked against the static CUDA
+runtime so the library carries no runtime-path dependency.
+"""
+from __future__ import annotations
+
+import os
+import shutil
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+CSRC = os.path.join(HERE, "csrc")
+BUILD = os.path.join(HERE, "_build")
+LIB = os.path.join(HERE, "libfpx_b200.so")
+INCLUDE = os.path.join(ROOT, "include")
+
+CUDA_HOME = os.environ.get("CUDA_HOME", "/usr/local/cuda")
+NVCC = os.path.join(CUDA_HOME, "bin", "nvcc")
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+
+CU_SOURCES = ["kernels.cu"]
+CPP_SOURCES = ["engine.cpp", "api.cpp"]
+HEADERS = ["field.cuh", "ntt_core.cuh", "kernels.h", "engine.h"]
+
+
+def _sources():
+    out = [os.path.join(CSRC, s) for s in CU_SOURCES + CPP_SOURCES + HEADERS]
+    out.append(os.path.join(INCLUDE, "fpx_b200.h"))
+    return out
+
+
+def _stale() -> bool:
+    if not os.path.exists(LIB):
+        return True
+    t = os.path.getmtime(LIB)
+    return any(os.path.getmtime(s) > t for s in _sources() if os.path.exists(s))
+
+
+def _run(cmd, verbose):
+    if verbose:
+        print(" ".join(cmd), flush=True)
+    subprocess.run(cmd, check=True)
+
+
+def build(force: bool = False, verbose: bool = False) -> str:
+    if not force and not _stale():
+        return LIB
+    os.makedirs(BUILD, exist_ok=True)
+    objs = []
+    for s in CU_SOURCES:
+        o = os.path.join(BUILD, s + ".o")
+        _run([NVCC, "-std=c++17", "-O3", *ARCH, "-lineinfo", "-Xcompiler", "-fPIC", "-I" + CSRC, "-I" + INCLUDE,
+              "-c", os.path.join(CSRC, s), "-o", o], verbose)
+        objs.append(o)
+    cxx = os.environ.get("CXX", shutil.which("g++") or "g++")
+    for s in CPP_SOURCES:
+        o = os.path.join(BUILD, s + ".o")
+        _run([cxx, "-std=c++20", "-O2", "-fPIC", "-Wall", "-I" + CSRC, "-I" + INCLUDE,
+              "-I" + os.path.join(CUDA_HOME, "include"), "-c", os.path.join(CSRC, s), "-o", o], verbose)
+        objs.append(o)
+    tmp = LIB + ".tmp"
+    _run([cxx, "-shared", "-o", tmp, *objs, "-L" + os.path.join(CUDA_HOME, "lib64"), "-lcudart_static", "-ldl",
+          "-lrt", "-pthread"], verbose)
+    os.replace(tmp, LIB)
+    return LIB
+
+
+if __name__ == "__main__":
+    build(force="--force" in sys.argv, verbose=True)

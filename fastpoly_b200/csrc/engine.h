@@ -1,0 +1,182 @@
+// engine.h - host orchestration of the fastpoly hot path on one GPU.
+//
+// The Engine owns a device, a stream, a caching device-memory pool and the plan
+// cache; every polynomial operation is a sequence of kernel launches on that
+// stream composed here, following the reference's algorithms
+// (include/fastpoly/detail/poly/*.hpp) with its transforms replaced by the
+// fused GPU passes of kernels.cu.
+#pragma once
+#include <cstdint>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "kernels.h"
+
+namespace fpx {
+
+struct Error {
+  int code;
+  std::string msg;
+};
+
+// Caching device allocator (the reference's ScratchPool, memory.hpp:117-187,
+// as a device pool): power-of-two classes, blocks recycled in stream order.
+class Pool {
+ public:
+  explicit Pool(size_t limit) : limit_(limit) {}
+  ~Pool();
+  uint32_t* get(size_t words, size_t* cls_out);
+  void put(uint32_t* p, size_t cls);
+  void release();
+  size_t cached_bytes = 0, cached_blocks = 0, in_use_bytes = 0, system_allocations = 0, cache_hits = 0;
+  size_t limit_ = 0;
+
+ private:
+  std::map<size_t, std::vector<void*>> free_;
+  std::mutex mu_;
+};
+
+class Engine;
+
+// RAII scratch buffer from the pool.
+class Buf {
+ public:
+  Buf() = default;
+  Buf(Pool* pool, size_t words) : pool_(pool) { ptr_ = pool->get(words ? words : 1, &cls_); }
+  Buf(const Buf&) = delete;
+  Buf& operator=(const Buf&) = delete;
+  Buf(Buf&& o) noexcept { *this = std::move(o); }
+  Buf& operator=(Buf&& o) noexcept {
+    reset();
+    pool_ = o.pool_; ptr_ = o.ptr_; cls_ = o.cls_;
+    o.ptr_ = nullptr;
+    return *this;
+  }
+  ~Buf() { reset(); }
+  void reset() {
+    if (ptr_) pool_->put(ptr_, cls_);
+    ptr_ = nullptr;
+  }
+  uint32_t* get() const { return ptr_; }
+  operator uint32_t*() const { return ptr_; }
+
+ private:
+  Pool* pool_ = nullptr;
+  uint32_t* ptr_ = nullptr;
+  size_t cls_ = 0;
+};
+
+struct PrimePlan {
+  PrimeTables t;
+  Buf fwd, inv;
+};
+struct BigPlan {
+  BigTables t;
+  Buf lo_fwd, hi_fwd, lo_inv, lo_inv_r, hi_inv;
+};
+
+// Host-side number theory.
+uint32_t powm(uint32_t a, uint64_t e, uint32_t p);
+uint32_t invm(uint32_t a, uint32_t p);
+int v2_of(uint32_t p);  // v2(p - 1)
+uint32_t primitive_root(uint32_t p);
+bool is_prime(uint32_t p);
+bool sqrt_mod(uint32_t x, uint32_t p, uint32_t* out);  // the reference's Tonelli-Shanks root choice
+size_t crt_prime_count(uint32_t p, size_t terms);
+
+class Engine {
+ public:
+  explicit Engine(int device, size_t pool_limit);
+  ~Engine();
+
+  int device() const { return device_; }
+  cudaStream_t stream() const { return stream_; }
+  void set_stream(cudaStream_t s);
+  Pool& pool() { return pool_; }
+
+  // Device-pointer operations (canonical residues).  Throw Error.
+  size_t conv(uint32_t p, const uint32_t* a, size_t la, const uint32_t* b, size_t lb, size_t n, uint32_t* out);
+  void inv(uint32_t p, const uint32_t* a, size_t la, size_t n, uint32_t* out);
+  void log(uint32_t p, const uint32_t* a, size_t la, size_t n, uint32_t* out);
+  void exp(uint32_t p, const uint32_t* a, size_t la, size_t n, uint32_t* out);
+  void sqrt(uint32_t p, const uint32_t* a, size_t la, size_t n, uint32_t* out);
+  void pow(uint32_t p, const uint32_t* a, size_t la, uint64_t k, size_t n, uint32_t* out);
+  void divmod(uint32_t p, const uint32_t* a, size_t la, const uint32_t* b, size_t lb, uint32_t* q, size_t* lq,
+              uint32_t* r, size_t* lr, bool want_q, bool want_r);
+  void ntt(uint32_t p, uint32_t* data, uint32_t n, bool inverse);
+
+  void check(cudaError_t e, const char* what);
+  void sync();
+
+  // Per-kernel timing (CUDA events on the launching stream) and launch count.
+  void profile(bool on);
+  std::string profile_report();  // {"kernel": [launches, total_ms], ...}
+  uint64_t launches() const { return launches_; }
+
+ private:
+  // ---- plans
+  const PrimePlan& prime_plan(uint32_t p);
+  const BigPlan& big_plan(uint32_t p, int logN);
+  const uint32_t* inv_table(uint32_t p, size_t n);  // Montgomery form 1/i, i <= n
+
+  bool native(uint32_t p, int logN) const;  // GPU NTT usable for (p, 2^logN)
+
+  // ---- transform compositions
+  struct CycOp {
+    InOp x;
+    int ymode = 0;              // 0 none, 1 raw y, 2 y spectrum, 3 square x
+    InOp y;
+    const uint32_t* yspec = nullptr;
+    uint32_t* yspec_out = nullptr;
+    Epi epi;                    // window of the inverse; epi.scale = extra factor (0: none)
+  };
+  // Cyclic product at size 2^logN on a native prime, inverse window through epi.
+  void cyc_product(uint32_t p, int logN, const CycOp& op);
+  // Exact product (direct / native / CRT), truncated to outn; optional
+  // post-multiplication by a Montgomery table (out[i] *= tab[i]).
+  void product(uint32_t p, const uint32_t* a, size_t la, const uint32_t* b, size_t lb, size_t outn, uint32_t* out,
+               const uint32_t* post_mont = nullptr, bool accumulate = false);
+  void crt_product(uint32_t p, const uint32_t* a, size_t la, const uint32_t* b, size_t lb, size_t outn,
+                   uint32_t* out, bool accumulate);
+  // Exact coefficients [off, off+cnt) of a*b.
+  void mul_window(uint32_t p, const uint32_t* a, size_t la, const uint32_t* b, size_t lb, size_t off, size_t cnt,
+                  uint32_t* out);
+  // c[0,k) -> c[0,wanted) for the inverse of a (inverse.hpp:18-65).
+  void extend_inverse(uint32_t p, const uint32_t* a, size_t la, uint32_t* c, size_t k, size_t wanted);
+  void inv_into(uint32_t p, const uint32_t* a, size_t la, size_t n, uint32_t* out);
+  void exp_into(uint32_t p, const uint32_t* a, size_t la, size_t n, uint32_t* out);
+  void log_into(uint32_t p, const uint32_t* a, size_t la, size_t n, uint32_t* out);
+
+  // small device->host reads
+  uint32_t read_word(const uint32_t* d);
+  size_t find_nonzero(const uint32_t* a, size_t n, bool last);  // n if none
+
+  void prof_begin();
+  void prof_end(const char* what);
+  struct ProfRec {
+    std::string name;
+    cudaEvent_t b, e;
+  };
+  bool prof_on_ = false;
+  cudaEvent_t prof_open_ = nullptr;
+  std::vector<ProfRec> prof_recs_;
+  std::vector<cudaEvent_t> ev_free_;
+  uint64_t launches_ = 0;
+
+  int device_;
+  cudaStream_t stream_ = nullptr, own_stream_ = nullptr;
+  Pool pool_;
+  std::mutex plan_mu_;
+  std::map<uint32_t, std::unique_ptr<PrimePlan>> primes_;
+  std::map<std::pair<uint32_t, int>, std::unique_ptr<BigPlan>> bigs_;
+  std::map<uint32_t, std::pair<size_t, Buf>> inv_tabs_;
+  unsigned long long* scratch_ull_ = nullptr;  // device word for scans
+  unsigned long long* host_ull_ = nullptr;     // pinned
+};
+
+}  // namespace fpx

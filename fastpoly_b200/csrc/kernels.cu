@@ -1,0 +1,671 @@
+// kernels.cu - sm_100a kernels for the NTT path and their host launchers.
+//
+// Transform decomposition (the reference's NttPlan, ntt.hpp:86-994, re-designed
+// for one GPU):
+//   * N <= 2^13: one CTA per transform, the whole DIF/DIT in shared memory
+//     (k_small); pointwise product, scaling and the output window are fused.
+//   * N  > 2^13: N = R x C, C = 2^12 (2^13 for N >= 2^24), R <= 2^12.
+//       pass A (k_colfwd):  R-point DIF down each of the C columns (stride C),
+//                           then the Bailey twiddle w_N^(j * bitrev_R(t));
+//       pass B (k_rows):    C-point DIF along each contiguous row; optionally the
+//                           second operand's rows, the pointwise product and the
+//                           C-point DIT of the product, all while the row is in
+//                           shared memory;
+//       pass A' (k_colinv): inverse Bailey twiddle (1/N folded in), R-point DIT
+//                           down the columns, and the caller's output window.
+//     The spectrum of this factorisation sits at position t*C+u as
+//     X[bitrev_R(t) + R*bitrev_C(u)] = X[bitrev_N(t*C+u)]: exactly the
+//     reference's bit-reversed DIF order.
+#include <cuda_runtime.h>
+
+#include "field.cuh"
+#include "kernels.h"
+#include "ntt_core.cuh"
+
+using namespace fpx_dev;
+
+namespace {
+
+struct Ptab {
+  const uint2* fwd;
+  const uint2* inv;
+  Fp f;
+  uint32_t q1;
+};
+
+Ptab dev_tab(const fpx::PrimeTables& pt) {
+  return Ptab{reinterpret_cast<const uint2*>(pt.fwd), reinterpret_cast<const uint2*>(pt.inv), make_fp(pt.p), pt.q1};
+}
+
+struct InD {
+  const uint32_t* ptr;
+  uint32_t count;
+  int reduce;
+};
+struct EpiD {
+  uint32_t* out;
+  uint32_t lo, hi;
+  uint2 scale;
+  const uint32_t* mul_mont;
+  int negate;
+  const uint32_t* sub_from;
+  uint32_t sub_len;
+  int accumulate;
+};
+
+InD dev_in(const fpx::InOp& x) { return InD{x.ptr, x.count, x.reduce}; }
+EpiD dev_epi(const fpx::Epi& e) {
+  return EpiD{e.out, e.lo, e.hi, make_uint2(e.scale.w, e.scale.q), e.mul_mont, e.negate, e.sub_from, e.sub_len,
+              e.accumulate};
+}
+
+__device__ __forceinline__ uint32_t load_in(const InD& in, uint32_t i, const Fp& f, uint32_t q1) {
+  if (i >= in.count) return 0u;
+  uint32_t v = __ldg(in.ptr + i);
+  return in.reduce ? reduce_any(v, q1, f) : v;
+}
+
+// Writes natural-order output x (lazy, < 4p) at global index gi through the epilogue.
+__device__ __forceinline__ void epi_store(const EpiD& e, uint32_t gi, uint32_t x, const Fp& f) {
+  if (gi < e.lo || gi >= e.hi) return;
+  const uint32_t j = gi - e.lo;
+  uint32_t v = e.scale.x ? shoup(x, e.scale, f.p) : red(x, f.p2);
+  if (e.mul_mont) v = mont(v, __ldg(e.mul_mont + j), f);
+  v = red(v, f.p);
+  if (e.negate) v = v ? f.p - v : 0u;
+  if (e.sub_from) {
+    const uint32_t s = j < e.sub_len ? __ldg(e.sub_from + j) : 0u;
+    v = s >= v ? s - v : s + f.p - v;
+  }
+  if (e.accumulate) v = red(v + e.out[j], f.p);
+  e.out[j] = v;
+}
+
+__device__ __forceinline__ int brev_n(int t, int logn) { return logn ? (int)(__brev((unsigned)t) >> (32 - logn)) : 0; }
+
+// ---------------------------------------------------------------------------
+// Single-CTA transforms (N <= 2^13).
+// ---------------------------------------------------------------------------
+struct SmallD {
+  InD x, y;
+  int forward, ymode, inverse;
+  const uint32_t* yspec;
+  uint32_t* yspec_out;
+  uint32_t* spec_x;
+  EpiD epi;
+};
+
+__global__ void __launch_bounds__(512) k_small(SmallD job, Ptab pt, int logN) {
+  extern __shared__ uint32_t sm[];
+  const int N = 1 << logN, tid = threadIdx.x, nt = blockDim.x;
+  uint32_t* X = sm;
+  uint32_t* Y = sm + padded_words(N);
+  const Fp f = pt.f;
+  for (int i = tid; i < N; i += nt) X[pad(i)] = job.forward ? load_in(job.x, i, f, pt.q1) : __ldg(job.x.ptr + i);
+  if (job.ymode == 1)
+    for (int i = tid; i < N; i += nt) Y[pad(i)] = load_in(job.y, i, f, pt.q1);
+  else if (job.ymode == 2)
+    for (int i = tid; i < N; i += nt) Y[pad(i)] = __ldg(job.yspec + i);
+  __syncthreads();
+  if (job.forward) {
+    tile_dif(X, logN, 0, pt.fwd, f, tid, nt);
+    __syncthreads();
+  }
+  if (job.ymode == 1) {
+    tile_dif(Y, logN, 0, pt.fwd, f, tid, nt);
+    __syncthreads();
+    if (job.yspec_out)
+      for (int i = tid; i < N; i += nt) job.yspec_out[i] = Y[pad(i)];
+  }
+  if (job.ymode == 1 || job.ymode == 2) {
+    for (int i = tid; i < N; i += nt) X[pad(i)] = mont(X[pad(i)], Y[pad(i)], f);
+  } else if (job.ymode == 3) {
+    for (int i = tid; i < N; i += nt) { const uint32_t v = X[pad(i)]; X[pad(i)] = mont(v, v, f); }
+  }
+  if (!job.inverse) {
+    for (int i = tid; i < N; i += nt) job.spec_x[i] = X[pad(i)];
+    return;
+  }
+  __syncthreads();
+  tile_dit(X, logN, 0, pt.inv, f, tid, nt);
+  __syncthreads();
+  const uint32_t hi = job.epi.hi < (uint32_t)N ? job.epi.hi : (uint32_t)N;
+  for (uint32_t i = job.epi.lo + tid; i < hi; i += nt) epi_store(job.epi, i, X[pad(i)], f);
+}
+
+// ---------------------------------------------------------------------------
+// Pass A forward (columns).
+// ---------------------------------------------------------------------------
+struct ColOps {
+  InD in[3];
+  uint32_t* out[3];
+};
+struct BigD {
+  int logR, logC, logW;
+  const uint2* lo;
+  const uint2* hi;
+};
+
+__global__ void __launch_bounds__(256) k_colfwd(ColOps ops, BigD bt, Ptab pt) {
+  extern __shared__ uint32_t sm[];
+  const int tid = threadIdx.x, nt = blockDim.x;
+  const int logW = bt.logW, W = 1 << logW, logC = bt.logC;
+  const int TE = W << bt.logR;
+  const int j0 = blockIdx.x << logW;
+  const InD in = ops.in[blockIdx.y];
+  uint32_t* out = ops.out[blockIdx.y];
+  const Fp f = pt.f;
+  for (int e = tid; e < TE; e += nt) {
+    const int t = e >> logW, c = e & (W - 1);
+    sm[pad(e)] = load_in(in, (uint32_t)((t << logC) + j0 + c), f, pt.q1);
+  }
+  __syncthreads();
+  tile_dif(sm, bt.logR, logW, pt.fwd, f, tid, nt);
+  __syncthreads();
+  for (int e = tid; e < TE; e += nt) {
+    const int t = e >> logW, c = e & (W - 1);
+    const int j = j0 + c;
+    const uint32_t ex = (uint32_t)j * (uint32_t)brev_n(t, bt.logR);
+    uint32_t v = shoup(sm[pad(e)], __ldg(bt.lo + (ex & 4095u)), f.p);
+    v = shoup(v, __ldg(bt.hi + (ex >> 12)), f.p);
+    out[(t << logC) + j] = v;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Pass B (rows), optionally fused with the second operand, the pointwise
+// product and the row inverse.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(512) k_rows(uint32_t* x, const uint32_t* y, int ymode, uint32_t* y_spec_out,
+                                               int forward, int inverse, int logC, Ptab pt) {
+  extern __shared__ uint32_t sm[];
+  const int tid = threadIdx.x, nt = blockDim.x, C = 1 << logC;
+  uint32_t* X = sm;
+  uint32_t* Y = sm + padded_words(C);
+  const size_t row = (size_t)blockIdx.x << logC;
+  const Fp f = pt.f;
+  for (int i = tid; i < C; i += nt) X[pad(i)] = x[row + i];
+  if (ymode == 1 || ymode == 2)
+    for (int i = tid; i < C; i += nt) Y[pad(i)] = __ldg(y + row + i);
+  __syncthreads();
+  if (forward) {
+    tile_dif(X, logC, 0, pt.fwd, f, tid, nt);
+    __syncthreads();
+  }
+  if (ymode == 1) {
+    tile_dif(Y, logC, 0, pt.fwd, f, tid, nt);
+    __syncthreads();
+    if (y_spec_out)
+      for (int i = tid; i < C; i += nt) y_spec_out[row + i] = Y[pad(i)];
+  }
+  if (ymode == 1 || ymode == 2) {
+    for (int i = tid; i < C; i += nt) X[pad(i)] = mont(X[pad(i)], Y[pad(i)], f);
+  } else if (ymode == 3) {
+    for (int i = tid; i < C; i += nt) { const uint32_t v = X[pad(i)]; X[pad(i)] = mont(v, v, f); }
+  }
+  if (inverse) {
+    __syncthreads();
+    tile_dit(X, logC, 0, pt.inv, f, tid, nt);
+  }
+  __syncthreads();
+  for (int i = tid; i < C; i += nt) x[row + i] = X[pad(i)];
+}
+
+// ---------------------------------------------------------------------------
+// Pass A inverse (columns) with the output epilogue.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_colinv(const uint32_t* in, BigD bt, Ptab pt, EpiD epi) {
+  extern __shared__ uint32_t sm[];
+  const int tid = threadIdx.x, nt = blockDim.x;
+  const int logW = bt.logW, W = 1 << logW, logC = bt.logC;
+  const int TE = W << bt.logR;
+  const int j0 = blockIdx.x << logW;
+  const Fp f = pt.f;
+  for (int e = tid; e < TE; e += nt) {
+    const int t = e >> logW, c = e & (W - 1);
+    const int j = j0 + c;
+    const uint32_t ex = (uint32_t)j * (uint32_t)brev_n(t, bt.logR);
+    uint32_t v = shoup(__ldg(in + (t << logC) + j), __ldg(bt.lo + (ex & 4095u)), f.p);
+    sm[pad(e)] = shoup(v, __ldg(bt.hi + (ex >> 12)), f.p);
+  }
+  __syncthreads();
+  tile_dit(sm, bt.logR, logW, pt.inv, f, tid, nt);
+  __syncthreads();
+  for (int e = tid; e < TE; e += nt) {
+    const int t = e >> logW, c = e & (W - 1);
+    epi_store(epi, (uint32_t)((t << logC) + j0 + c), sm[pad(e)], f);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Elementwise kernels.
+// ---------------------------------------------------------------------------
+__global__ void k_pointwise(Fp f, uint32_t* a, const uint32_t* b, size_t n) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    a[i] = mont(a[i], b[i], f);
+}
+
+struct GarnerC {
+  uint32_t P1, P2, P3;
+  uint2 inv12;      // P1^-1 mod P2 (Shoup)
+  uint2 p1_in3;     // P1 mod P3
+  uint2 inv123;     // (P1 P2)^-1 mod P3
+  uint32_t t;       // target modulus
+  uint32_t t_q1;    // floor(2^32 / t)
+  uint2 p1_t;       // P1 mod t
+  uint2 p12_t;      // P1 P2 mod t
+};
+
+__device__ __forceinline__ uint32_t redc_any(uint32_t x, uint32_t m) { return min(x, x - m); }
+
+__global__ void k_garner(GarnerC g, int primes, const uint32_t* c1, const uint32_t* c2, const uint32_t* c3,
+                         uint32_t* out, size_t n, int accumulate) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    const uint32_t x1 = c1[i];
+    uint32_t v = x1 - __umulhi(x1, g.t_q1) * g.t;
+    v = redc_any(v, g.t);
+    if (primes >= 2) {
+      uint32_t x2 = redc_any(shoup(c2[i] + g.P2 - x1, g.inv12, g.P2), g.P2);
+      uint32_t v2 = redc_any(shoup(x2, g.p1_t, g.t), g.t);
+      v = redc_any(v + v2, g.t);
+      if (primes == 3) {
+        const uint32_t y = redc_any(shoup(x2, g.p1_in3, g.P3), g.P3);
+        const uint32_t x12 = redc_any(x1 + y, g.P3);  // x1 + P1*x2 mod P3
+        const uint32_t x3 = redc_any(shoup(c3[i] + g.P3 - x12, g.inv123, g.P3), g.P3);
+        const uint32_t v3 = redc_any(shoup(x3, g.p12_t, g.t), g.t);
+        v = redc_any(v + v3, g.t);
+      }
+    }
+    if (accumulate) v = redc_any(v + out[i], g.t);
+    out[i] = v;
+  }
+}
+
+__global__ void k_from_mont(Fp f, const uint32_t* in, uint32_t* out, size_t n) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    out[i] = red(mont(in[i], 1u, f), f.p);
+}
+__global__ void k_bits2(const uint32_t* in, uint32_t* out, size_t n) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    out[i] = in[i] & 1u;
+}
+__global__ void k_scale(uint32_t p, const uint32_t* in, uint32_t* out, size_t n, uint2 c) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    out[i] = redc_any(shoup(in[i], c, p), p);
+}
+
+__device__ uint32_t mont_pow(uint32_t base_m, uint32_t e, uint32_t one_m, const Fp& f) {
+  uint32_t r = one_m, b = base_m;
+  while (e) {
+    if (e & 1) r = red(mont(r, b, f), f.p);
+    b = red(mont(b, b, f), f.p);
+    e >>= 1;
+  }
+  return r;
+}
+
+// tab[i] = (1/i) * 2^32 mod p for 1 <= i <= n (i < p), tab[0] = 0.
+__global__ void k_inv_table(Fp f, uint2 r_sh, uint2 r2_sh, uint32_t* tab, size_t n) {
+  const uint32_t one_m = red(shoup(1u, r_sh, f.p), f.p);
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i <= n; i += (size_t)gridDim.x * blockDim.x) {
+    if (i == 0) { tab[0] = 0; continue; }
+    const uint32_t im = red(shoup((uint32_t)i, r_sh, f.p), f.p);  // i * 2^32 mod p
+    tab[i] = mont_pow(im, f.p - 2, one_m, f);                        // (1/i) * 2^32
+  }
+}
+
+__global__ void k_derivative(Fp f, uint32_t q1, uint2 r_sh, const uint32_t* a, uint32_t* r, size_t cnt1) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < cnt1; i += (size_t)gridDim.x * blockDim.x) {
+    const uint32_t k = reduce_any((uint32_t)(i + 1), q1, f);
+    const uint32_t t = red(mont(a[i + 1], k, f), f.p);   // a*k/R
+    r[i] = red(shoup(t, r_sh, f.p), f.p);                // * R
+  }
+}
+
+// Direct product window (short operand a, la <= 40):
+// out[i] = sum_j a[j] * b[i + off - j].
+__global__ void k_direct(uint32_t p, Fp f, uint2 r_sh, const uint32_t* a, int la, const uint32_t* b, size_t lb,
+                         size_t off, size_t cnt, uint32_t* out, int accumulate) {
+  __shared__ uint32_t am[64];
+  if (threadIdx.x < la) {
+    const uint32_t v = a[threadIdx.x];
+    am[threadIdx.x] = (p == 2) ? v : (uint32_t)(((uint64_t)v << 32) % p);  // Montgomery form of a[j]
+  }
+  __syncthreads();
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < cnt; i += (size_t)gridDim.x * blockDim.x) {
+    const size_t k = i + off;
+    uint64_t acc = 0;
+    uint32_t bits = 0;
+    const int jlo = k >= lb ? (int)(k - lb + 1) : 0;
+    const int jhi = (int)((size_t)la - 1 < k ? (size_t)la - 1 : k);
+    for (int j = jlo; j <= jhi; ++j) {
+      const uint32_t bv = __ldg(b + (k - j));
+      if (p == 2) bits ^= am[j] & bv;
+      else acc += mont(am[j], bv, f);
+    }
+    uint32_t v = (p == 2) ? (bits & 1u) : (uint32_t)(acc % p);
+    if (accumulate) {
+      const uint64_t s = (uint64_t)v + out[i];
+      v = (uint32_t)(s >= p ? s - p : s);
+    }
+    out[i] = v;
+  }
+}
+
+int grid_for(size_t n, int threads) {
+  size_t b = (n + threads - 1) / threads;
+  if (b > 148 * 16) b = 148 * 16;
+  return b ? (int)b : 1;
+}
+
+uint2 shoup_const(uint32_t w, uint32_t p) { return make_uint2(w, (uint32_t)(((uint64_t)w << 32) / p)); }
+
+}  // namespace
+
+namespace fpx {
+
+int small_kernel_max_log() { return kSmallLog; }
+
+// Opt-in shared-memory limits; per device, called once per context.
+cudaError_t kernels_init() {
+  cudaError_t e = cudaSuccess;
+  auto set = [&](const void* fn, int bytes) {
+    const cudaError_t r = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (r != cudaSuccess) e = r;
+  };
+  set((const void*)k_small, 2 * padded_words(1 << kSmallLog) * 4);
+  set((const void*)k_colfwd, padded_words(1 << 14) * 4);
+  set((const void*)k_rows, 2 * padded_words(1 << 13) * 4);
+  set((const void*)k_colinv, padded_words(1 << 14) * 4);
+  return e;
+}
+
+cudaError_t launch_small(const PrimeTables& pt, int logN, const SmallJob& job, cudaStream_t s) {
+  SmallD d;
+  d.x = dev_in(job.x);
+  d.y = dev_in(job.y);
+  d.forward = job.forward;
+  d.ymode = job.ymode;
+  d.inverse = job.inverse;
+  d.yspec = job.yspec;
+  d.yspec_out = job.yspec_out;
+  d.spec_x = job.spec_x;
+  d.epi = dev_epi(job.epi);
+  const int N = 1 << logN;
+  int nt = N / 16;
+  if (nt < 32) nt = 32;
+  if (nt > 512) nt = 512;
+  const size_t smem = (size_t)2 * padded_words(N) * 4;
+  k_small<<<1, nt, smem, s>>>(d, dev_tab(pt), logN);
+  return cudaGetLastError();
+}
+
+// Column tile: W = 2^logW adjacent columns x R rows, at most 2^14 words (64 KiB
+// of shared memory, three CTAs per SM); 2^13 words for short columns so that
+// mid-size transforms still spread over several CTAs.
+static BigD big_dev(const BigTables& bt, const Tw2* lo, const Tw2* hi) {
+  int logW = bt.logR >= 11 ? 14 - bt.logR : 13 - bt.logR;
+  if (logW < 2) logW = 2;
+  if (logW > bt.logC) logW = bt.logC;
+  BigD d;
+  d.logR = bt.logR;
+  d.logC = bt.logC;
+  d.logW = logW;
+  d.lo = reinterpret_cast<const uint2*>(lo);
+  d.hi = reinterpret_cast<const uint2*>(hi);
+  return d;
+}
+
+static int col_tile_words(const BigD& d) { return (1 << d.logW) << d.logR; }
+
+cudaError_t launch_colfwd(const PrimeTables& pt, const BigTables& bt, int nops, const InOp* in, uint32_t* const* out,
+                          cudaStream_t s) {
+  ColOps ops{};
+  for (int i = 0; i < nops; ++i) {
+    ops.in[i] = dev_in(in[i]);
+    ops.out[i] = out[i];
+  }
+  const BigD d = big_dev(bt, bt.lo_fwd, bt.hi_fwd);
+  const size_t smem = (size_t)padded_words(col_tile_words(d)) * 4;
+  dim3 grid(1u << (d.logC - d.logW), (unsigned)nops);
+  k_colfwd<<<grid, 256, smem, s>>>(ops, d, dev_tab(pt));
+  return cudaGetLastError();
+}
+
+cudaError_t launch_rows(const PrimeTables& pt, const BigTables& bt, uint32_t* x, const uint32_t* y, int ymode,
+                        uint32_t* y_spec_out, int forward, int inverse, cudaStream_t s) {
+  const int C = 1 << bt.logC;
+  const size_t smem = (size_t)2 * padded_words(C) * 4;
+  const int nt = C / 16 > 512 ? 512 : C / 16;
+  k_rows<<<1u << bt.logR, nt, smem, s>>>(x, y, ymode, y_spec_out, forward, inverse, bt.logC, dev_tab(pt));
+  return cudaGetLastError();
+}
+
+cudaError_t launch_colinv(const PrimeTables& pt, const BigTables& bt, const uint32_t* in, int mont_scaled,
+                          const Epi& epi, cudaStream_t s) {
+  const BigD d = big_dev(bt, mont_scaled ? bt.lo_inv_r : bt.lo_inv, bt.hi_inv);
+  const size_t smem = (size_t)padded_words(col_tile_words(d)) * 4;
+  k_colinv<<<1u << (d.logC - d.logW), 256, smem, s>>>(in, d, dev_tab(pt), dev_epi(epi));
+  return cudaGetLastError();
+}
+
+cudaError_t launch_pointwise(uint32_t p, uint32_t* a, const uint32_t* b, size_t n, cudaStream_t s) {
+  k_pointwise<<<grid_for(n, 256), 256, 0, s>>>(make_fp(p), a, b, n);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_garner(uint32_t target, int primes, const uint32_t* c1, const uint32_t* c2, const uint32_t* c3,
+                          uint32_t* out, size_t n, int accumulate, cudaStream_t s) {
+  const uint64_t P1 = 167772161u, P2 = 469762049u, P3 = 754974721u;
+  auto powm = [](uint64_t a, uint64_t e, uint64_t m) {
+    uint64_t r = 1 % m;
+    a %= m;
+    for (; e; e >>= 1, a = a * a % m)
+      if (e & 1) r = r * a % m;
+    return r;
+  };
+  GarnerC g;
+  g.P1 = (uint32_t)P1; g.P2 = (uint32_t)P2; g.P3 = (uint32_t)P3;
+  g.inv12 = shoup_const((uint32_t)powm(P1 % P2, P2 - 2, P2), (uint32_t)P2);
+  g.p1_in3 = shoup_const((uint32_t)(P1 % P3), (uint32_t)P3);
+  g.inv123 = shoup_const((uint32_t)powm((P1 * P2) % P3, P3 - 2, P3), (uint32_t)P3);
+  g.t = target;
+  g.t_q1 = (uint32_t)((((uint64_t)1) << 32) / target);
+  g.p1_t = shoup_const((uint32_t)(P1 % target), target);
+  g.p12_t = shoup_const((uint32_t)((P1 * P2) % target), target);
+  k_garner<<<grid_for(n, 256), 256, 0, s>>>(g, primes, c1, c2, c3, out, n, accumulate);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_from_mont(uint32_t p, const uint32_t* in, uint32_t* out, size_t n, cudaStream_t s) {
+  if (n == 0) return cudaSuccess;
+  if (p == 2) k_bits2<<<grid_for(n, 256), 256, 0, s>>>(in, out, n);
+  else k_from_mont<<<grid_for(n, 256), 256, 0, s>>>(make_fp(p), in, out, n);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_to_mont(uint32_t p, const uint32_t* in, uint32_t* out, size_t n, cudaStream_t s) {
+  if (n == 0) return cudaSuccess;
+  if (p == 2) k_bits2<<<grid_for(n, 256), 256, 0, s>>>(in, out, n);
+  else k_scale<<<grid_for(n, 256), 256, 0, s>>>(p, in, out, n, shoup_const((uint32_t)((((uint64_t)1) << 32) % p), p));
+  return cudaGetLastError();
+}
+
+cudaError_t launch_scale(uint32_t p, const uint32_t* a, uint32_t* out, size_t n, uint32_t c, cudaStream_t s) {
+  if (n == 0) return cudaSuccess;
+  k_scale<<<grid_for(n, 256), 256, 0, s>>>(p, a, out, n, shoup_const(c % p, p));
+  return cudaGetLastError();
+}
+
+cudaError_t launch_inv_table(uint32_t p, uint32_t* tab, size_t n, cudaStream_t s) {
+  const uint32_t r = (uint32_t)((((uint64_t)1) << 32) % p);
+  const uint32_t r2 = (uint32_t)((uint64_t)r * r % p);
+  k_inv_table<<<grid_for(n + 1, 256), 256, 0, s>>>(make_fp(p), shoup_const(r, p), shoup_const(r2, p), tab, n);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_derivative(uint32_t p, const uint32_t* a, uint32_t* r, size_t cnt, cudaStream_t s) {
+  if (cnt <= 1) return cudaSuccess;
+  const uint32_t rr = (uint32_t)((((uint64_t)1) << 32) % p);
+  const uint32_t q1 = (uint32_t)((((uint64_t)1) << 32) / p);
+  k_derivative<<<grid_for(cnt - 1, 256), 256, 0, s>>>(make_fp(p), q1, shoup_const(rr, p), a, r, cnt - 1);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_direct_product(uint32_t p, const uint32_t* a, size_t la, const uint32_t* b, size_t lb, size_t off,
+                                  size_t cnt, uint32_t* out, int accumulate, cudaStream_t s) {
+  if (cnt == 0) return cudaSuccess;
+  const Fp f = (p & 1u) ? make_fp(p) : Fp{p, 2 * p, 1};
+  const uint32_t r = (uint32_t)((((uint64_t)1) << 32) % p);
+  k_direct<<<grid_for(cnt, 256), 256, 0, s>>>(p, f, shoup_const(r, p), a, (int)la, b, lb, off, cnt, out, accumulate);
+  return cudaGetLastError();
+}
+
+}  // namespace fpx
+
+// ---------------------------------------------------------------------------
+// Series helpers: seeds (O(32^2) recurrences), scans, reversal, subtraction.
+// Generic 64-bit arithmetic: any prime 2 <= p < 2^31.
+// ---------------------------------------------------------------------------
+namespace {
+
+__device__ __forceinline__ uint32_t mm64(uint32_t a, uint32_t b, uint32_t p) { return (uint32_t)((uint64_t)a * b % p); }
+__device__ uint32_t pow64(uint32_t a, uint64_t e, uint32_t p) {
+  uint32_t r = 1 % p, b = a % p;
+  for (; e; e >>= 1) {
+    if (e & 1) r = mm64(r, b, p);
+    b = mm64(b, b, p);
+  }
+  return r;
+}
+__device__ __forceinline__ uint32_t inv64(uint32_t a, uint32_t p) { return p == 2 ? a : pow64(a, p - 2, p); }
+
+// Warp-wide sum mod p of per-lane values < p.
+__device__ __forceinline__ uint32_t warp_sum_mod(uint32_t v, uint32_t p) {
+  uint64_t s = v;
+#pragma unroll
+  for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  return (uint32_t)(s % p);
+}
+
+// kind 0: inverse seed   c[i] = -(sum_{j=1..i, j<la} a[j] c[i-j]) * c[0], c[0] = 1/a[0]
+// kind 1: exp seed       b[i] = (sum_{j=1..min(i,la)} a[j-1] b[i-j]) / i,   b[0] = 1   (a = a')
+// kind 2: sqrt seed      b[i] = (u[i] - sum_{j=1..i-1} b[j] b[i-j]) * w,     b[0] = r0, w = 1/(2 r0)
+// One warp; n <= 64.  Writes out[0..n).
+__global__ void k_seed(int kind, uint32_t p, const uint32_t* a, size_t la, uint32_t* out, int n, uint32_t r0) {
+  __shared__ uint32_t c[64];
+  const int lane = threadIdx.x;
+  uint32_t w = 0;
+  if (lane == 0) {
+    if (kind == 0) c[0] = inv64(a[0] % p, p);
+    else if (kind == 1) c[0] = 1 % p;
+    else { c[0] = r0; w = inv64(mm64(2 % p, r0, p), p); }
+  }
+  w = __shfl_sync(0xffffffffu, w, 0);
+  __syncwarp();
+  for (int i = 1; i < n; ++i) {
+    uint32_t part = 0;
+    for (int j = 1 + lane; j <= i; j += 32) {
+      if (kind == 0) { if ((size_t)j < la) part = (uint32_t)((part + (uint64_t)mm64(a[j] % p, c[i - j], p)) % p); }
+      else if (kind == 1) { if ((size_t)j <= la) part = (uint32_t)((part + (uint64_t)mm64(a[j - 1] % p, c[i - j], p)) % p); }
+      else { if (j < i) part = (uint32_t)((part + (uint64_t)mm64(c[j], c[i - j], p)) % p); }
+    }
+    const uint32_t s = warp_sum_mod(part, p);
+    if (lane == 0) {
+      uint32_t v;
+      if (kind == 0) v = mm64(s ? p - s : 0u, c[0], p);
+      else if (kind == 1) v = mm64(s, inv64((uint32_t)i % p, p), p);
+      else {
+        const uint32_t u = (size_t)i < la ? a[i] % p : 0u;
+        v = mm64(u >= s ? u - s : u + p - s, w, p);
+      }
+      c[i] = v;
+    }
+    __syncwarp();
+  }
+  for (int i = lane; i < n; i += 32) out[i] = c[i];
+}
+
+// First (mode 0) or last (mode 1) index in [0, n) with a[i] != 0; n if none.
+__global__ void k_find_nonzero(const uint32_t* a, size_t n, int mode, unsigned long long* res) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    if (a[i]) {
+      if (mode == 0) atomicMin(res, (unsigned long long)i);
+      else atomicMax(res, (unsigned long long)i);
+    }
+  }
+}
+
+__global__ void k_reverse(const uint32_t* a, uint32_t* r, size_t n) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    r[i] = a[n - 1 - i];
+}
+
+// r[i] = a[i] - b[i] (mod p), b missing beyond lb.
+__global__ void k_sub(uint32_t p, const uint32_t* a, const uint32_t* b, size_t lb, uint32_t* r, size_t n) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    const uint32_t x = a[i], y = i < lb ? b[i] : 0u;
+    r[i] = x >= y ? x - y : x + (p - y);
+  }
+}
+
+// Characteristic two square root (square_root.hpp:14-23): out[i/2] = a[i] for even i.
+__global__ void k_sqrt_char2(const uint32_t* a, size_t cnt, uint32_t* out, unsigned long long* odd_flag) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < cnt; i += (size_t)gridDim.x * blockDim.x) {
+    const uint32_t v = a[i] & 1u;
+    if (i & 1) { if (v) atomicMax(odd_flag, 1ull); }
+    else out[i / 2] = v;
+  }
+}
+
+// Elementwise Montgomery-table product: out[i] = a[i] * tab[i] (tab in Montgomery form).
+__global__ void k_mul_mont_tab(Fp f, const uint32_t* a, const uint32_t* tab, uint32_t* out, size_t n) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    out[i] = red(mont(a[i], tab[i], f), f.p);
+}
+
+}  // namespace
+
+namespace fpx {
+
+cudaError_t launch_seed(int kind, uint32_t p, const uint32_t* a, size_t la, uint32_t* out, int n, uint32_t r0,
+                        cudaStream_t s) {
+  if (n <= 0) return cudaSuccess;
+  k_seed<<<1, 32, 0, s>>>(kind, p, a, la, out, n, r0);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_find_nonzero(const uint32_t* a, size_t n, int mode, unsigned long long* res, cudaStream_t s) {
+  if (n == 0) return cudaSuccess;
+  k_find_nonzero<<<grid_for(n, 256), 256, 0, s>>>(a, n, mode, res);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_reverse(const uint32_t* a, uint32_t* r, size_t n, cudaStream_t s) {
+  if (n == 0) return cudaSuccess;
+  k_reverse<<<grid_for(n, 256), 256, 0, s>>>(a, r, n);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_sub(uint32_t p, const uint32_t* a, const uint32_t* b, size_t lb, uint32_t* r, size_t n,
+                       cudaStream_t s) {
+  if (n == 0) return cudaSuccess;
+  k_sub<<<grid_for(n, 256), 256, 0, s>>>(p, a, b, lb, r, n);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_sqrt_char2(const uint32_t* a, size_t cnt, uint32_t* out, unsigned long long* odd_flag,
+                              cudaStream_t s) {
+  if (cnt == 0) return cudaSuccess;
+  k_sqrt_char2<<<grid_for(cnt, 256), 256, 0, s>>>(a, cnt, out, odd_flag);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_mul_mont_tab(uint32_t p, const uint32_t* a, const uint32_t* tab, uint32_t* out, size_t n,
+                                cudaStream_t s) {
+  if (n == 0) return cudaSuccess;
+  k_mul_mont_tab<<<grid_for(n, 256), 256, 0, s>>>(make_fp(p), a, tab, out, n);
+  return cudaGetLastError();
+}
+
+}  // namespace fpx

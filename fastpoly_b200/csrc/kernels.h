@@ -1,0 +1,122 @@
+// kernels.h - host-side launchers for the sm_100a transform kernels.
+// Only plain types cross this header; the engine (engine.cpp) composes them.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace fpx {
+
+struct Tw2 { uint32_t w, q; };  // twiddle value + Shoup quotient (device: uint2)
+
+// Per-prime, size-independent tables: tw[h + k] = w_{2h}^{+-k} for 2h <= 2^13.
+struct PrimeTables {
+  uint32_t p = 0;
+  int max_log = 0;            // v2(p-1)
+  int small_log = 0;          // tables cover block lengths up to 2^small_log
+  const Tw2* fwd = nullptr;   // device
+  const Tw2* inv = nullptr;   // device
+  uint32_t q1 = 0;            // floor(2^32 / p)
+};
+
+// Per-(prime, N) tables for the two-pass (four-step) decomposition.
+struct BigTables {
+  int logN = 0, logR = 0, logC = 0;
+  const Tw2* lo_fwd = nullptr;     // w_N^y, y < 4096
+  const Tw2* hi_fwd = nullptr;     // w_N^(4096 x), x < N/4096
+  const Tw2* lo_inv = nullptr;     // w_N^-y / N
+  const Tw2* lo_inv_r = nullptr;   // w_N^-y * 2^32 / N  (after a Montgomery pointwise)
+  const Tw2* hi_inv = nullptr;     // w_N^-(4096 x)
+};
+
+// A forward-transform input: values at ptr[0, count), zero beyond.
+struct InOp {
+  const uint32_t* ptr = nullptr;
+  uint32_t count = 0;
+  int reduce = 0;  // inputs may be >= 2p (any 32-bit value): reduce mod p on load
+};
+
+// Output epilogue of an inverse transform: natural-order outputs [lo, hi) go to
+// out[i - lo] as: y = canonical(x); y = y * scale; y = y * mul[i-lo] (Montgomery
+// table); y = -y; y = sub_from[i-lo] - y; y = out[i-lo] + y (accumulate).
+struct Epi {
+  uint32_t* out = nullptr;
+  uint32_t lo = 0, hi = 0;
+  Tw2 scale{0, 0};
+  const uint32_t* mul_mont = nullptr;
+  int negate = 0;
+  const uint32_t* sub_from = nullptr;
+  uint32_t sub_len = 0;
+  int accumulate = 0;
+};
+
+// -------- single-CTA transforms, N = 2^logN <= 2^13 ----------------------------
+// x: forward input.  y: second operand (mode 0 none, 1 raw input, 2 spectrum,
+// 3 square x).  If spec_out != null the forward spectrum of y (mode 1) is stored
+// there.  If inverse, the product (or x's spectrum) is inverse-transformed with
+// scale epi.scale and written through the epilogue; otherwise x's spectrum
+// (times y when mode != 0, Montgomery) is written to spec_x (lazy, [0, 2p)).
+struct SmallJob {
+  int forward = 1;   // 0: x already holds a spectrum (N words), inverse only
+  InOp x;
+  InOp y;
+  int ymode = 0;
+  const uint32_t* yspec = nullptr;
+  uint32_t* yspec_out = nullptr;
+  uint32_t* spec_x = nullptr;
+  int inverse = 1;
+  Epi epi;
+};
+cudaError_t launch_small(const PrimeTables& pt, int logN, const SmallJob& job, cudaStream_t s);
+
+// -------- two-pass transforms, N = R*C > 2^13 ----------------------------------
+// Pass A forward: column DIF over up to 3 operands, each to its own N-word buffer.
+cudaError_t launch_colfwd(const PrimeTables& pt, const BigTables& bt, int nops, const InOp* in,
+                          uint32_t* const* out, cudaStream_t s);
+// Pass B: per row: DIF x (and y if ymode==1), pointwise (ymode 1/2/3), DIT if inverse.
+// ymode: 0 none, 1 raw (after pass A), 2 spectrum, 3 square.  y_spec_out: store y's row spectrum.
+cudaError_t launch_rows(const PrimeTables& pt, const BigTables& bt, uint32_t* x, const uint32_t* y, int ymode,
+                        uint32_t* y_spec_out, int forward, int inverse, cudaStream_t s);
+// Pass A inverse: Bailey twiddle (scaled), column DIT, epilogue on the window.
+cudaError_t launch_colinv(const PrimeTables& pt, const BigTables& bt, const uint32_t* in, int mont_scaled,
+                          const Epi& epi, cudaStream_t s);
+
+// -------- elementwise ------------------------------------------------------------
+// out[i] = mont(a[i], b[i]) for lazy spectra (result in (0, 2p)).
+cudaError_t launch_pointwise(uint32_t p, uint32_t* a, const uint32_t* b, size_t n, cudaStream_t s);
+// Garner reconstruction of `primes` auxiliary residues into the target field:
+// out[i] (+)= CRT(c1[i], c2[i], c3[i]) mod target.  Inputs canonical.
+cudaError_t launch_garner(uint32_t target, int primes, const uint32_t* c1, const uint32_t* c2,
+                          const uint32_t* c3, uint32_t* out, size_t n, int accumulate, cudaStream_t s);
+// Montgomery limbs <-> canonical residues (repr conversion), in place allowed.
+cudaError_t launch_from_mont(uint32_t p, const uint32_t* in, uint32_t* out, size_t n, cudaStream_t s);
+cudaError_t launch_to_mont(uint32_t p, const uint32_t* in, uint32_t* out, size_t n, cudaStream_t s);
+// out[i] = a[i] * c (canonical, Shoup constant).
+cudaError_t launch_scale(uint32_t p, const uint32_t* a, uint32_t* out, size_t n, uint32_t c, cudaStream_t s);
+// 1/i for i in [1, n] into tab (Montgomery form: (1/i) * 2^32 mod p), tab[0] = 0.
+cudaError_t launch_inv_table(uint32_t p, uint32_t* tab, size_t n, cudaStream_t s);
+// r[i] = a[i+1] * (i+1) for i < cnt-1 (derivative of the first cnt coefficients).
+cudaError_t launch_derivative(uint32_t p, const uint32_t* a, uint32_t* r, size_t cnt, cudaStream_t s);
+// Direct (schoolbook) product window for short operands:
+// out[i] = sum_j a[j] b[i+off-j], i < cnt (canonical).  Used for min(la,lb) <= 40.
+cudaError_t launch_direct_product(uint32_t p, const uint32_t* a, size_t la, const uint32_t* b, size_t lb,
+                                  size_t off, size_t cnt, uint32_t* out, int accumulate, cudaStream_t s);
+
+int small_kernel_max_log();
+cudaError_t kernels_init();
+
+}  // namespace fpx
+
+namespace fpx {
+// Seeds of the Newton loops (kind 0 inverse, 1 exp (a = a'), 2 sqrt (a = u, r0 = root)); n <= 64.
+cudaError_t launch_seed(int kind, uint32_t p, const uint32_t* a, size_t la, uint32_t* out, int n, uint32_t r0,
+                        cudaStream_t s);
+// *res = min (mode 0) / max (mode 1) index with a[i] != 0; caller initialises *res.
+cudaError_t launch_find_nonzero(const uint32_t* a, size_t n, int mode, unsigned long long* res, cudaStream_t s);
+cudaError_t launch_reverse(const uint32_t* a, uint32_t* r, size_t n, cudaStream_t s);
+cudaError_t launch_sub(uint32_t p, const uint32_t* a, const uint32_t* b, size_t lb, uint32_t* r, size_t n,
+                       cudaStream_t s);
+cudaError_t launch_sqrt_char2(const uint32_t* a, size_t cnt, uint32_t* out, unsigned long long* odd_flag,
+                              cudaStream_t s);
+cudaError_t launch_mul_mont_tab(uint32_t p, const uint32_t* a, const uint32_t* tab, uint32_t* out, size_t n,
+                                cudaStream_t s);
+}  // namespace fpx

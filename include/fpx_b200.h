@@ -1,0 +1,125 @@
+/*
+ * fpx_b200.h - C ABI of the B200-native fastpoly hot path.
+ *
+ * Plain C types only.  Every function returns an fpx status (0 = success).
+ * Values are 32-bit residues modulo a prime 2 <= p < 2^31, either canonical
+ * (FPX_REPR_CANONICAL: x in [0, p)) or the reference's Montgomery limbs
+ * (FPX_REPR_MONTGOMERY: x * 2^32 mod p, include/fastpoly/modint.hpp:57-98;
+ * for p = 2 the limb is the bit itself), so a fpx::Poly<fpx::Mont<p>> can hand
+ * over its storage unchanged.
+ *
+ * Two flavours of each operation:
+ *   - host buffers (blocking): inputs are copied to the GPU, the result copied
+ *     back; the call returns when the output is in place;
+ *   - "_device" (asynchronous): all pointers are device pointers, canonical
+ *     residues, work is queued on the context's stream (fpx_ctx_set_stream).
+ *
+ * Error conditions follow the reference exactly: FPX_EDOMAIN where it throws
+ * fpx::poly::domain_error, FPX_ESIZE for fpx::ntt_size_error, FPX_ELENGTH for
+ * std::length_error.  Nothing is written to outputs on error.
+ */
+#ifndef FPX_B200_H
+#define FPX_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum fpx_status {
+  FPX_OK = 0,
+  FPX_EDOMAIN = 1,      /* fpx::poly::domain_error (base.hpp:26-30) */
+  FPX_ESIZE = 2,        /* fpx::ntt_size_error (ntt.hpp:59-70) */
+  FPX_ELENGTH = 3,      /* std::length_error (convolution.hpp:20-21) */
+  FPX_ENOMEM = 4,       /* device memory pool exhausted */
+  FPX_ETIMEDOUT = 5,    /* a bounded device wait gave up */
+  FPX_ECUDA = 6,        /* CUDA runtime error (see fpx_last_error_message) */
+  FPX_EINVAL = 7,       /* bad argument (null pointer, modulus not prime < 2^31, ...) */
+  FPX_EUNSUPPORTED = 8  /* no usable CUDA device */
+};
+
+enum fpx_repr { FPX_REPR_CANONICAL = 0, FPX_REPR_MONTGOMERY = 1 };
+
+typedef struct fpx_ctx fpx_ctx;
+
+typedef struct fpx_pool_stats_t {
+  size_t cached_bytes;       /* idle bytes held for reuse */
+  size_t cached_blocks;
+  size_t in_use_bytes;       /* bytes handed out and not yet returned */
+  size_t system_allocations; /* cudaMalloc calls made so far */
+  size_t cache_hits;         /* requests served from the idle cache */
+  size_t limit_bytes;        /* 0 = unlimited */
+} fpx_pool_stats_t;
+
+/* ---- context (replaces the reference's per-thread scratch pool and plan cache:
+ *      memory.hpp:117-187, ntt.hpp:250-276) ------------------------------------ */
+int fpx_ctx_create(int device, size_t pool_limit_bytes, fpx_ctx** out);
+int fpx_ctx_destroy(fpx_ctx* ctx);
+/* cudaStream_t passed as void*; NULL selects the context's own stream. */
+int fpx_ctx_set_stream(fpx_ctx* ctx, void* stream);
+void* fpx_ctx_stream(fpx_ctx* ctx);
+int fpx_ctx_synchronize(fpx_ctx* ctx);
+const char* fpx_last_error_message(fpx_ctx* ctx);
+/* scratch_memory_stats() / release_scratch_memory() (memory.hpp:21-26, 252-258) */
+int fpx_pool_stats(fpx_ctx* ctx, fpx_pool_stats_t* out);
+int fpx_release_pool(fpx_ctx* ctx);
+
+/* ---- instrumentation (the reference's bench harness timing, bench/bench.cpp:161-203,
+ *      moved onto the device) ---------------------------------------------------
+ * fpx_profile(ctx, 1) starts recording a CUDA event pair on the launching stream
+ * around every kernel launch (and clears earlier records); fpx_profile_report
+ * writes {"kernel": [launches, total_ms], ...} as a NUL-terminated JSON object.
+ * fpx_launch_count counts every kernel launched by the context. */
+int fpx_profile(fpx_ctx* ctx, int enable);
+int fpx_profile_report(fpx_ctx* ctx, char* buf, size_t cap, size_t* needed);
+uint64_t fpx_launch_count(fpx_ctx* ctx);
+
+/* ---- transforms (NttPlan<M>::forward / inverse, ntt.hpp:140-192) -------------
+ * In place, n a power of two with 2 <= n <= 2^v2(p-1), p < 2^30 odd.  forward
+ * leaves the spectrum in the reference's bit-reversed order; inverse takes that
+ * order back and scales by 1/n.  Outputs canonical. */
+int fpx_ntt_max_log(uint32_t p);
+int fpx_ntt_forward(fpx_ctx* ctx, uint32_t p, uint32_t* data, uint32_t n, int repr);
+int fpx_ntt_inverse(fpx_ctx* ctx, uint32_t p, uint32_t* data, uint32_t n, int repr);
+int fpx_ntt_forward_device(fpx_ctx* ctx, uint32_t p, uint32_t* d_data, uint32_t n);
+int fpx_ntt_inverse_device(fpx_ctx* ctx, uint32_t p, uint32_t* d_data, uint32_t n);
+
+/* ---- polynomial operations (fpx::poly, include/fastpoly/detail/poly) ----------- */
+/* conv(a, b, n): the product truncated to min(la+lb-1, n) terms, *out_len set;
+ * n = SIZE_MAX for the full product (convolution.hpp:17-147).  out needs
+ * min(la+lb-1, n) words. */
+int fpx_conv(fpx_ctx* ctx, uint32_t p, const uint32_t* a, size_t la, const uint32_t* b, size_t lb, size_t n,
+             uint32_t* out, size_t* out_len, int repr);
+int fpx_conv_device(fpx_ctx* ctx, uint32_t p, const uint32_t* d_a, size_t la, const uint32_t* d_b, size_t lb,
+                    size_t n, uint32_t* d_out, size_t* out_len);
+
+/* Series operations mod x^n; out needs n words (inverse.hpp:163, exponential.hpp:85,
+ * :107, square_root.hpp:12, power.hpp:17). */
+int fpx_inv(fpx_ctx* ctx, uint32_t p, const uint32_t* a, size_t la, size_t n, uint32_t* out, int repr);
+int fpx_log(fpx_ctx* ctx, uint32_t p, const uint32_t* a, size_t la, size_t n, uint32_t* out, int repr);
+int fpx_exp(fpx_ctx* ctx, uint32_t p, const uint32_t* a, size_t la, size_t n, uint32_t* out, int repr);
+int fpx_sqrt(fpx_ctx* ctx, uint32_t p, const uint32_t* a, size_t la, size_t n, uint32_t* out, int repr);
+int fpx_pow(fpx_ctx* ctx, uint32_t p, const uint32_t* a, size_t la, uint64_t k, size_t n, uint32_t* out, int repr);
+int fpx_inv_device(fpx_ctx* ctx, uint32_t p, const uint32_t* d_a, size_t la, size_t n, uint32_t* d_out);
+int fpx_log_device(fpx_ctx* ctx, uint32_t p, const uint32_t* d_a, size_t la, size_t n, uint32_t* d_out);
+int fpx_exp_device(fpx_ctx* ctx, uint32_t p, const uint32_t* d_a, size_t la, size_t n, uint32_t* d_out);
+int fpx_sqrt_device(fpx_ctx* ctx, uint32_t p, const uint32_t* d_a, size_t la, size_t n, uint32_t* d_out);
+int fpx_pow_device(fpx_ctx* ctx, uint32_t p, const uint32_t* d_a, size_t la, uint64_t k, size_t n,
+                   uint32_t* d_out);
+
+/* divmod(a, b) (division.hpp:86-104): q needs la words, r needs lb words; the
+ * returned lengths are trimmed like the reference's results. */
+int fpx_divmod(fpx_ctx* ctx, uint32_t p, const uint32_t* a, size_t la, const uint32_t* b, size_t lb, uint32_t* q,
+               size_t* q_len, uint32_t* r, size_t* r_len, int repr);
+int fpx_div(fpx_ctx* ctx, uint32_t p, const uint32_t* a, size_t la, const uint32_t* b, size_t lb, uint32_t* q,
+            size_t* q_len, int repr);
+int fpx_mod(fpx_ctx* ctx, uint32_t p, const uint32_t* a, size_t la, const uint32_t* b, size_t lb, uint32_t* r,
+            size_t* r_len, int repr);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FPX_B200_H */
