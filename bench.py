@@ -187,8 +187,10 @@ def run_fpx(args):
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     ctx = F.Context(local)
-    stream = torch.cuda.current_stream()
+    # one stream for the library's kernels, the L2 flush and the timing events
+    stream = torch.cuda.Stream()
     ctx.set_stream(stream.cuda_stream)
+    torch.cuda.set_stream(stream)
 
     a, b = inputs(1 + rank)
     da = torch.from_numpy(a.view(np.int32)).cuda()

@@ -444,7 +444,7 @@ void Engine::cyc_product(uint32_t p, int logN, const CycOp& op) {
     if (epi.scale.w) s = s * epi.scale.w % p;
     epi.scale = shoup_pair((uint32_t)s, p);
     j.epi = epi;
-    kcheck(launch_small(pt, logN, j, stream_), "small transform");
+    kcheck(launch_small(pt, logN, j, stream_), "small");
     return;
   }
   const BigTables& bt = big_plan(p, logN).t;
@@ -458,10 +458,10 @@ void Engine::cyc_product(uint32_t p, int logN, const CycOp& op) {
     outs[1] = t2.get();
     nops = 2;
   }
-  kcheck(launch_colfwd(pt, bt, nops, ins, outs, stream_), "column pass");
+  kcheck(launch_colfwd(pt, bt, nops, ins, outs, stream_), "colfwd");
   const uint32_t* y = op.ymode == 1 ? t2.get() : op.yspec;
-  kcheck(launch_rows(pt, bt, t1.get(), y, op.ymode, op.yspec_out, 1, 1, stream_), "row pass");
-  kcheck(launch_colinv(pt, bt, t1.get(), op.ymode != 0, epi, stream_), "inverse column pass");
+  kcheck(launch_rows(pt, bt, t1.get(), y, op.ymode, op.yspec_out, 1, 1, stream_), "rows");
+  kcheck(launch_colinv(pt, bt, t1.get(), op.ymode != 0, epi, stream_), "colinv");
 }
 
 void Engine::product(uint32_t p, const uint32_t* a, size_t la, const uint32_t* b, size_t lb, size_t outn,
@@ -483,7 +483,7 @@ void Engine::product(uint32_t p, const uint32_t* a, size_t la, const uint32_t* b
     const bool swap = la > lb;
     kcheck(launch_direct_product(p, swap ? b : a, swap ? lb : la, swap ? a : b, swap ? la : lb, 0, outn, out,
                                 accumulate ? 1 : 0, stream_),
-          "direct product");
+          "direct");
     if (post_mont) kcheck(launch_mul_mont_tab(p, out, post_mont, out, outn, stream_), "post scale");
     return;
   }
@@ -526,7 +526,7 @@ void Engine::crt_product(uint32_t p, const uint32_t* a, size_t la, const uint32_
         const bool swap = na > nb;
         kcheck(launch_direct_product(p, swap ? pb : pa, swap ? nb : na, swap ? pa : pb, swap ? na : nb, 0, cnt, po, 1,
                                     stream_),
-              "direct product");
+              "direct");
       } else {
         const size_t primes = crt_prime_count(p, std::min(na, nb));
         const int logN = std::bit_width(na + nb - 2);
@@ -943,22 +943,22 @@ void Engine::ntt(uint32_t p, uint32_t* data, uint32_t n, bool inverse) {
     j.epi.lo = 0;
     j.epi.hi = n;
     j.epi.scale = shoup_pair(invm(n % p, p), p);
-    kcheck(launch_small(pt, logN, j, stream_), "transform");
+    kcheck(launch_small(pt, logN, j, stream_), "small");
     return;
   }
   const BigTables& bt = big_plan(p, logN).t;
   if (!inverse) {
     InOp in{data, n, 0};
     uint32_t* outs[1] = {data};
-    kcheck(launch_colfwd(pt, bt, 1, &in, outs, stream_), "column pass");
-    kcheck(launch_rows(pt, bt, data, nullptr, 0, nullptr, 1, 0, stream_), "row pass");
+    kcheck(launch_colfwd(pt, bt, 1, &in, outs, stream_), "colfwd");
+    kcheck(launch_rows(pt, bt, data, nullptr, 0, nullptr, 1, 0, stream_), "rows");
   } else {
-    kcheck(launch_rows(pt, bt, data, nullptr, 0, nullptr, 0, 1, stream_), "row pass");
+    kcheck(launch_rows(pt, bt, data, nullptr, 0, nullptr, 0, 1, stream_), "rows");
     Epi e;
     e.out = data;
     e.lo = 0;
     e.hi = n;
-    kcheck(launch_colinv(pt, bt, data, 0, e, stream_), "column pass");
+    kcheck(launch_colinv(pt, bt, data, 0, e, stream_), "colinv");
   }
 }
 

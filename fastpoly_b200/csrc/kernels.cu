@@ -115,7 +115,7 @@ __global__ void __launch_bounds__(512) k_small(SmallD job, Ptab pt, int logN) {
     tile_dif(Y, logN, 0, pt.fwd, f, tid, nt);
     __syncthreads();
     if (job.yspec_out)
-      for (int i = tid; i < N; i += nt) job.yspec_out[i] = Y[pad(i)];
+      for (int i = tid; i < N; i += nt) job.yspec_out[i] = red(Y[pad(i)], f.p);
   }
   if (job.ymode == 1 || job.ymode == 2) {
     for (int i = tid; i < N; i += nt) X[pad(i)] = mont(X[pad(i)], Y[pad(i)], f);
@@ -123,7 +123,7 @@ __global__ void __launch_bounds__(512) k_small(SmallD job, Ptab pt, int logN) {
     for (int i = tid; i < N; i += nt) { const uint32_t v = X[pad(i)]; X[pad(i)] = mont(v, v, f); }
   }
   if (!job.inverse) {
-    for (int i = tid; i < N; i += nt) job.spec_x[i] = X[pad(i)];
+    for (int i = tid; i < N; i += nt) job.spec_x[i] = red(X[pad(i)], f.p);
     return;
   }
   __syncthreads();
@@ -196,7 +196,7 @@ __global__ void __launch_bounds__(512) k_rows(uint32_t* x, const uint32_t* y, in
     tile_dif(Y, logC, 0, pt.fwd, f, tid, nt);
     __syncthreads();
     if (y_spec_out)
-      for (int i = tid; i < C; i += nt) y_spec_out[row + i] = Y[pad(i)];
+      for (int i = tid; i < C; i += nt) y_spec_out[row + i] = red(Y[pad(i)], f.p);
   }
   if (ymode == 1 || ymode == 2) {
     for (int i = tid; i < C; i += nt) X[pad(i)] = mont(X[pad(i)], Y[pad(i)], f);
@@ -208,7 +208,11 @@ __global__ void __launch_bounds__(512) k_rows(uint32_t* x, const uint32_t* y, in
     tile_dit(X, logC, 0, pt.inv, f, tid, nt);
   }
   __syncthreads();
-  for (int i = tid; i < C; i += nt) x[row + i] = X[pad(i)];
+  if (inverse) {
+    for (int i = tid; i < C; i += nt) x[row + i] = X[pad(i)];
+  } else {  // a spectrum leaves canonical (lazy values stay inside the transform)
+    for (int i = tid; i < C; i += nt) x[row + i] = red(X[pad(i)], f.p);
+  }
 }
 
 // ---------------------------------------------------------------------------

@@ -1,0 +1,460 @@
+// fpx/fastpoly.hpp - C++20 drop-in for the reference's polynomial API, backed
+// by the B200 library through its C ABI (fpx_b200.h).
+//
+// Same names, signatures, value semantics and error types as the reference's
+// umbrella header include/fastpoly/fastpoly.hpp:
+//   fpx::Mont<Mod, Root>, fpx::ModInt<Mod>, fpx::mod998244353 ...   (modint.hpp:57-205)
+//   fpx::Poly<M> : std::vector<M>                                    (poly.hpp:16-86)
+//   fpx::poly::conv / inv / log / exp / sqrt / pow / divmod / div / mod
+//   fpx::NttPlan<M>::get(n)->forward / inverse                       (ntt.hpp:130-192)
+//   fpx::poly::domain_error, fpx::ntt_size_error
+// A Poly<Mont<p>> hands its Montgomery limbs to the GPU unchanged
+// (FPX_REPR_MONTGOMERY); the first and last GPU passes convert.  The O(n) host
+// helpers (add, sub, neg, mul_scalar, shift, eval, derivative, integral) are
+// plain loops: they are not on the transform path.
+//
+// Link with fastpoly_b200/libfpx_b200.so.  One process-wide context on device
+// FPX_DEVICE (default 0) is created on first use; calls from several threads
+// are serialised inside it.
+#ifndef FPX_DROPIN_FASTPOLY_HPP
+#define FPX_DROPIN_FASTPOLY_HPP
+
+#include <algorithm>
+#include <array>
+#include <cstdint>
+#include <cstdlib>
+#include <istream>
+#include <memory>
+#include <mutex>
+#include <ostream>
+#include <stdexcept>
+#include <string>
+#include <type_traits>
+#include <utility>
+#include <vector>
+
+#include "fpx_b200.h"
+
+namespace fpx {
+
+// ------------------------------------------------------------------ field
+
+constexpr uint32_t inv_mod_2_32(uint32_t a) {
+  uint32_t x = 1;
+  for (int i = 0; i < 5; ++i) x *= 2u - a * x;
+  return x;
+}
+
+constexpr uint32_t primitive_root(uint32_t p) {
+  if (p == 2) return 1;
+  std::array<uint32_t, 10> f{};
+  size_t nf = 0;
+  uint32_t rem = p - 1;
+  for (uint32_t d = 2; uint64_t(d) * d <= rem; ++d) {
+    if (rem % d) continue;
+    f[nf++] = d;
+    while (rem % d == 0) rem /= d;
+  }
+  if (rem > 1) f[nf++] = rem;
+  auto pw = [p](uint64_t a, uint32_t e) {
+    uint64_t r = 1;
+    for (; e; e >>= 1, a = a * a % p)
+      if (e & 1) r = r * a % p;
+    return r;
+  };
+  for (uint32_t g = 2; g < p; ++g) {
+    bool ok = true;
+    for (size_t i = 0; i < nf && ok; ++i) ok = pw(g, (p - 1) / f[i]) != 1;
+    if (ok) return g;
+  }
+  return 0;
+}
+
+/// Element of GF(Mod) stored as the Montgomery limb x * 2^32 mod Mod (a single
+/// bit for Mod = 2), bit-compatible with the reference's Mont.
+template <uint32_t Mod, uint32_t Root = 0>
+class Mont {
+ public:
+  static_assert(Mod < (1u << 31) && Mod >= 2, "modulus must be a prime in [2, 2^31)");
+  static constexpr uint32_t mod = Mod;
+  static constexpr uint32_t primitive_root = Root != 0 ? Root : fpx::primitive_root(Mod);
+  static constexpr uint32_t ninv = static_cast<uint32_t>(0u - inv_mod_2_32(Mod | 1u));
+  static constexpr uint32_t one = Mod == 2 ? 1u : static_cast<uint32_t>((uint64_t(1) << 32) % Mod);
+  static constexpr uint32_t r2 = static_cast<uint32_t>(uint64_t(one) * one % Mod);
+  static constexpr uint32_t inv2 = (Mod + 1) / 2;
+
+  constexpr Mont() : v_(0) {}
+  template <class I, class = std::enable_if_t<std::is_integral_v<I> && !std::is_same_v<I, bool>>>
+  constexpr Mont(I x) : v_(enter(static_cast<uint64_t>(x))) {}
+
+  static constexpr Mont from_int(uint64_t x) { return wrap(enter(x)); }
+  static constexpr Mont raw(uint32_t x) { return wrap(x); }
+  static constexpr uint32_t reduce(uint64_t t) {
+    if constexpr (Mod == 2) return static_cast<uint32_t>(t & 1u);
+    const uint32_t m = static_cast<uint32_t>(t) * ninv;
+    const uint64_t u = (t + uint64_t(m) * Mod) >> 32;
+    return static_cast<uint32_t>(u >= Mod ? u - Mod : u);
+  }
+  constexpr uint32_t val() const { return reduce(v_); }
+  constexpr uint32_t raw_val() const { return v_; }
+
+  friend constexpr Mont operator+(Mont a, Mont b) {
+    const uint32_t s = a.v_ + b.v_;
+    return wrap(s >= Mod ? s - Mod : s);
+  }
+  friend constexpr Mont operator-(Mont a, Mont b) { return wrap(a.v_ >= b.v_ ? a.v_ - b.v_ : a.v_ - b.v_ + Mod); }
+  friend constexpr Mont operator-(Mont a) { return wrap(a.v_ == 0 ? 0 : Mod - a.v_); }
+  friend constexpr Mont operator*(Mont a, Mont b) { return wrap(reduce(uint64_t(a.v_) * b.v_)); }
+  friend constexpr Mont operator/(Mont a, Mont b) { return a * b.inv(); }
+  constexpr Mont& operator+=(Mont b) { return *this = *this + b; }
+  constexpr Mont& operator-=(Mont b) { return *this = *this - b; }
+  constexpr Mont& operator*=(Mont b) { return *this = *this * b; }
+  constexpr Mont& operator/=(Mont b) { return *this = *this / b; }
+  friend constexpr bool operator==(Mont a, Mont b) { return a.v_ == b.v_; }
+  friend constexpr bool operator!=(Mont a, Mont b) { return a.v_ != b.v_; }
+  constexpr bool is_zero() const { return v_ == 0; }
+  constexpr bool operator!() const { return v_ == 0; }
+  constexpr explicit operator bool() const { return v_ != 0; }
+
+  constexpr Mont pow(uint64_t e) const {
+    Mont r = from_int(1), b = *this;
+    for (; e; e >>= 1) {
+      if (e & 1) r *= b;
+      b *= b;
+    }
+    return r;
+  }
+  constexpr Mont inv() const {
+    if constexpr (Mod == 2) return *this;
+    else return pow(Mod - 2);
+  }
+  /// Tonelli-Shanks with the reference's root choice (z searched upward from 2).
+  bool sqrt(Mont& out) const {
+    if constexpr (Mod == 2) { out = *this; return true; }
+    const Mont o = from_int(1);
+    if (v_ == 0) { out = *this; return true; }
+    if (pow((Mod - 1) / 2) != o) return false;
+    if (Mod % 4 == 3) { out = pow((uint64_t(Mod) + 1) / 4); return true; }
+    uint64_t q = Mod - 1;
+    int s = 0;
+    while (q % 2 == 0) { q /= 2; ++s; }
+    Mont z = from_int(2);
+    while (z.pow((Mod - 1) / 2) != -o) z += o;
+    Mont c = z.pow(q), x = pow((q + 1) / 2), t = pow(q);
+    int m = s;
+    while (t != o) {
+      int i = 0;
+      for (Mont t2 = t; t2 != o; t2 *= t2) ++i;
+      const Mont b = c.pow(uint64_t(1) << (m - i - 1));
+      x *= b;
+      c = b * b;
+      t *= c;
+      m = i;
+    }
+    out = x;
+    return true;
+  }
+  std::string str() const { return std::to_string(val()); }
+
+ private:
+  static constexpr uint32_t enter(uint64_t x) { return static_cast<uint32_t>(x % Mod) * uint64_t(one) % Mod; }
+  static constexpr Mont wrap(uint32_t v) {
+    Mont m;
+    m.v_ = v;
+    return m;
+  }
+  uint32_t v_;
+};
+
+template <uint32_t M, uint32_t R>
+std::ostream& operator<<(std::ostream& os, const Mont<M, R>& a) { return os << a.val(); }
+template <uint32_t M, uint32_t R>
+std::istream& operator>>(std::istream& is, Mont<M, R>& a) {
+  uint64_t x = 0;
+  is >> x;
+  a = Mont<M, R>::from_int(x);
+  return is;
+}
+
+using mod998244353 = Mont<998244353u, 3>;
+using mod1004535809 = Mont<1004535809u, 3>;
+using mod469762049 = Mont<469762049u, 3>;
+using mod167772161 = Mont<167772161u, 3>;
+using mod754974721 = Mont<754974721u, 11>;
+using mod1224736769 = Mont<1224736769u, 3>;
+template <uint32_t Mod>
+using ModInt = Mont<Mod>;
+using mod1000000007 = Mont<1000000007u>;
+
+// ------------------------------------------------------------------ errors
+
+class ntt_size_error : public std::runtime_error {
+ public:
+  explicit ntt_size_error(const std::string& s) : std::runtime_error(s) {}
+};
+namespace poly {
+class domain_error : public std::runtime_error {
+ public:
+  explicit domain_error(const std::string& s) : std::runtime_error(s) {}
+};
+template <class M>
+using vec = std::vector<M>;
+}  // namespace poly
+
+namespace gpu {
+
+/// The process-wide context (device from FPX_DEVICE, default 0).
+inline fpx_ctx* context() {
+  static std::once_flag once;
+  static fpx_ctx* ctx = nullptr;
+  static int status = 0;
+  std::call_once(once, [] {
+    const char* d = std::getenv("FPX_DEVICE");
+    status = fpx_ctx_create(d ? std::atoi(d) : 0, 0, &ctx);
+  });
+  if (!ctx) throw std::runtime_error("fastpoly_b200: no usable CUDA device (status " + std::to_string(status) + ")");
+  return ctx;
+}
+
+inline void check(int rc, const char* what) {
+  if (rc == FPX_OK) return;
+  const std::string msg = std::string(what) + ": " + fpx_last_error_message(context());
+  if (rc == FPX_EDOMAIN) throw poly::domain_error(msg);
+  if (rc == FPX_ESIZE) throw ntt_size_error(msg);
+  if (rc == FPX_ELENGTH) throw std::length_error(msg);
+  if (rc == FPX_ENOMEM) throw std::bad_alloc();
+  throw std::runtime_error(msg);
+}
+
+template <class M>
+const uint32_t* limbs(const std::vector<M>& v) {
+  static_assert(sizeof(M) == sizeof(uint32_t), "Mont must be a single 32-bit limb");
+  return reinterpret_cast<const uint32_t*>(v.data());
+}
+template <class M>
+uint32_t* limbs(std::vector<M>& v) {
+  return reinterpret_cast<uint32_t*>(v.data());
+}
+
+}  // namespace gpu
+
+// ---------------------------------------------------------------- NttPlan
+
+/// GPU transform of one size (the reference's NttPlan<M>, ntt.hpp:86-194):
+/// forward is the bit-reversal-free DIF (spectrum in bit-reversed order),
+/// inverse the matching DIT scaled by 1/n; both on Montgomery limbs, in place,
+/// outputs in [0, Mod).  Requires Mod < 2^30.
+template <class M>
+class NttPlan {
+ public:
+  static std::shared_ptr<const NttPlan> get(uint32_t n) {
+    check_size(n);
+    return std::shared_ptr<const NttPlan>(new NttPlan(n));
+  }
+  uint32_t size() const { return n_; }
+  void forward(uint32_t* a) const { gpu::check(fpx_ntt_forward(gpu::context(), M::mod, a, n_, FPX_REPR_MONTGOMERY), "ntt"); }
+  void inverse(uint32_t* a) const { gpu::check(fpx_ntt_inverse(gpu::context(), M::mod, a, n_, FPX_REPR_MONTGOMERY), "ntt"); }
+
+ private:
+  explicit NttPlan(uint32_t n) : n_(n) {}
+  static void check_size(uint32_t n) {
+    if (n < 2 || (n & (n - 1)) != 0) throw ntt_size_error("NTT size must be a power of two");
+    if (n > (uint64_t(1) << fpx_ntt_max_log(M::mod))) throw ntt_size_error("NTT size exceeds 2^v2(mod-1) for this modulus");
+  }
+  uint32_t n_;
+};
+
+// ------------------------------------------------------------------ poly
+
+namespace poly {
+
+inline constexpr size_t naive_threshold = 40;
+
+template <class M>
+void trim(vec<M>& a) {
+  while (!a.empty() && a.back().is_zero()) a.pop_back();
+}
+
+/// Product of a and b truncated to n coefficients (convolution.hpp:145-147).
+template <class M>
+vec<M> conv(const vec<M>& a, const vec<M>& b, size_t n = SIZE_MAX) {
+  if (a.empty() || b.empty() || n == 0) return {};
+  const size_t la = std::min(a.size(), n), lb = std::min(b.size(), n);
+  if (la > SIZE_MAX - (lb - 1)) throw std::length_error("poly::conv: result length overflows size_t");
+  vec<M> r(std::min(la + lb - 1, n));
+  size_t got = 0;
+  gpu::check(fpx_conv(gpu::context(), M::mod, gpu::limbs(a), a.size(), gpu::limbs(b), b.size(), n, gpu::limbs(r), &got,
+                      FPX_REPR_MONTGOMERY),
+             "poly::conv");
+  r.resize(got);
+  return r;
+}
+
+#define FPX_SERIES(name, fn)                                                                                   \
+  template <class M>                                                                                           \
+  vec<M> name(const vec<M>& a, size_t n) {                                                                     \
+    vec<M> r(n);                                                                                               \
+    gpu::check(fn(gpu::context(), M::mod, gpu::limbs(a), a.size(), n, gpu::limbs(r), FPX_REPR_MONTGOMERY),     \
+               "poly::" #name);                                                                                \
+    return r;                                                                                                  \
+  }
+FPX_SERIES(inv, fpx_inv)
+FPX_SERIES(log, fpx_log)
+FPX_SERIES(exp, fpx_exp)
+FPX_SERIES(sqrt, fpx_sqrt)
+#undef FPX_SERIES
+
+template <class M>
+vec<M> pow(const vec<M>& a, uint64_t k, size_t n) {
+  vec<M> r(n);
+  gpu::check(fpx_pow(gpu::context(), M::mod, gpu::limbs(a), a.size(), k, n, gpu::limbs(r), FPX_REPR_MONTGOMERY),
+             "poly::pow");
+  return r;
+}
+
+template <class M>
+std::pair<vec<M>, vec<M>> divmod(const vec<M>& a, const vec<M>& b) {
+  vec<M> q(std::max<size_t>(a.size(), 1)), r(std::max<size_t>(b.size(), 1));
+  size_t lq = 0, lr = 0;
+  gpu::check(fpx_divmod(gpu::context(), M::mod, gpu::limbs(a), a.size(), gpu::limbs(b), b.size(), gpu::limbs(q), &lq,
+                        gpu::limbs(r), &lr, FPX_REPR_MONTGOMERY),
+             "poly::divmod");
+  q.resize(lq);
+  r.resize(lr);
+  return {std::move(q), std::move(r)};
+}
+template <class M>
+vec<M> div(const vec<M>& a, const vec<M>& b) { return divmod(a, b).first; }
+template <class M>
+vec<M> mod(const vec<M>& a, const vec<M>& b) { return divmod(a, b).second; }
+
+// ---- O(n) host helpers (basic.hpp, calculus.hpp); not on the transform path.
+template <class M>
+vec<M> add(const vec<M>& a, const vec<M>& b) {
+  vec<M> r = a.size() >= b.size() ? a : b;
+  const vec<M>& s = a.size() >= b.size() ? b : a;
+  for (size_t i = 0; i < s.size(); ++i) r[i] += s[i];
+  return r;
+}
+template <class M>
+vec<M> sub(const vec<M>& a, const vec<M>& b) {
+  vec<M> r = a;
+  if (r.size() < b.size()) r.resize(b.size());
+  for (size_t i = 0; i < b.size(); ++i) r[i] -= b[i];
+  return r;
+}
+template <class M>
+vec<M> neg(vec<M> a) {
+  for (auto& x : a) x = -x;
+  return a;
+}
+template <class M>
+vec<M> mul_scalar(const vec<M>& a, M c) {
+  vec<M> r(a.size());
+  for (size_t i = 0; i < a.size(); ++i) r[i] = a[i] * c;
+  return r;
+}
+template <class M>
+vec<M> shift(const vec<M>& a, size_t k, size_t n = SIZE_MAX) {
+  vec<M> r(std::min(a.size() + k, n), M());
+  for (size_t i = 0; i < a.size() && i + k < r.size(); ++i) r[i + k] = a[i];
+  return r;
+}
+template <class M>
+M eval(const vec<M>& a, M x) {
+  M r;
+  for (size_t i = a.size(); i-- > 0;) r = r * x + a[i];
+  return r;
+}
+template <class M>
+vec<M> derivative(const vec<M>& a) {
+  if (a.size() <= 1) return {};
+  vec<M> r(a.size() - 1);
+  for (size_t i = 1; i < a.size(); ++i) r[i - 1] = a[i] * M::from_int(i);
+  return r;
+}
+template <class M>
+vec<M> inv_series(size_t n) {
+  if (n >= M::mod) throw domain_error("poly::inv_series: length must be < mod");
+  vec<M> r(n + 1, M());
+  if (n == 0) return r;
+  r[1] = M::from_int(1);
+  for (size_t i = 2; i <= n; ++i) r[i] = -(M::from_int(M::mod / i) * r[M::mod % i]);
+  return r;
+}
+template <class M>
+vec<M> integral(const vec<M>& a) {
+  if (a.empty()) return {};
+  const vec<M> iv = inv_series<M>(a.size());
+  vec<M> r(a.size() + 1);
+  for (size_t i = 0; i < a.size(); ++i) r[i + 1] = a[i] * iv[i + 1];
+  return r;
+}
+
+}  // namespace poly
+
+// ------------------------------------------------------------------ Poly
+
+template <class M>
+class Poly : public std::vector<M> {
+ public:
+  using base = std::vector<M>;
+  using value_type = M;
+  Poly() = default;
+  Poly(const base& v) : base(v) {}
+  Poly(base&& v) : base(std::move(v)) {}
+  Poly(std::initializer_list<M> il) : base(il) {}
+  explicit Poly(size_t n, M v = M()) : base(n, v) {}
+  using base::size;
+  using base::operator[];
+
+  size_t degree() const { return this->empty() ? 0 : this->size() - 1; }
+  bool is_zero() const {
+    for (const auto& x : *this)
+      if (!x.is_zero()) return false;
+    return true;
+  }
+  Poly& trim() { poly::trim(*this); return *this; }
+  Poly& resize_(size_t n) { this->resize(n); return *this; }
+  Poly operator+(const base& b) const { return poly::add<M>(*this, b); }
+  Poly operator-(const base& b) const { return poly::sub<M>(*this, b); }
+  Poly operator-() const { return poly::neg<M>(*this); }
+  Poly operator*(const base& b) const { return poly::conv<M>(*this, b); }
+  Poly operator*(M c) const { return poly::mul_scalar<M>(*this, c); }
+  Poly operator<<(size_t k) const { return poly::shift<M>(*this, k); }
+  Poly& operator+=(const base& b) { return *this = *this + b; }
+  Poly& operator-=(const base& b) { return *this = *this - b; }
+  Poly& operator*=(const base& b) { return *this = poly::conv<M>(*this, b); }
+  Poly& operator*=(M c) { return *this = *this * c; }
+  Poly mul(const base& b, size_t n) const { return poly::conv<M>(*this, b, n); }
+  Poly derivative() const { return poly::derivative<M>(*this); }
+  Poly integral() const { return poly::integral<M>(*this); }
+  Poly inv(size_t n) const { return poly::inv<M>(*this, n); }
+  Poly log(size_t n) const { return poly::log<M>(*this, n); }
+  Poly exp(size_t n) const { return poly::exp<M>(*this, n); }
+  Poly sqrt(size_t n) const { return poly::sqrt<M>(*this, n); }
+  Poly pow(uint64_t k, size_t n) const { return poly::pow<M>(*this, k, n); }
+  std::pair<Poly, Poly> divmod(const base& b) const {
+    auto r = poly::divmod<M>(*this, b);
+    return {Poly(std::move(r.first)), Poly(std::move(r.second))};
+  }
+  Poly div(const base& b) const { return poly::div<M>(*this, b); }
+  Poly mod(const base& b) const { return poly::mod<M>(*this, b); }
+  M eval(M x) const { return poly::eval<M>(*this, x); }
+  std::vector<uint32_t> to_ints() const {
+    std::vector<uint32_t> r(this->size());
+    for (size_t i = 0; i < this->size(); ++i) r[i] = (*this)[i].val();
+    return r;
+  }
+  static Poly from_ints(const std::vector<uint32_t>& v) {
+    Poly r(v.size());
+    for (size_t i = 0; i < v.size(); ++i) r[i] = M::from_int(v[i]);
+    return r;
+  }
+};
+
+inline const char* simd_backend() { return "cuda-sm_100a"; }
+
+}  // namespace fpx
+
+#endif  // FPX_DROPIN_FASTPOLY_HPP

@@ -1,0 +1,124 @@
+// Drop-in check: reference-style code compiled against include/fpx/fastpoly.hpp
+// runs on the GPU library and satisfies the reference's own contracts
+// (tests/test_prime_poly.cpp:315-362, tests/test_poly.cpp:160-345), checked
+// against O(n^2) definitions written here.
+#include <cstdio>
+#include <cstdlib>
+#include <random>
+#include <vector>
+
+#include "fpx/fastpoly.hpp"
+
+using namespace fpx;
+
+static int failures = 0;
+#define CHECK(c)                                                       \
+  do {                                                                 \
+    if (!(c)) {                                                        \
+      std::printf("FAIL %s:%d: %s\n", __FILE__, __LINE__, #c);         \
+      ++failures;                                                      \
+    }                                                                  \
+  } while (0)
+
+template <class M>
+std::vector<M> naive(const std::vector<M>& a, const std::vector<M>& b, size_t n) {
+  if (a.empty() || b.empty() || n == 0) return {};
+  std::vector<M> r(std::min(n, a.size() + b.size() - 1));
+  for (size_t i = 0; i < a.size(); ++i)
+    for (size_t j = 0; j < b.size() && i + j < r.size(); ++j) r[i + j] += a[i] * b[j];
+  return r;
+}
+
+template <class M>
+std::vector<M> rnd(size_t n, std::mt19937_64& g) {
+  std::vector<M> a(n);
+  for (auto& x : a) x = M::from_int(g() % M::mod);
+  return a;
+}
+
+template <class M>
+void suite(const char* name) {
+  std::mt19937_64 g(7);
+  for (size_t la : {size_t(1), size_t(39), size_t(41), size_t(300), size_t(5000)}) {
+    auto a = rnd<M>(la, g), b = rnd<M>(la + 13, g);
+    CHECK(poly::conv(a, b) == naive(a, b, SIZE_MAX));
+    CHECK(poly::conv(a, b, la) == naive(a, b, la));
+  }
+  for (size_t n : {size_t(1), size_t(33), size_t(257), size_t(3000)}) {
+    auto a = rnd<M>(n, g);
+    a[0] = M::from_int(1);
+    auto ia = poly::inv(a, n);
+    auto unit = naive(a, ia, n);
+    CHECK(unit[0] == M::from_int(1));
+    bool zero = true;
+    for (size_t i = 1; i < n; ++i) zero = zero && unit[i].is_zero();
+    CHECK(zero);
+    if (n <= M::mod) {
+      auto l = poly::log(a, n);
+      CHECK(poly::exp(l, n) == a);
+    }
+    auto sq = naive(a, a, n);
+    auto r = poly::sqrt(sq, n);
+    CHECK(naive(r, r, n) == sq);
+    auto p3 = poly::pow(a, 3, n);
+    CHECK(p3 == naive(naive(a, a, n), a, n));
+  }
+  // divmod round trip (tests/test_poly.cpp:316-344)
+  auto bdiv = rnd<M>(143, g);
+  bdiv.back() = M::from_int(1);
+  auto q0 = rnd<M>(177, g);
+  q0.back() = M::from_int(1);
+  auto rem = rnd<M>(141, g);
+  poly::trim(rem);
+  auto prod = naive(bdiv, q0, SIZE_MAX);
+  auto dividend = poly::add(prod, rem);
+  auto [q, r] = poly::divmod(dividend, bdiv);
+  CHECK(q == q0);
+  CHECK(r == rem);
+  // errors
+  bool threw = false;
+  try { (void)poly::inv(std::vector<M>{M(), M::from_int(1)}, 8); } catch (const poly::domain_error&) { threw = true; }
+  CHECK(threw);
+  std::printf("  %s ok\n", name);
+}
+
+int main() {
+  suite<mod998244353>("998244353");
+  suite<mod1000000007>("1000000007");
+  suite<ModInt<2147483647u>>("2147483647");
+  {  // tests/test_prime_poly.cpp:346-360 (Poly method API)
+    using M = mod1000000007;
+    const Poly<M> a{1, 2, 3}, b{1, 1};
+    CHECK(((a + b) - b) == a);
+    CHECK((a * (-M(1))) == -a);
+    CHECK((a << 2)[2] == a[0]);
+    CHECK(a.eval(M(2)) == M(17));
+    CHECK(a.integral().derivative() == a);
+    CHECK(a.inv(257).size() == 257u);
+    auto padded = a;
+    padded.resize(257);
+    CHECK(a.log(257).exp(257) == padded);
+    const auto square = a.mul(a, 257);
+    CHECK(square.sqrt(257).mul(square.sqrt(257), 257) == a.pow(2, 257));
+    CHECK((a * b).div(b) == a);
+    CHECK((a * b).mod(b).empty());
+  }
+  {  // GPU NttPlan keeps the reference's permutation: constant -> impulse at 0 (test_ntt.cpp:223-235)
+    using M = mod998244353;
+    const uint32_t n = 64;
+    auto plan = NttPlan<M>::get(n);
+    std::vector<uint32_t> a(n, M::from_int(5).raw_val());
+    plan->forward(a.data());
+    int nonzero = 0;
+    for (auto x : a) nonzero += x != 0;
+    CHECK(nonzero == 1);
+    CHECK(a[0] == M::from_int(5ull * n).raw_val());
+    plan->inverse(a.data());
+    CHECK(a[7] == M::from_int(5).raw_val());
+    bool threw = false;
+    try { (void)NttPlan<M>::get(1u << 24); } catch (const ntt_size_error&) { threw = true; }
+    CHECK(threw);
+  }
+  std::printf(failures ? "FAILED (%d)\n" : "all drop-in checks passed\n", failures);
+  return failures ? 1 : 0;
+}
