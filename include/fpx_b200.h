@@ -118,6 +118,26 @@ int fpx_div(fpx_ctx* ctx, uint32_t p, const uint32_t* a, size_t la, const uint32
 int fpx_mod(fpx_ctx* ctx, uint32_t p, const uint32_t* a, size_t la, const uint32_t* b, size_t lb, uint32_t* r,
             size_t* r_len, int repr);
 
+/* ---- allocation-free convolution (no counterpart in the reference) ------------
+ * For callers that cannot allocate device memory when they need a product: code
+ * whose device memory is owned by a host framework's allocator (often reserved
+ * in full at start-up), or latency-critical loops that cannot take cudaMalloc's
+ * implicit device synchronisation.  Same result and same output length as
+ * fpx_conv_device, but no context is needed and nothing is allocated: the
+ * transform buffers and twiddle tables live in one static device array sized
+ * for transforms of up to 2^20 points (about 8.3 MiB, held by every GPU that
+ * loads the library until the process exits).  Device pointers, canonical
+ * residues, work queued on `stream` (a cudaStream_t, NULL = legacy default).
+ * Limits: p an odd NTT prime below 2^30 (FPX_EINVAL otherwise); the padded
+ * product length next_pow2(min(la,n) + min(lb,n) - 1) at most 2^20 and
+ * 2^v2(p-1), unless the shorter operand has <= 40 terms (FPX_ESIZE otherwise).
+ * The first call on a device looks the array up (cudaGetSymbolAddress) and
+ * should come before any stream capture.  All calls share the array and keep
+ * its last contents; calls that overlap on the GPU race and must be serialised
+ * by the caller. */
+int fpx_conv_noalloc(uint32_t p, const uint32_t* d_a, size_t la, const uint32_t* d_b, size_t lb, size_t n,
+                     uint32_t* d_out, size_t* out_len, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
