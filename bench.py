@@ -123,6 +123,25 @@ class ClockSampler:
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def max_over_ranks(dist, values, device="cpu"):
+    """Element-wise max of per-rank timings (every rank gets the result)."""
+    if not dist:
+        return list(values)
+    import torch
+    t = torch.tensor(values, dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(v) for v in t.cpu()]
+
+
+def whole_job_rates(world: int, steps: int, total_ms: float, e2e_steps: int, e2e_s: float):
+    """(ms per step, whole-job Mcoeff/s device-resident, whole-job Mcoeff/s end to end):
+    every rank converts its own inputs each step (replicas), timed by the slowest rank."""
+    ms_per_step = total_ms / steps
+    value = world * N_OUT / (ms_per_step * 1e-3) / 1e6
+    e2e_value = world * N_OUT * e2e_steps / e2e_s / 1e6
+    return ms_per_step, value, e2e_value
+
+
 def cpu_reference_sample(reps: int, threads: int | None = None):
     """The reference's conv on this host's cores: `threads` concurrent calls per rep."""
     from oracle.oracle import Reference, OP_CONV, Oracle
@@ -252,14 +271,8 @@ def run_fpx(args):
     clk = clocks.stop()
     assert int(po[0]) == want0
 
-    if dist:
-        t = torch.tensor([total_ms, e2e_s], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms, e2e_s = float(t[0]), float(t[1])
-
-    ms_per_step = total_ms / args.steps
-    value = world * N_OUT / (ms_per_step * 1e-3) / 1e6
-    e2e_value = world * N_OUT * e2e_steps / e2e_s / 1e6
+    total_ms, e2e_s = max_over_ranks(dist, [total_ms, e2e_s], device="cuda")
+    ms_per_step, value, e2e_value = whole_job_rates(world, args.steps, total_ms, e2e_steps, e2e_s)
 
     # roofline of the dominant kernel
     peak, peak_kind = measured_peak_hbm()

@@ -370,6 +370,10 @@ namespace fpx {
 
 int small_kernel_max_log() { return kSmallLog; }
 
+cudaError_t kernels_fast_init();
+cudaError_t launch_rows_generic(const PrimeTables& pt, const BigTables& bt, uint32_t* x, const uint32_t* y, int ymode,
+                                uint32_t* y_spec_out, int forward, int inverse, cudaStream_t s);
+
 // Opt-in shared-memory limits; per device, called once per context.
 cudaError_t kernels_init() {
   cudaError_t e = cudaSuccess;
@@ -381,7 +385,8 @@ cudaError_t kernels_init() {
   set((const void*)k_colfwd, padded_words(1 << 14) * 4);
   set((const void*)k_rows, 2 * padded_words(1 << 13) * 4);
   set((const void*)k_colinv, padded_words(1 << 14) * 4);
-  return e;
+  const cudaError_t r = kernels_fast_init();
+  return e != cudaSuccess ? e : r;
 }
 
 cudaError_t launch_small(const PrimeTables& pt, int logN, const SmallJob& job, cudaStream_t s) {
@@ -422,8 +427,8 @@ static BigD big_dev(const BigTables& bt, const Tw2* lo, const Tw2* hi) {
 
 static int col_tile_words(const BigD& d) { return (1 << d.logW) << d.logR; }
 
-cudaError_t launch_colfwd(const PrimeTables& pt, const BigTables& bt, int nops, const InOp* in, uint32_t* const* out,
-                          cudaStream_t s) {
+cudaError_t launch_colfwd_generic(const PrimeTables& pt, const BigTables& bt, int nops, const InOp* in,
+                                  uint32_t* const* out, cudaStream_t s) {
   ColOps ops{};
   for (int i = 0; i < nops; ++i) {
     ops.in[i] = dev_in(in[i]);
@@ -436,8 +441,8 @@ cudaError_t launch_colfwd(const PrimeTables& pt, const BigTables& bt, int nops, 
   return cudaGetLastError();
 }
 
-cudaError_t launch_rows(const PrimeTables& pt, const BigTables& bt, uint32_t* x, const uint32_t* y, int ymode,
-                        uint32_t* y_spec_out, int forward, int inverse, cudaStream_t s) {
+cudaError_t launch_rows_generic(const PrimeTables& pt, const BigTables& bt, uint32_t* x, const uint32_t* y, int ymode,
+                                uint32_t* y_spec_out, int forward, int inverse, cudaStream_t s) {
   const int C = 1 << bt.logC;
   const size_t smem = (size_t)2 * padded_words(C) * 4;
   const int nt = C / 16 > 512 ? 512 : C / 16;
@@ -445,8 +450,8 @@ cudaError_t launch_rows(const PrimeTables& pt, const BigTables& bt, uint32_t* x,
   return cudaGetLastError();
 }
 
-cudaError_t launch_colinv(const PrimeTables& pt, const BigTables& bt, const uint32_t* in, int mont_scaled,
-                          const Epi& epi, cudaStream_t s) {
+cudaError_t launch_colinv_generic(const PrimeTables& pt, const BigTables& bt, const uint32_t* in, int mont_scaled,
+                                  const Epi& epi, cudaStream_t s) {
   const BigD d = big_dev(bt, mont_scaled ? bt.lo_inv_r : bt.lo_inv, bt.hi_inv);
   const size_t smem = (size_t)padded_words(col_tile_words(d)) * 4;
   k_colinv<<<1u << (d.logC - d.logW), 256, smem, s>>>(in, d, dev_tab(pt), dev_epi(epi));
@@ -669,6 +674,409 @@ cudaError_t launch_mul_mont_tab(uint32_t p, const uint32_t* a, const uint32_t* t
                                 cudaStream_t s) {
   if (n == 0) return cudaSuccess;
   k_mul_mont_tab<<<grid_for(n, 256), 256, 0, s>>>(make_fp(p), a, tab, out, n);
+  return cudaGetLastError();
+}
+
+}  // namespace fpx
+
+// ===========================================================================
+// Specialised two-pass kernels (ntt_fast.cuh): the row pass for C = 2^12 and
+// the column passes for every R = 2^2 .. 2^12.
+// ===========================================================================
+#include "ntt_fast.cuh"
+
+namespace {
+
+// Row pass, C = 4096.  Modes as k_rows: forward (DIF of x, and of y when
+// ymode == 1), pointwise product (ymode 1 raw y, 2 y spectrum, 3 square),
+// inverse (DIT).  The forward's last group, the product and the inverse's first
+// group all act on the same 16 positions per thread, in registers.
+__global__ void __launch_bounds__(256, 3) k_rows12(uint32_t* __restrict__ x, const uint32_t* __restrict__ y,
+                                                  int ymode, uint32_t* __restrict__ y_spec_out, int forward,
+                                                  int inverse, Ptab pt) {
+  __shared__ uint32_t sX[4096];
+  __shared__ uint32_t sY[4096];
+  const int t = threadIdx.x;
+  const size_t row = (size_t)blockIdx.x << 12;
+  const Fp f = pt.f;
+  uint32_t v[2][16];
+  if (forward) {
+    if (ymode == 1) {
+#pragma unroll
+      for (int i = 0; i < 16; ++i) {
+        v[0][i] = x[row + posA(t, i)];
+        v[1][i] = __ldg(y + row + posA(t, i));
+      }
+      bf_group<4, 12, false, 2>(v, pt.fwd, t, f);
+#pragma unroll
+      for (int i = 0; i < 16; ++i) {
+        sX[swz12(posA(t, i))] = v[0][i];
+        sY[swz12(posA(t, i))] = v[1][i];
+      }
+      __syncthreads();
+#pragma unroll
+      for (int i = 0; i < 16; ++i) {
+        v[0][i] = sX[swz12(posB(t, i))];
+        v[1][i] = sY[swz12(posB(t, i))];
+      }
+      bf_group<4, 8, false, 2>(v, pt.fwd, t & 15, f);
+#pragma unroll
+      for (int i = 0; i < 16; ++i) {
+        sX[swz12(posB(t, i))] = v[0][i];
+        sY[swz12(posB(t, i))] = v[1][i];
+      }
+      __syncthreads();
+#pragma unroll
+      for (int i = 0; i < 16; ++i) {
+        v[0][i] = sX[swz12(posC(t, i))];
+        v[1][i] = sY[swz12(posC(t, i))];
+      }
+      bf_group<4, 4, false, 2>(v, pt.fwd, 0, f);
+      if (y_spec_out) {
+        uint4* o = reinterpret_cast<uint4*>(y_spec_out + row + posC(t, 0));
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+          o[q] = make_uint4(red(v[1][4 * q], f.p), red(v[1][4 * q + 1], f.p), red(v[1][4 * q + 2], f.p),
+                            red(v[1][4 * q + 3], f.p));
+      }
+    } else {
+#pragma unroll
+      for (int i = 0; i < 16; ++i) v[0][i] = x[row + posA(t, i)];
+      bf_group<4, 12, false, 1>(v, pt.fwd, t, f);
+#pragma unroll
+      for (int i = 0; i < 16; ++i) sX[swz12(posA(t, i))] = v[0][i];
+      __syncthreads();
+#pragma unroll
+      for (int i = 0; i < 16; ++i) v[0][i] = sX[swz12(posB(t, i))];
+      bf_group<4, 8, false, 1>(v, pt.fwd, t & 15, f);
+#pragma unroll
+      for (int i = 0; i < 16; ++i) sX[swz12(posB(t, i))] = v[0][i];
+      __syncthreads();
+#pragma unroll
+      for (int i = 0; i < 16; ++i) v[0][i] = sX[swz12(posC(t, i))];
+      bf_group<4, 4, false, 1>(v, pt.fwd, 0, f);
+    }
+  } else {
+    const uint4* in = reinterpret_cast<const uint4*>(x + row + posC(t, 0));
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const uint4 u = in[q];
+      v[0][4 * q] = u.x; v[0][4 * q + 1] = u.y; v[0][4 * q + 2] = u.z; v[0][4 * q + 3] = u.w;
+    }
+  }
+  if (ymode == 1) {
+#pragma unroll
+    for (int i = 0; i < 16; ++i) v[0][i] = mont(v[0][i], v[1][i], f);
+  } else if (ymode == 2) {
+    const uint4* ys = reinterpret_cast<const uint4*>(y + row + posC(t, 0));
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const uint4 u = __ldg(ys + q);
+      v[0][4 * q] = mont(v[0][4 * q], u.x, f);
+      v[0][4 * q + 1] = mont(v[0][4 * q + 1], u.y, f);
+      v[0][4 * q + 2] = mont(v[0][4 * q + 2], u.z, f);
+      v[0][4 * q + 3] = mont(v[0][4 * q + 3], u.w, f);
+    }
+  } else if (ymode == 3) {
+#pragma unroll
+    for (int i = 0; i < 16; ++i) v[0][i] = mont(v[0][i], v[0][i], f);
+  }
+  if (!inverse) {
+    uint4* o = reinterpret_cast<uint4*>(x + row + posC(t, 0));
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+      o[q] = make_uint4(red(v[0][4 * q], f.p), red(v[0][4 * q + 1], f.p), red(v[0][4 * q + 2], f.p),
+                        red(v[0][4 * q + 3], f.p));
+    return;
+  }
+  bf_group<4, 4, true, 1>(v, pt.inv, 0, f);
+#pragma unroll
+  for (int i = 0; i < 16; ++i) sX[swz12(posC(t, i))] = v[0][i];
+  __syncthreads();
+#pragma unroll
+  for (int i = 0; i < 16; ++i) v[0][i] = sX[swz12(posB(t, i))];
+  bf_group<4, 8, true, 1>(v, pt.inv, t & 15, f);
+#pragma unroll
+  for (int i = 0; i < 16; ++i) sX[swz12(posB(t, i))] = v[0][i];
+  __syncthreads();
+#pragma unroll
+  for (int i = 0; i < 16; ++i) v[0][i] = sX[swz12(posA(t, i))];
+  bf_group<4, 12, true, 1>(v, pt.inv, t, f);
+#pragma unroll
+  for (int i = 0; i < 16; ++i) x[row + posA(t, i)] = v[0][i];
+}
+
+template <int LOGR>
+struct ColCfg {
+  static constexpr int LOGW = LOGR >= 11 ? 14 - LOGR : 13 - LOGR;
+  static constexpr int W = 1 << LOGW;
+  static constexpr int TE = 1 << (LOGR + LOGW);
+  static constexpr int K = ColGroups<LOGR>::K;
+  static constexpr int GL = ColGroups<LOGR>::size(K - 1);
+};
+
+// Loads the W x R column tile (rows t, columns j0..j0+W) into shared memory
+// with cp.async: all copies in flight at once, no register staging, zero
+// beyond `count`.  16-byte copies when the source is 16-byte aligned.
+template <int LOGR>
+__device__ __forceinline__ void col_tile_load(uint32_t* sm, const uint32_t* src, uint32_t count, int j0, int logC,
+                                              int tid) {
+  using C = ColCfg<LOGR>;
+  if (src == nullptr || count == 0) {
+    for (int e = tid; e < C::TE; e += 256) sm[e] = 0u;
+    return;
+  }
+  if (((uintptr_t)src & 15u) == 0) {
+    constexpr int CPR = C::W / 4;  // 16-byte chunks per row segment
+#pragma unroll 4
+    for (int q = tid; q < C::TE / 4; q += 256) {
+      const int t = q / CPR, cc = (q % CPR) * 4;
+      const uint32_t gi = ((uint32_t)t << logC) + j0 + cc;
+      const int valid = gi < count ? (int)min(4u, count - gi) : 0;
+      cp_async16(sm + swz_col<LOGR, C::LOGW, C::GL>((t << C::LOGW) + cc), src + (valid ? gi : 0), valid * 4);
+    }
+  } else {
+#pragma unroll 4
+    for (int e = tid; e < C::TE; e += 256) {
+      const int t = e >> C::LOGW, c = e & (C::W - 1);
+      const uint32_t gi = ((uint32_t)t << logC) + j0 + c;
+      const bool v = gi < count;
+      cp_async4(sm + swz_col<LOGR, C::LOGW, C::GL>(e), src + (v ? gi : 0), v ? 4 : 0);
+    }
+  }
+  cp_async_wait_all();
+}
+
+// One group over the tile, shared -> registers -> shared.  REDUCE: inputs may be
+// any 32-bit value (CRT lift), reduce them on the way in (first forward group).
+template <int LOGR, int KG, bool INV, bool REDUCE>
+__device__ __forceinline__ void col_group_smem(uint32_t* sm, const uint2* tw, const Fp& f, uint32_t q1, int tid) {
+  using C = ColCfg<LOGR>;
+  constexpr int G = ColGroups<LOGR>::size(KG);
+  constexpr int T = ColGroups<LOGR>::top(KG);
+  constexpr int S = T - G;
+  constexpr int NINST = C::TE >> G;
+#pragma unroll 1
+  for (int inst = tid; inst < NINST; inst += 256) {
+    const int c = inst & (C::W - 1);
+    const int rest = inst >> C::LOGW;
+    const int base = rest & ((1 << S) - 1);
+    const int p0 = ((rest >> S) << T) + base;
+    uint32_t v[2][1 << G];
+#pragma unroll
+    for (int i = 0; i < (1 << G); ++i) {
+      const uint32_t x = sm[swz_col<LOGR, C::LOGW, C::GL>(((p0 + (i << S)) << C::LOGW) + c)];
+      v[0][i] = REDUCE ? reduce_any(x, q1, f) : x;
+    }
+    bf_group<G, T, INV, 1>(v, tw, base, f);
+#pragma unroll
+    for (int i = 0; i < (1 << G); ++i) sm[swz_col<LOGR, C::LOGW, C::GL>(((p0 + (i << S)) << C::LOGW) + c)] = v[0][i];
+  }
+}
+
+// Forward groups 0 .. K-2 (the last group is the caller's).
+template <int LOGR, int KG>
+__device__ __forceinline__ void col_fwd_groups(uint32_t* sm, const Ptab& pt, bool reduce, int tid) {
+  if constexpr (KG < ColGroups<LOGR>::K - 1) {
+    if (KG == 0 && reduce) col_group_smem<LOGR, KG, false, true>(sm, pt.fwd, pt.f, pt.q1, tid);
+    else col_group_smem<LOGR, KG, false, false>(sm, pt.fwd, pt.f, pt.q1, tid);
+    __syncthreads();
+    col_fwd_groups<LOGR, KG + 1>(sm, pt, reduce, tid);
+  }
+}
+
+// Inverse groups K-2 .. 1 (the first, smallest group and the last, group 0, are the caller's).
+template <int LOGR, int KG>
+__device__ __forceinline__ void col_inv_groups(uint32_t* sm, const Ptab& pt, int tid) {
+  if constexpr (KG >= 1) {
+    col_group_smem<LOGR, KG, true, false>(sm, pt.inv, pt.f, pt.q1, tid);
+    __syncthreads();
+    col_inv_groups<LOGR, KG - 1>(sm, pt, tid);
+  }
+}
+
+template <int LOGR>
+__global__ void __launch_bounds__(256, 3) k_colfwd_t(ColOps ops, BigD bt, Ptab pt) {
+  using C = ColCfg<LOGR>;
+  constexpr int K = ColGroups<LOGR>::K;
+  constexpr int G = C::GL;
+  extern __shared__ uint32_t sm[];
+  const int tid = threadIdx.x, logC = bt.logC;
+  const int j0 = blockIdx.x << C::LOGW;
+  const InD in = blockIdx.y == 0 ? ops.in[0] : (blockIdx.y == 1 ? ops.in[1] : ops.in[2]);
+  uint32_t* out = blockIdx.y == 0 ? ops.out[0] : (blockIdx.y == 1 ? ops.out[1] : ops.out[2]);
+  const Fp f = pt.f;
+  col_tile_load<LOGR>(sm, in.ptr, in.count, j0, logC, tid);
+  __syncthreads();
+  col_fwd_groups<LOGR, 0>(sm, pt, in.reduce != 0, tid);
+  // last group: shared -> registers -> Bailey twiddle -> global
+  constexpr int NINST = C::TE >> G;
+  const bool reduce_here = K == 1 && in.reduce;
+#pragma unroll 1
+  for (int inst = tid; inst < NINST; inst += 256) {
+    const int c = inst & (C::W - 1);
+    const int b = inst >> C::LOGW;
+    const int p0 = b << G;
+    uint32_t v[2][1 << G];
+#pragma unroll
+    for (int i = 0; i < (1 << G); ++i) {
+      const uint32_t x = sm[swz_col<LOGR, C::LOGW, C::GL>(((p0 + i) << C::LOGW) + c)];
+      v[0][i] = reduce_here ? reduce_any(x, pt.q1, f) : x;
+    }
+    bf_group<G, G, false, 1>(v, pt.fwd, 0, f);
+    const uint32_t j = j0 + c;
+    const uint32_t eb = j * brev_c(b, LOGR - G);
+    const uint32_t js = j << (LOGR - G);
+#pragma unroll
+    for (int i = 0; i < (1 << G); ++i) {
+      const uint32_t ex = eb + js * brev_c(i, G);
+      uint32_t w = shoup(v[0][i], __ldg(bt.lo + (ex & 4095u)), f.p);
+      out[((p0 + i) << logC) + j] = shoup(w, __ldg(bt.hi + (ex >> 12)), f.p);
+    }
+  }
+}
+
+template <int LOGR>
+__global__ void __launch_bounds__(256, 3) k_colinv_t(const uint32_t* __restrict__ in, BigD bt, Ptab pt, EpiD epi) {
+  using C = ColCfg<LOGR>;
+  constexpr int K = ColGroups<LOGR>::K;
+  extern __shared__ uint32_t sm[];
+  const int tid = threadIdx.x, logC = bt.logC;
+  const int j0 = blockIdx.x << C::LOGW;
+  const Fp f = pt.f;
+  col_tile_load<LOGR>(sm, in, 0xffffffffu, j0, logC, tid);
+  __syncthreads();
+  // first: the smallest blocks (Bailey twiddle on the way in), in place
+  {
+    constexpr int G = C::GL;
+    constexpr int NINST = C::TE >> G;
+#pragma unroll 1
+    for (int inst = tid; inst < NINST; inst += 256) {
+      const int c = inst & (C::W - 1);
+      const int b = inst >> C::LOGW;
+      const int p0 = b << G;
+      const uint32_t j = j0 + c;
+      const uint32_t eb = j * brev_c(b, LOGR - G);
+      const uint32_t js = j << (LOGR - G);
+      uint32_t v[2][1 << G];
+#pragma unroll
+      for (int i = 0; i < (1 << G); ++i) {
+        const uint32_t ex = eb + js * brev_c(i, G);
+        uint32_t w = shoup(sm[swz_col<LOGR, C::LOGW, C::GL>(((p0 + i) << C::LOGW) + c)], __ldg(bt.lo + (ex & 4095u)), f.p);
+        v[0][i] = shoup(w, __ldg(bt.hi + (ex >> 12)), f.p);
+      }
+      bf_group<G, G, true, 1>(v, pt.inv, 0, f);
+      if constexpr (K == 1) {
+#pragma unroll
+        for (int i = 0; i < (1 << G); ++i) epi_store(epi, (uint32_t)(((p0 + i) << logC) + j), v[0][i], f);
+      } else {
+#pragma unroll
+        for (int i = 0; i < (1 << G); ++i) sm[swz_col<LOGR, C::LOGW, C::GL>(((p0 + i) << C::LOGW) + c)] = v[0][i];
+      }
+    }
+  }
+  if constexpr (K > 1) {
+    __syncthreads();
+    col_inv_groups<LOGR, K - 2>(sm, pt, tid);
+    // last: the full column blocks, shared -> registers -> epilogue (global)
+    constexpr int G = ColGroups<LOGR>::size(0);
+    constexpr int S = LOGR - G;
+    constexpr int NINST = C::TE >> G;
+#pragma unroll 1
+    for (int inst = tid; inst < NINST; inst += 256) {
+      const int c = inst & (C::W - 1);
+      const int base = inst >> C::LOGW;
+      uint32_t v[2][1 << G];
+#pragma unroll
+      for (int i = 0; i < (1 << G); ++i) v[0][i] = sm[swz_col<LOGR, C::LOGW, C::GL>(((base + (i << S)) << C::LOGW) + c)];
+      bf_group<G, LOGR, true, 1>(v, pt.inv, base, f);
+#pragma unroll
+      for (int i = 0; i < (1 << G); ++i) epi_store(epi, (uint32_t)(((base + (i << S)) << logC) + j0 + c), v[0][i], f);
+    }
+  }
+}
+
+template <int LOGR>
+int col_smem_bytes() { return ColCfg<LOGR>::TE * 4; }
+
+using ColFwdFn = void (*)(ColOps, BigD, Ptab);
+using ColInvFn = void (*)(const uint32_t*, BigD, Ptab, EpiD);
+
+template <int... L>
+struct ColTable {
+  static ColFwdFn fwd(int logR) {
+    ColFwdFn r = nullptr;
+    ((logR == L ? (r = k_colfwd_t<L>, 0) : 0), ...);
+    return r;
+  }
+  static ColInvFn inv(int logR) {
+    ColInvFn r = nullptr;
+    ((logR == L ? (r = k_colinv_t<L>, 0) : 0), ...);
+    return r;
+  }
+  static int words(int logR) {
+    int r = 0;
+    ((logR == L ? (r = ColCfg<L>::TE, 0) : 0), ...);
+    return r;
+  }
+  static int logw(int logR) {
+    int r = 0;
+    ((logR == L ? (r = ColCfg<L>::LOGW, 0) : 0), ...);
+    return r;
+  }
+  static cudaError_t init() {
+    cudaError_t e = cudaSuccess;
+    auto set = [&](const void* fn, int bytes) {
+      const cudaError_t r = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+      if (r != cudaSuccess) e = r;
+    };
+    (set((const void*)k_colfwd_t<L>, ColCfg<L>::TE * 4), ...);
+    (set((const void*)k_colinv_t<L>, ColCfg<L>::TE * 4), ...);
+    return e;
+  }
+};
+using Cols = ColTable<2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12>;
+
+}  // namespace
+
+namespace fpx {
+
+cudaError_t kernels_fast_init() { return Cols::init(); }
+
+
+
+
+cudaError_t launch_colfwd(const PrimeTables& pt, const BigTables& bt, int nops, const InOp* in,
+                               uint32_t* const* out, cudaStream_t s) {
+  ColOps ops{};
+  for (int i = 0; i < nops; ++i) {
+    ops.in[i] = dev_in(in[i]);
+    ops.out[i] = out[i];
+  }
+  BigD d{bt.logR, bt.logC, Cols::logw(bt.logR), reinterpret_cast<const uint2*>(bt.lo_fwd),
+         reinterpret_cast<const uint2*>(bt.hi_fwd)};
+  ColFwdFn fn = Cols::fwd(bt.logR);
+  if (!fn || d.logW > bt.logC) return cudaErrorInvalidValue;
+  dim3 grid(1u << (bt.logC - d.logW), (unsigned)nops);
+  fn<<<grid, 256, Cols::words(bt.logR) * 4, s>>>(ops, d, dev_tab(pt));
+  return cudaGetLastError();
+}
+
+cudaError_t launch_colinv(const PrimeTables& pt, const BigTables& bt, const uint32_t* in, int mont_scaled,
+                               const Epi& epi, cudaStream_t s) {
+  BigD d{bt.logR, bt.logC, Cols::logw(bt.logR),
+         reinterpret_cast<const uint2*>(mont_scaled ? bt.lo_inv_r : bt.lo_inv),
+         reinterpret_cast<const uint2*>(bt.hi_inv)};
+  ColInvFn fn = Cols::inv(bt.logR);
+  if (!fn || d.logW > bt.logC) return cudaErrorInvalidValue;
+  fn<<<1u << (bt.logC - d.logW), 256, Cols::words(bt.logR) * 4, s>>>(in, d, dev_tab(pt), dev_epi(epi));
+  return cudaGetLastError();
+}
+
+cudaError_t launch_rows(const PrimeTables& pt, const BigTables& bt, uint32_t* x, const uint32_t* y, int ymode,
+                             uint32_t* y_spec_out, int forward, int inverse, cudaStream_t s) {
+  if (bt.logC != 12) return launch_rows_generic(pt, bt, x, y, ymode, y_spec_out, forward, inverse, s);
+  k_rows12<<<1u << bt.logR, 256, 0, s>>>(x, y, ymode, y_spec_out, forward, inverse, dev_tab(pt));
   return cudaGetLastError();
 }
 

@@ -1,0 +1,116 @@
+// ntt_fast.cuh - specialised transform passes for the two-pass (N > 2^13) path.
+//
+// Same arithmetic and level order as ntt_core.cuh (radix-2 Gentleman-Sande DIF
+// forward, Cooley-Tukey DIT inverse, grouped four levels per register pass),
+// but every index is a compile-time function of the tile shape, the first
+// group reads global memory straight into registers (16 or 32 independent
+// loads in flight per thread) and the last group writes global memory straight
+// from registers, so a pass costs one shared-memory round trip per middle group
+// only.  Shared memory is XOR-swizzled so that every group's access pattern is
+// free of bank conflicts.
+#pragma once
+#include "field.cuh"
+
+namespace fpx_dev {
+
+// ---------------------------------------------------------------------------
+// Register butterfly groups.
+// x holds 2^G points p0 + i*s (s = 2^S) of a block of length 2^LL; base = p0
+// mod s.  Forward: levels len = 2^LL .. 2^(LL-G+1); inverse: the reverse.
+// Twiddle index for level l, pair j: (len/2) + base + j*s.
+// ---------------------------------------------------------------------------
+template <int G, int LL, bool INV, int NA>
+__device__ __forceinline__ void bf_group(uint32_t (&x)[2][1 << G], const uint2* __restrict__ tw, int base,
+                                         const Fp& f) {
+  constexpr int E = 1 << G;
+  constexpr int S = LL - G;
+  // all twiddles of the group up front: more loads in flight
+  uint2 w[E];  // w[hs + j] for level with pair distance hs (hs = 1, 2, 4, 8)
+#pragma unroll
+  for (int hs = 1; hs < E; hs <<= 1) {
+    // level with pair distance hs: len = 2^(S + log2(hs) + 1), half = 2^(S + log2 hs)
+#pragma unroll
+    for (int j = 0; j < hs; ++j) {
+      const int half = hs << S;
+      w[hs + j] = __ldg(&tw[half + base + (j << S)]);
+    }
+  }
+  if (!INV) {
+#pragma unroll
+    for (int hs = E / 2; hs >= 1; hs >>= 1) {
+#pragma unroll
+      for (int i = 0; i < E; ++i)
+        if (!(i & hs)) {
+#pragma unroll
+          for (int a = 0; a < NA; ++a) dif_bf(x[a][i], x[a][i + hs], w[hs + (i & (hs - 1))], f);
+        }
+    }
+  } else {
+#pragma unroll
+    for (int hs = 1; hs < E; hs <<= 1) {
+#pragma unroll
+      for (int i = 0; i < E; ++i)
+        if (!(i & hs)) {
+#pragma unroll
+          for (int a = 0; a < NA; ++a) dit_bf(x[a][i], x[a][i + hs], w[hs + (i & (hs - 1))], f);
+        }
+    }
+  }
+}
+
+__device__ __forceinline__ uint32_t brev_c(uint32_t t, int logn) { return logn ? (__brev(t) >> (32 - logn)) : 0u; }
+
+// ---------------------------------------------------------------------------
+// Row pass, C = 2^12, 256 threads, 16 points per thread per group.
+//   group A: len 4096..512, thread t holds t + 256 i
+//   group B: len 256..32,   thread t holds 256 (t>>4) + (t&15) + 16 i
+//   group C: len 16..2,     thread t holds 16 t + i
+// smem word for row position a: a ^ g(a >> 5), g(r) = (r & 15) | ((r >> 3 & 1) << 4)
+// (conflict-free for all three patterns).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ int swz12(int a) {
+  const int r = a >> 5;
+  return a ^ ((r & 15) | (((r >> 3) & 1) << 4));
+}
+__device__ __forceinline__ int posA(int t, int i) { return t + (i << 8); }
+__device__ __forceinline__ int posB(int t, int i) { return ((t >> 4) << 8) + (t & 15) + (i << 4); }
+__device__ __forceinline__ int posC(int t, int i) { return (t << 4) + i; }
+
+// Column pass tile: W = 2^LOGW adjacent columns x R = 2^LOGR rows, element
+// (row t, col c) at smem word a = t*W + c, swizzled for the last group's
+// pattern (instances one group-length apart): a ^ ((a >> (GL+LOGW)) & (32/W-1)) << LOGW.
+template <int LOGR, int LOGW, int GL>
+__device__ __forceinline__ int swz_col(int a) {
+  if constexpr (GL + LOGW >= 5 && LOGW < 5) {
+    return a ^ (((a >> (GL + LOGW)) & ((32 >> LOGW) - 1)) << LOGW);
+  } else {
+    return a;
+  }
+}
+
+// Asynchronous global -> shared copies (cp.async), zero-filling past src_bytes.
+__device__ __forceinline__ void cp_async16(uint32_t* smem, const uint32_t* gmem, int src_bytes) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gmem), "r"(src_bytes));
+}
+__device__ __forceinline__ void cp_async4(uint32_t* smem, const uint32_t* gmem, int src_bytes) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(s), "l"(gmem), "r"(src_bytes));
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
+}
+
+// Group sizes of an R = 2^LOGR point column transform, largest first.
+template <int LOGR>
+struct ColGroups {
+  static constexpr int K = (LOGR + 3) / 4;
+  __host__ __device__ static constexpr int size(int k) { return LOGR / K + (k < LOGR % K ? 1 : 0); }
+  __host__ __device__ static constexpr int top(int k) {  // log2 of the group's first block length
+    int t = LOGR;
+    for (int i = 0; i < k; ++i) t -= size(i);
+    return t;
+  }
+};
+
+}  // namespace fpx_dev
