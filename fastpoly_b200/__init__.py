@@ -91,8 +91,23 @@ def load_library(path: str = LIB_PATH):
     L.fpx_divmod.argtypes = [vp, u32, _u32p, sz, _u32p, sz, _u32p, _szp, _u32p, _szp, i32]
     L.fpx_div.argtypes = [vp, u32, _u32p, sz, _u32p, sz, _u32p, _szp, i32]
     L.fpx_mod.argtypes = [vp, u32, _u32p, sz, _u32p, sz, _u32p, _szp, i32]
+    L.fpx_batch_submit.argtypes = [vp, vp, sz]
+    L.fpx_batch_wait.argtypes = [vp]
+    L.fpx_batch_run.argtypes = [vp, vp, sz, i32]
     _lib = L
     return L
+
+
+OP_CONV, OP_INV, OP_LOG, OP_EXP, OP_SQRT, OP_POW, OP_DIVMOD = range(7)
+_OPS = {"conv": OP_CONV, "inv": OP_INV, "log": OP_LOG, "exp": OP_EXP, "sqrt": OP_SQRT, "pow": OP_POW,
+        "divmod": OP_DIVMOD}
+
+
+class Job(C.Structure):
+    """struct fpx_job (include/fpx_b200.h): one operation of a batch."""
+    _fields_ = [("op", C.c_int), ("p", C.c_uint32), ("a", C.c_void_p), ("la", C.c_size_t), ("b", C.c_void_p),
+                ("lb", C.c_size_t), ("k", C.c_uint64), ("n", C.c_size_t), ("out", C.c_void_p),
+                ("out2", C.c_void_p), ("out_len", C.c_size_t), ("out2_len", C.c_size_t), ("status", C.c_int)]
 
 
 class PoolStats(C.Structure):
@@ -288,9 +303,71 @@ class Context:
         return r[: lr.value]
 
 
+    # -- batches -------------------------------------------------------------------
+    def batch(self, jobs, repr: int = CANONICAL) -> list:
+        """Runs many operations in one call (fpx_batch_run, host buffers).
+
+        Each job is a tuple: ("conv", p, a, b[, n]), ("inv" | "log" | "exp" | "sqrt", p, a, n),
+        ("pow", p, a, k, n) or ("divmod", p, a, b).  Returns one entry per job: the
+        result array ((q, r) for divmod), or the exception the single-job call would
+        raise for that job (not raised).
+        """
+        arr = (Job * max(len(jobs), 1))()
+        keep, outs = [], []
+        for i, jb in enumerate(jobs):
+            op, p = _OPS[jb[0]], int(jb[1])
+            a = _arr(jb[2])
+            b = np.zeros(0, np.uint32)
+            k, n = 0, 0
+            if op == OP_CONV:
+                b = _arr(jb[3])
+                n = SIZE_MAX if len(jb) < 5 or jb[4] is None else int(jb[4])
+                cap = min(a.size, n) + min(b.size, n) - 1 if a.size and b.size and n else 0
+                o1, o2 = np.empty(max(min(cap, n), 1), np.uint32), None
+            elif op == OP_POW:
+                k, n = int(jb[3]), int(jb[4])
+                o1, o2 = np.empty(max(n, 1), np.uint32), None
+            elif op == OP_DIVMOD:
+                b = _arr(jb[3])
+                o1, o2 = np.empty(max(a.size, 1), np.uint32), np.empty(max(b.size, 1), np.uint32)
+            else:
+                n = int(jb[3])
+                o1, o2 = np.empty(max(n, 1), np.uint32), None
+            j = arr[i]
+            j.op, j.p, j.la, j.lb, j.k, j.n = op, p, a.size, b.size, k, n
+            j.a = a.ctypes.data if a.size else None
+            j.b = b.ctypes.data if b.size else None
+            j.out = o1.ctypes.data
+            j.out2 = o2.ctypes.data if o2 is not None else None
+            keep += [a, b]
+            outs.append((o1, o2))
+        rc = self._L.fpx_batch_run(self._h, C.cast(arr, C.c_void_p), len(jobs), repr)
+        if rc not in (OK, EDOMAIN, ESIZE, ELENGTH, EINVAL):
+            self._check(rc, "batch")
+        res = []
+        for i in range(len(jobs)):
+            j = arr[i]
+            if j.status != OK:
+                res.append(_ERRORS.get(j.status, FpxError)(j.status, f"batch job {i} ({jobs[i][0]})"))
+            elif j.op == OP_DIVMOD:
+                res.append((outs[i][0][: j.out_len], outs[i][1][: j.out2_len]))
+            else:
+                res.append(outs[i][0][: j.out_len])
+        return res
+
+    def batch_submit(self, jobs) -> int:
+        """fpx_batch_submit on a ctypes array of Job with device pointers; returns the call's status
+        (per-job statuses and lengths are written into the array)."""
+        return self._L.fpx_batch_submit(self._h, C.cast(jobs, C.c_void_p), len(jobs))
+
+    def batch_wait(self):
+        self._check(self._L.fpx_batch_wait(self._h), "batch_wait")
+
+
 def ntt_max_log(p: int) -> int:
     return load_library().fpx_ntt_max_log(p)
 
 
 __all__ = ["Context", "DomainError", "NttSizeError", "LengthError", "FpxError", "CANONICAL", "MONTGOMERY",
-           "load_library", "ntt_max_log", "LIB_PATH"]
+           "load_library", "ntt_max_log", "LIB_PATH", "Job", "OP_CONV", "OP_INV", "OP_LOG", "OP_EXP", "OP_SQRT",
+           "OP_POW", "OP_DIVMOD"]

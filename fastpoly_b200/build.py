@@ -25,8 +25,8 @@ NVCC = os.path.join(CUDA_HOME, "bin", "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 CU_SOURCES = ["kernels.cu", "noalloc.cu"]
-CPP_SOURCES = ["engine.cpp", "api.cpp"]
-HEADERS = ["field.cuh", "ntt_core.cuh", "kernels.h", "engine.h"]
+CPP_SOURCES = ["engine.cpp", "batch.cpp", "serve.cpp", "api.cpp"]
+HEADERS = ["field.cuh", "ntt_core.cuh", "ntt_fast.cuh", "kernels.h", "engine.h"]
 
 
 def _sources():
@@ -45,7 +45,9 @@ def _stale() -> bool:
 def _run(cmd, verbose):
     if verbose:
         print(" ".join(cmd), flush=True)
-    subprocess.run(cmd, check=True)
+    r = subprocess.run(cmd)
+    if r.returncode != 0:
+        raise RuntimeError(f"build step failed with status {r.returncode}: {cmd[0]} {cmd[-1]}")
 
 
 def build(force: bool = False, verbose: bool = False) -> str:

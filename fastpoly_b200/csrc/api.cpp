@@ -360,4 +360,35 @@ int fpx_mod(fpx_ctx* ctx, uint32_t p, const uint32_t* a, size_t la, const uint32
   return divmod_host(ctx, p, a, la, b, lb, nullptr, nullptr, r, r_len, repr, false, true);
 }
 
+// ---- batches
+
+int fpx_batch_submit(fpx_ctx* ctx, fpx_job* jobs, size_t count) {
+  if (count && !jobs) return FPX_EINVAL;
+  const int rc = guarded(ctx, [&](fpx::Engine& e) { e.batch(jobs, count); });
+  if (rc != FPX_OK) return rc;
+  for (size_t i = 0; i < count; ++i)
+    if (jobs[i].status != FPX_OK) {
+      ctx->err = "job " + std::to_string(i) + " failed with status " + std::to_string(jobs[i].status);
+      return jobs[i].status;
+    }
+  return FPX_OK;
+}
+
+int fpx_batch_wait(fpx_ctx* ctx) { return fpx_ctx_synchronize(ctx); }
+
+int fpx_batch_run(fpx_ctx* ctx, fpx_job* jobs, size_t count, int repr) {
+  if (count && !jobs) return FPX_EINVAL;
+  const int rc = guarded(ctx, [&](fpx::Engine& e) {
+    check_repr(repr);
+    e.batch_host(jobs, count, repr);
+  });
+  if (rc != FPX_OK) return rc;
+  for (size_t i = 0; i < count; ++i)
+    if (jobs[i].status != FPX_OK) {
+      ctx->err = "job " + std::to_string(i) + " failed with status " + std::to_string(jobs[i].status);
+      return jobs[i].status;
+    }
+  return FPX_OK;
+}
+
 }  // extern "C"

@@ -1,0 +1,765 @@
+// batch.cpp - many independent polynomial operations sharing launches.
+//
+// Products are recorded into a BatchRec and flushed together: one descriptor
+// upload and one launch set per transform size, whatever the mix of primes
+// (direct products for short operands, native transforms, 3-prime CRT lifts
+// with batched Garner reconstruction, crt_convolution.hpp:132-205).  The Newton
+// loops of inv, log and exp (inverse.hpp:163-188, exponential.hpp:85-207)
+// advance in lockstep over all jobs: one doubling step is two flushes for the
+// inverse extensions (inv jobs, the inverse inside log, and exp's running
+// inverse together) plus three for exp, however many jobs there are.
+#include <algorithm>
+#include <bit>
+#include <cstring>
+
+#include "engine.h"
+
+namespace fpx {
+
+namespace {
+constexpr size_t kNaiveB = 40;                                        // base.hpp:89
+const uint32_t kCrtPrimesB[3] = {167772161u, 469762049u, 754974721u};  // crt_convolution.hpp:14-18
+// Batched transforms use rows of 2^12 points: at most 2^23 points.
+constexpr int kBatchMaxLog = 23;
+
+Tw2 shoup_pair_b(uint32_t w, uint32_t p) { return Tw2{w, (uint32_t)(((uint64_t)w << 32) / p)}; }
+size_t round64(size_t w) { return (w + 63) & ~size_t(63); }
+}  // namespace
+
+// c[0, k) -> c[0, wanted) for the inverse of a (extend_inverse, inverse.hpp:18-65).
+struct ExtJob {
+  uint32_t p;
+  const uint32_t* a;
+  size_t la;
+  uint32_t* c;
+  size_t k, wanted;
+  uint32_t* cs;  // spectrum of c[0, k) at N = 2^ceil(log2 2k) (native primes), N words
+  uint32_t* h;   // wanted - k words
+};
+
+class BatchRec {
+ public:
+  explicit BatchRec(Engine& e) : e_(e) {}
+
+  // One cyclic product of size 2^logN on a native prime (Engine::cyc_product semantics).
+  void cyc(uint32_t p, int logN, const Engine::CycOp& op) {
+    XJob j;
+    j.pt = &e_.prime_plan(p).t;
+    j.logN = logN;
+    j.x = op.x;
+    j.y = op.y;
+    j.ymode = op.ymode;
+    j.yspec = op.yspec;
+    j.yspec_out = op.yspec_out;
+    j.epi = op.epi;
+    const uint32_t N = 1u << logN;
+    if (logN <= small_kernel_max_log()) {
+      // 1/N, times 2^32 after a Montgomery pointwise product, times the caller's factor
+      uint64_t s = invm(N % p, p);
+      if (op.ymode != 0) s = s * ((((uint64_t)1) << 32) % p) % p;
+      if (j.epi.scale.w) s = s * j.epi.scale.w % p;
+      j.epi.scale = shoup_pair_b((uint32_t)s, p);
+      need_.push_back(0);
+    } else {
+      j.bt = &e_.big_plan(p, logN).t;
+      if (j.epi.scale.w) j.epi.scale = shoup_pair_b(j.epi.scale.w % p, p);
+      need_.push_back(op.ymode == 1 ? 2 * (size_t)N : N);
+    }
+    cref_.push_back(-1);
+    plan_.xjobs.push_back(j);
+  }
+
+  // Coefficients [off, off+cnt) of a*b into out (times post_mont[i], negated),
+  // any prime.  cyc_log > 0: the caller guarantees that a cyclic product of
+  // 2^cyc_log points leaves the window free of wraparound (the Newton middle
+  // products, crt_middle_product, crt_convolution.hpp:211-227).
+  void product(uint32_t p, const uint32_t* a, size_t la, const uint32_t* b, size_t lb, size_t off, size_t cnt,
+               uint32_t* out, int cyc_log, const uint32_t* post_mont, bool negate) {
+    if (cnt == 0) return;
+    la = std::min(la, off + cnt);
+    lb = std::min(lb, off + cnt);
+    if (la == 0 || lb == 0 || la + lb - 1 <= off) {
+      zero_.emplace_back(out, cnt);
+      return;
+    }
+    const size_t full = la + lb - 1;
+    if (off + cnt > full) {  // past the full product: zeros
+      zero_.emplace_back(out + (full - off), off + cnt - full);
+      cnt = full - off;
+    }
+    if (std::min(la, lb) <= kNaiveB) {  // convolution.hpp:33-95
+      const bool swap = la > lb;
+      DirectJob d{p, swap ? b : a, swap ? lb : la, swap ? a : b, swap ? la : lb, off, cnt, out};
+      d.post_mont = post_mont;
+      d.negate = negate ? 1 : 0;
+      plan_.direct.push_back(d);
+      return;
+    }
+    const int logN = cyc_log > 0 ? cyc_log : std::bit_width(full - 1);
+    Epi epi;
+    epi.lo = (uint32_t)off;
+    epi.hi = (uint32_t)(off + cnt);
+    if (e_.native(p, logN)) {
+      Engine::CycOp op;
+      op.x = InOp{a, (uint32_t)la, 0};
+      if (a == b && la == lb) {
+        op.ymode = 3;
+      } else {
+        op.ymode = 1;
+        op.y = InOp{b, (uint32_t)lb, 0};
+      }
+      epi.out = out;
+      epi.mul_mont = post_mont;
+      epi.negate = negate ? 1 : 0;
+      op.epi = epi;
+      cyc(p, logN, op);
+      return;
+    }
+    // 3-prime CRT: each auxiliary product lands in a scratch buffer assigned at
+    // flush, then one Garner job reconstructs the window in the target field.
+    const size_t primes = crt_prime_count(p, std::min(la, lb));
+    GarnerJob g{p, (int)primes, nullptr, nullptr, nullptr, out, cnt};
+    g.post_mont = post_mont;
+    g.negate = negate ? 1 : 0;
+    const int gi = (int)plan_.garner.size();
+    for (size_t k = 0; k < primes; ++k) {
+      Engine::CycOp op;
+      op.x = InOp{a, (uint32_t)la, 1};
+      if (a == b && la == lb) {
+        op.ymode = 3;
+      } else {
+        op.ymode = 1;
+        op.y = InOp{b, (uint32_t)lb, 1};
+      }
+      op.epi = epi;
+      cyc(kCrtPrimesB[k], logN, op);
+      cref_.back() = (int)cbuf_.size();
+      cbuf_.push_back(CBuf{gi, (int)k, cnt});
+    }
+    plan_.garner.push_back(g);
+  }
+
+  bool empty() const { return plan_.xjobs.empty() && plan_.direct.empty() && plan_.garner.empty() && zero_.empty(); }
+
+  void flush() {
+    if (empty()) return;
+    for (auto& [ptr, n] : zero_) e_.check(cudaMemsetAsync(ptr, 0, n * 4, e_.stream()), "memset");
+    size_t words = 0;
+    for (size_t w : need_) words += round64(w);
+    for (const CBuf& c : cbuf_) words += round64(c.words);
+    Buf arena;
+    if (words) arena = Buf(&e_.pool(), words);
+    uint32_t* q = arena.get();
+    for (size_t i = 0; i < plan_.xjobs.size(); ++i) {
+      XJob& j = plan_.xjobs[i];
+      if (!need_[i]) continue;
+      const size_t N = size_t(1) << j.logN;
+      j.t1 = q;
+      j.t2 = need_[i] > N ? q + N : nullptr;
+      q += round64(need_[i]);
+    }
+    std::vector<uint32_t*> cptr(cbuf_.size());
+    for (size_t c = 0; c < cbuf_.size(); ++c) {
+      cptr[c] = q;
+      q += round64(cbuf_[c].words);
+      GarnerJob& g = plan_.garner[cbuf_[c].garner];
+      (cbuf_[c].k == 0 ? g.c1 : cbuf_[c].k == 1 ? g.c2 : g.c3) = cptr[c];
+    }
+    for (size_t i = 0; i < plan_.xjobs.size(); ++i)
+      if (cref_[i] >= 0) plan_.xjobs[i].epi.out = cptr[cref_[i]];
+    for (GarnerJob& g : plan_.garner) {
+      if (!g.c2) g.c2 = g.c1;
+      if (!g.c3) g.c3 = g.c1;
+    }
+    Engine::Stage& st = e_.stage(batch_descriptor_bytes(plan_));
+    e_.prof_begin();
+    e_.check(launch_batch(plan_, st.host, st.dev.get(), e_.stream(), st.ev), "batch");
+    e_.prof_end("batch");
+    e_.count_batch(plan_);
+    plan_ = BatchPlan();
+    need_.clear();
+    cref_.clear();
+    cbuf_.clear();
+    zero_.clear();
+  }
+
+ private:
+  struct CBuf {
+    int garner, k;
+    size_t words;
+  };
+  Engine& e_;
+  BatchPlan plan_;
+  std::vector<size_t> need_;  // scratch words per xjob
+  std::vector<int> cref_;     // xjob -> CRT buffer index, or -1
+  std::vector<CBuf> cbuf_;
+  std::vector<std::pair<uint32_t*, size_t>> zero_;
+};
+
+// ------------------------------------------------------------ staging ring
+
+Engine::Stage& Engine::stage(size_t bytes) {
+  Stage& s = stages_[stage_next_];
+  stage_next_ = (stage_next_ + 1) % kStages;
+  if (!s.ev) check(cudaEventCreateWithFlags(&s.ev, cudaEventDisableTiming), "cudaEventCreate");
+  else check(cudaEventSynchronize(s.ev), "staging wait");  // the slot's previous copy has left
+  if (bytes > s.cap) {
+    const size_t cap = std::max<size_t>(bytes + bytes / 2, size_t(1) << 16);
+    if (s.host) cudaFreeHost(s.host);
+    s.host = nullptr;
+    s.cap = 0;
+    check(cudaMallocHost(&s.host, cap), "cudaMallocHost");
+    s.dev = Buf(&pool_, cap / 4 + 1);
+    s.cap = cap;
+  }
+  return s;
+}
+
+void Engine::free_stages() {
+  if (pin_) cudaFreeHost(pin_);
+  pin_ = nullptr;
+  pin_words_ = 0;
+  for (Stage& s : stages_) {
+    if (s.host) cudaFreeHost(s.host);
+    if (s.ev) cudaEventDestroy(s.ev);
+    s.host = nullptr;
+    s.ev = nullptr;
+    s.cap = 0;
+    s.dev.reset();
+  }
+}
+
+void Engine::count_batch(const BatchPlan& b) {
+  std::vector<int> sizes;
+  for (const XJob& j : b.xjobs) sizes.push_back(j.logN);
+  std::sort(sizes.begin(), sizes.end());
+  sizes.erase(std::unique(sizes.begin(), sizes.end()), sizes.end());
+  for (int s : sizes) launches_ += s <= small_kernel_max_log() ? 1 : 3;
+  launches_ += (b.direct.empty() ? 0 : 1) + (b.garner.empty() ? 0 : 1);
+}
+
+void Engine::gather_first(const std::vector<const uint32_t*>& ptrs, uint32_t* host_out) {
+  Stage& st = stage(ptrs.size() * 12 + 512);
+  prof_begin();
+  check(launch_gather_first(ptrs, st.host, st.dev.get(), host_out, stream_), "gather");
+  prof_end("gather");
+  ++launches_;
+  sync();
+}
+
+void Engine::convert_repr(const std::vector<ReprSeg>& segs) {
+  if (segs.empty()) return;
+  Stage& st = stage(repr_batch_bytes(segs.size()));
+  prof_begin();
+  check(launch_repr_batch(segs, st.host, st.dev.get(), stream_, st.ev), "repr");
+  prof_end("repr");
+  launches_ += (segs.size() + 65534) / 65535;
+}
+
+// ------------------------------------------------- lockstep inverse extension
+
+// Five transforms at N = 2k for a native prime (as Engine::extend_inverse):
+// phase 1 = forward a, forward c (kept), inverse window [k, wanted) negated.
+void Engine::ext_phase1(BatchRec& rec, const ExtJob& j) {
+  const size_t hlen = j.wanted - j.k;
+  const int logN = std::bit_width(2 * j.k - 1);
+  const size_t aw = std::min(j.la, j.wanted);
+  if (native(j.p, logN)) {
+    CycOp op;
+    op.x = InOp{j.a, (uint32_t)aw, 0};
+    op.ymode = 1;
+    op.y = InOp{j.c, (uint32_t)j.k, 0};
+    op.yspec_out = j.cs;
+    op.epi.out = j.h;
+    op.epi.lo = (uint32_t)j.k;
+    op.epi.hi = (uint32_t)(j.k + hlen);
+    op.epi.negate = 1;
+    rec.cyc(j.p, logN, op);
+  } else {  // crt_middle_product (inverse.hpp:35-38)
+    rec.product(j.p, j.a, aw, j.c, j.k, j.k, hlen, j.h, logN, nullptr, true);
+  }
+}
+
+// phase 2 = forward h, times c's spectrum, inverse window [0, wanted - k) -> c + k.
+void Engine::ext_phase2(BatchRec& rec, const ExtJob& j) {
+  const size_t hlen = j.wanted - j.k;
+  const int logN = std::bit_width(2 * j.k - 1);
+  if (native(j.p, logN)) {
+    CycOp op;
+    op.x = InOp{j.h, (uint32_t)hlen, 0};
+    op.ymode = 2;
+    op.yspec = j.cs;
+    op.epi.out = j.c + j.k;
+    op.epi.lo = 0;
+    op.epi.hi = (uint32_t)hlen;
+    rec.cyc(j.p, logN, op);
+  } else {  // conv_limbs (inverse.hpp:39-40)
+    rec.product(j.p, j.h, hlen, j.c, j.k, 0, hlen, j.c + j.k, logN, nullptr, false);
+  }
+}
+
+// ------------------------------------------------------------------ batch
+
+namespace {
+enum Route : uint8_t { kNone, kConv, kInv, kLog, kExp, kSingle };
+}
+
+void Engine::batch(fpx_job* jobs, size_t count) {
+  std::vector<uint8_t> route(count, kNone);
+  std::vector<const uint32_t*> firsts(count, nullptr);
+  std::vector<size_t> conv_len(count, 0);
+  bool need_first = false;
+  const size_t max_series = size_t(1) << kBatchMaxLog;
+  for (size_t i = 0; i < count; ++i) {
+    fpx_job& j = jobs[i];
+    j.status = FPX_OK;
+    j.out_len = 0;
+    j.out2_len = 0;
+    if (j.p < 2 || j.p >= (1u << 31) || !is_prime(j.p) || (j.la && !j.a)) {
+      j.status = FPX_EINVAL;
+      continue;
+    }
+    switch (j.op) {
+      case FPX_OP_CONV: {
+        if (j.lb && !j.b) { j.status = FPX_EINVAL; break; }
+        if (j.la == 0 || j.lb == 0 || j.n == 0) break;  // convolution.hpp:17-31
+        const size_t la = std::min(j.la, j.n), lb = std::min(j.lb, j.n);
+        if (la > SIZE_MAX - (lb - 1)) { j.status = FPX_ELENGTH; break; }
+        const size_t outn = std::min(la + lb - 1, j.n);
+        if (!j.out) { j.status = FPX_EINVAL; break; }
+        j.out_len = outn;
+        conv_len[i] = outn;
+        const bool fits = std::min(la, lb) <= kNaiveB || std::bit_width(la + lb - 2) <= kBatchMaxLog;
+        route[i] = fits ? kConv : kSingle;
+        break;
+      }
+      case FPX_OP_INV:
+      case FPX_OP_LOG:
+      case FPX_OP_EXP: {
+        if (j.n == 0) break;
+        if (!j.out) { j.status = FPX_EINVAL; break; }
+        j.out_len = j.n;
+        // log's final product has 2n - 3 terms: at most 2^23 points for n <= 2^22
+        const size_t lim = j.op == FPX_OP_LOG ? max_series / 2 : max_series;
+        if (j.p == 2 || j.n > lim) {
+          route[i] = kSingle;
+          break;
+        }
+        route[i] = j.op == FPX_OP_INV ? kInv : (j.op == FPX_OP_LOG ? kLog : kExp);
+        if (j.la) firsts[i] = j.a;
+        need_first = true;
+        break;
+      }
+      case FPX_OP_SQRT:
+      case FPX_OP_POW:
+        if (j.n == 0) break;
+        if (!j.out) { j.status = FPX_EINVAL; break; }
+        j.out_len = j.n;
+        route[i] = kSingle;
+        break;
+      case FPX_OP_DIVMOD:  // out / out2 may be null: quotient / remainder not wanted
+        if (j.lb && !j.b) { j.status = FPX_EINVAL; break; }
+        route[i] = kSingle;
+        break;
+      default:
+        j.status = FPX_EINVAL;
+    }
+  }
+
+  // ---- domain checks of inv / log / exp: one gather of every constant term
+  if (need_first) {
+    std::vector<uint32_t> a0(count, 0);
+    gather_first(firsts, a0.data());
+    for (size_t i = 0; i < count; ++i) {
+      fpx_job& j = jobs[i];
+      const uint32_t p = j.p;
+      bool bad = false;
+      if (route[i] == kInv) bad = j.la == 0 || a0[i] == 0;                         // inverse.hpp:165-166
+      else if (route[i] == kLog) bad = j.la == 0 || a0[i] != 1 % p || j.n > p;     // exponential.hpp:86-90
+      else if (route[i] == kExp) bad = (j.la != 0 && a0[i] != 0) || j.n - 1 >= p;  // exponential.hpp:108-111
+      if (bad) {
+        j.status = FPX_EDOMAIN;
+        j.out_len = 0;
+        route[i] = kNone;
+      }
+    }
+  }
+
+  // ---- convolutions: one flush
+  {
+    BatchRec rec(*this);
+    for (size_t i = 0; i < count; ++i) {
+      if (route[i] != kConv) continue;
+      const fpx_job& j = jobs[i];
+      rec.product(j.p, j.a, std::min(j.la, j.n), j.b, std::min(j.lb, j.n), 0, conv_len[i], j.out, 0, nullptr,
+                  false);
+    }
+    rec.flush();
+  }
+
+  // ---- series: scratch, preparation, seeds
+  struct InvT {  // inverse of a[0, la) to n terms into out
+    uint32_t p;
+    const uint32_t* a;
+    size_t la, n;
+    uint32_t* out;
+    uint32_t *cs, *h;
+  };
+  struct ExpT {
+    size_t i;
+    size_t lap, csize;
+    uint32_t *ap, *c, *bs, *cs, *h, *t1, *t2;
+    const uint32_t* tab;
+  };
+  struct LogT {
+    size_t i, ld;
+    uint32_t *ap, *ia;
+    const uint32_t* tab;
+  };
+  std::vector<InvT> invs;
+  std::vector<ExpT> exps;
+  std::vector<LogT> logs;
+  size_t words = 0;
+  std::map<uint32_t, size_t> tab_need;  // prime -> largest 1/i needed
+  for (size_t i = 0; i < count; ++i) {
+    const fpx_job& j = jobs[i];
+    const size_t n = j.n, cnt = std::min(j.la, n);
+    if (route[i] == kInv) words += round64(2 * n) + round64(n);
+    if (route[i] == kLog && cnt > 1) {
+      words += 3 * round64(n) + round64(2 * n);
+      size_t& t = tab_need[j.p];
+      t = std::max(t, n - 1);
+    }
+    if (route[i] == kExp) {
+      words += 5 * round64(n) + 2 * round64(2 * n);
+      if (cnt > 1 && n > 1) {
+        size_t& t = tab_need[j.p];
+        t = std::max(t, n - 1);
+      }
+    }
+  }
+  bool any_series = false;
+  for (size_t i = 0; i < count; ++i) any_series |= route[i] == kInv || route[i] == kLog || route[i] == kExp;
+  if (any_series) {
+    for (auto& [p, need] : tab_need) inv_table(p, need);  // grow once per prime, before any pointer is kept
+    Buf arena(&pool_, words ? words : 1);
+    uint32_t* q = arena.get();
+    auto take = [&](size_t w) {
+      uint32_t* r = q;
+      q += round64(w);
+      return r;
+    };
+    std::vector<ExpPrep> preps;
+    std::vector<SeedJob> seeds1, seeds2;
+    for (size_t i = 0; i < count; ++i) {
+      fpx_job& j = jobs[i];
+      const size_t n = j.n, cnt = std::min(j.la, n);
+      if (route[i] == kInv) {
+        InvT t{j.p, j.a, cnt, n, j.out, take(2 * n), take(n)};
+        invs.push_back(t);
+        seeds1.push_back(SeedJob{0, j.p, j.a, cnt, j.out, (int)std::min<size_t>(n, 32), 0});
+      } else if (route[i] == kLog) {
+        if (cnt <= 1 || n == 1) {  // log = 0
+          ExpPrep e{j.p, j.a, 0, nullptr, j.out, n};
+          e.out0 = 0;
+          preps.push_back(e);
+          continue;
+        }
+        LogT l{i, cnt - 1, take(n), take(n), inv_table(j.p, n - 1)};
+        ExpPrep e{j.p, j.a, cnt, l.ap, j.out, n};
+        e.out0 = 0;
+        preps.push_back(e);
+        // inverse of a to n - 1 terms (exponential.hpp:92-95)
+        const size_t ila = std::min(cnt, n - 1);
+        InvT t{j.p, j.a, ila, n - 1, l.ia, take(2 * n), take(n)};
+        invs.push_back(t);
+        seeds1.push_back(SeedJob{0, j.p, j.a, ila, l.ia, (int)std::min<size_t>(n - 1, 32), 0});
+        logs.push_back(l);
+      } else if (route[i] == kExp) {
+        ExpT e{};
+        e.i = i;
+        e.lap = cnt ? cnt - 1 : 0;
+        e.csize = 16;
+        e.ap = take(n);
+        e.c = take(n);
+        e.bs = take(2 * n);
+        e.cs = take(2 * n);
+        e.h = take(n);
+        e.t1 = take(n);
+        e.t2 = take(n);
+        preps.push_back(ExpPrep{j.p, j.a, cnt, e.ap, j.out, n});
+        if (e.lap && n > 1) {
+          e.tab = inv_table(j.p, n - 1);
+          seeds1.push_back(SeedJob{1, j.p, e.ap, e.lap, j.out, (int)std::min<size_t>(n, 32), 0});
+          if (n > 32) seeds2.push_back(SeedJob{0, j.p, j.out, 32, e.c, 16, 0});
+        } else {
+          e.lap = 0;
+        }
+        exps.push_back(e);
+      }
+    }
+    if (!preps.empty()) {
+      Stage& st = stage(batch_aux_bytes(preps.size()));
+      prof_begin();
+      check(launch_exp_prep_batch(preps, st.host, st.dev.get(), stream_, st.ev), "prep");
+      prof_end("prep");
+      ++launches_;
+    }
+    if (!seeds1.empty()) {
+      Stage& st = stage(batch_aux_bytes(seeds1.size()));
+      prof_begin();
+      check(launch_seeds_batch(seeds1, st.host, st.dev.get(), stream_, st.ev), "seed");
+      prof_end("seed");
+      ++launches_;
+    }
+    if (!seeds2.empty()) {
+      Stage& st = stage(batch_aux_bytes(seeds2.size()));
+      prof_begin();
+      check(launch_seeds_batch(seeds2, st.host, st.dev.get(), stream_, st.ev), "seed");
+      prof_end("seed");
+      ++launches_;
+    }
+
+    // ---- lockstep doubling
+    for (size_t m = 32;; m <<= 1) {
+      std::vector<ExtJob> ext;
+      for (const InvT& t : invs)
+        if (m < t.n) ext.push_back(ExtJob{t.p, t.a, t.la, t.out, m, std::min(2 * m, t.n), t.cs, t.h});
+      std::vector<ExpT*> act;
+      for (ExpT& e : exps) {
+        const fpx_job& j = jobs[e.i];
+        if (!e.lap || m >= j.n) continue;
+        act.push_back(&e);
+        const size_t hlen = std::min(2 * m, j.n) - m;
+        if (e.csize < hlen) {  // exponential.hpp:158-163: extend the inverse of b
+          ext.push_back(ExtJob{j.p, j.out, m, e.c, e.csize, hlen, e.cs, e.h});
+          e.csize = hlen;
+        }
+      }
+      if (ext.empty() && act.empty()) break;
+      if (!ext.empty()) {
+        BatchRec r1(*this);
+        for (const ExtJob& x : ext) ext_phase1(r1, x);
+        r1.flush();
+        BatchRec r2(*this);
+        for (const ExtJob& x : ext) ext_phase2(r2, x);
+        r2.flush();
+      }
+      if (act.empty()) continue;
+      // exp step (exponential.hpp:165-205), eight transforms at N = 2m per job
+      const int logN = std::bit_width(2 * m - 1);
+      BatchRec r3(*this);
+      for (ExpT* e : act) {  // (a' b)[m-1, m-1+hlen); b's spectrum kept
+        const fpx_job& j = jobs[e->i];
+        const size_t m2 = std::min(2 * m, j.n), hlen = m2 - m, lx = std::min(e->lap, m2 - 1);
+        if (native(j.p, logN)) {
+          CycOp op;
+          op.x = InOp{e->ap, (uint32_t)lx, 0};
+          op.ymode = 1;
+          op.y = InOp{j.out, (uint32_t)m, 0};
+          op.yspec_out = e->bs;
+          op.epi.out = e->t1;
+          op.epi.lo = (uint32_t)(m - 1);
+          op.epi.hi = (uint32_t)(m - 1 + hlen);
+          r3.cyc(j.p, logN, op);
+        } else {
+          r3.product(j.p, e->ap, lx, j.out, m, m - 1, hlen, e->t1, logN, nullptr, false);
+        }
+      }
+      r3.flush();
+      BatchRec r4(*this);
+      for (ExpT* e : act) {  // (residual * c) mod x^hlen, integrated: times 1/(m+i)
+        const fpx_job& j = jobs[e->i];
+        const size_t hlen = std::min(2 * m, j.n) - m;
+        if (native(j.p, logN)) {
+          CycOp op;
+          op.x = InOp{e->t1, (uint32_t)hlen, 0};
+          op.ymode = 1;
+          op.y = InOp{e->c, (uint32_t)e->csize, 0};
+          op.epi.out = e->t2;
+          op.epi.lo = 0;
+          op.epi.hi = (uint32_t)hlen;
+          op.epi.mul_mont = e->tab + m;
+          r4.cyc(j.p, logN, op);
+        } else {
+          r4.product(j.p, e->t1, hlen, e->c, e->csize, 0, hlen, e->t2, logN, e->tab + m, false);
+        }
+      }
+      r4.flush();
+      BatchRec r5(*this);
+      for (ExpT* e : act) {  // b[m, m+hlen) = (correction * b) mod x^hlen
+        const fpx_job& j = jobs[e->i];
+        const size_t hlen = std::min(2 * m, j.n) - m;
+        if (native(j.p, logN)) {
+          CycOp op;
+          op.x = InOp{e->t2, (uint32_t)hlen, 0};
+          op.ymode = 2;
+          op.yspec = e->bs;
+          op.epi.out = j.out + m;
+          op.epi.lo = 0;
+          op.epi.hi = (uint32_t)hlen;
+          r5.cyc(j.p, logN, op);
+        } else {
+          r5.product(j.p, e->t2, hlen, j.out, m, 0, hlen, j.out + m, logN, nullptr, false);
+        }
+      }
+      r5.flush();
+    }
+
+    // ---- log: integral(a' * inv(a)) (exponential.hpp:92-97)
+    if (!logs.empty()) {
+      BatchRec rl(*this);
+      for (const LogT& l : logs) {
+        const fpx_job& j = jobs[l.i];
+        const size_t lp = std::min(l.ld + j.n - 2, j.n - 1);
+        rl.product(j.p, l.ap, l.ld, l.ia, j.n - 1, 0, lp, j.out + 1, 0, l.tab + 1, false);
+      }
+      rl.flush();
+    }
+  }
+
+  // ---- jobs that share no launches run one after another
+  for (size_t i = 0; i < count; ++i) {
+    if (route[i] != kSingle) continue;
+    fpx_job& j = jobs[i];
+    try {
+      switch (j.op) {
+        case FPX_OP_CONV: j.out_len = conv(j.p, j.a, j.la, j.b, j.lb, j.n, j.out); break;
+        case FPX_OP_INV: inv(j.p, j.a, std::min(j.la, j.n), j.n, j.out); break;
+        case FPX_OP_LOG: log(j.p, j.a, std::min(j.la, j.n), j.n, j.out); break;
+        case FPX_OP_EXP: exp(j.p, j.a, std::min(j.la, j.n), j.n, j.out); break;
+        case FPX_OP_SQRT: sqrt(j.p, j.a, std::min(j.la, j.n), j.n, j.out); break;
+        case FPX_OP_POW: pow(j.p, j.a, j.la, j.k, j.n, j.out); break;
+        case FPX_OP_DIVMOD: {
+          size_t lq = 0, lr = 0;
+          divmod(j.p, j.a, j.la, j.b, j.lb, j.out, &lq, j.out2, &lr, j.out != nullptr, j.out2 != nullptr);
+          j.out_len = lq;
+          j.out2_len = lr;
+          break;
+        }
+        default: j.status = FPX_EINVAL;
+      }
+    } catch (const Error& e) {
+      if (e.code == FPX_ECUDA) throw;  // the stream is unusable: fail the whole batch
+      j.status = e.code;
+      j.out_len = 0;
+      j.out2_len = 0;
+    }
+  }
+}
+
+
+// ------------------------------------------------------- host-buffer batches
+
+// Packs every input into one pinned buffer (one host->device copy), runs the
+// batch on device copies, and brings every output back in one copy.
+void Engine::batch_host(fpx_job* jobs, size_t count, int repr) {
+  // Words each job reads and writes (host side); the device copy of a job
+  // points into one input and one output region.
+  std::vector<size_t> wa(count), wb(count), wo(count), wo2(count);
+  size_t in_words = 0, out_words = 0;
+  for (size_t i = 0; i < count; ++i) {
+    const fpx_job& j = jobs[i];
+    size_t a = 0, b = 0, o = 0, o2 = 0;
+    switch (j.op) {
+      case FPX_OP_CONV:
+        a = j.la < j.n ? j.la : j.n;
+        b = j.lb < j.n ? j.lb : j.n;
+        if (a && b) o = a > SIZE_MAX - b ? j.n : (a + b - 1 < j.n ? a + b - 1 : j.n);
+        break;
+      case FPX_OP_INV:
+      case FPX_OP_LOG:
+      case FPX_OP_EXP:
+      case FPX_OP_SQRT:
+        a = j.la < j.n ? j.la : j.n;
+        o = j.n;
+        break;
+      case FPX_OP_POW:
+        a = j.la;
+        o = j.n;
+        break;
+      case FPX_OP_DIVMOD:
+        a = j.la;
+        b = j.lb;
+        o = j.out ? j.la : 0;
+        o2 = j.out2 ? j.lb : 0;
+        break;
+      default:
+        break;
+    }
+    if (a && !j.a) a = 0;  // the batch reports the null pointer
+    if (b && !j.b) b = 0;
+    if (o && !j.out) o = 0;
+    wa[i] = a;
+    wb[i] = b;
+    wo[i] = o;
+    wo2[i] = o2;
+    in_words += a + b;
+    out_words += o + o2;
+  }
+  const size_t total = in_words + out_words;
+  if (total > pin_words_) {
+    if (pin_) cudaFreeHost(pin_);
+    pin_ = nullptr;
+    pin_words_ = 0;
+    const size_t want = total + total / 4 + 1024;
+    check(cudaMallocHost(&pin_, want * 4), "cudaMallocHost");
+    pin_words_ = want;
+  }
+  uint32_t* hin = pin_;
+  uint32_t* hout = pin_ + in_words;
+  Buf dbuf(&pool_, total ? total : 1);
+  uint32_t* din = dbuf.get();
+  uint32_t* dout = din + in_words;
+  std::vector<fpx_job> dj(jobs, jobs + count);
+  std::vector<ReprSeg> segs;
+  size_t qi = 0, qo = 0;
+  for (size_t i = 0; i < count; ++i) {
+    const fpx_job& j = jobs[i];
+    fpx_job& d = dj[i];
+    if (wa[i]) std::memcpy(hin + qi, j.a, wa[i] * 4);
+    d.a = j.a ? din + qi : nullptr;
+    if (wa[i]) segs.push_back(ReprSeg{j.p, din + qi, wa[i], 0});
+    qi += wa[i];
+    if (wb[i]) std::memcpy(hin + qi, j.b, wb[i] * 4);
+    d.b = j.b ? din + qi : nullptr;
+    if (wb[i]) segs.push_back(ReprSeg{j.p, din + qi, wb[i], 0});
+    qi += wb[i];
+    d.la = j.a ? wa[i] : j.la;  // a null pointer keeps its length: the batch reports it
+    d.lb = j.b ? wb[i] : j.lb;
+    d.out = j.out ? dout + qo : nullptr;
+    qo += wo[i];
+    d.out2 = j.out2 ? dout + qo : nullptr;
+    qo += wo2[i];
+  }
+  if (in_words) check(cudaMemcpyAsync(din, hin, in_words * 4, cudaMemcpyHostToDevice, stream_), "H2D");
+  if (repr == FPX_REPR_MONTGOMERY) convert_repr(segs);
+  batch(dj.data(), count);
+  if (repr == FPX_REPR_MONTGOMERY) {
+    segs.clear();
+    for (size_t i = 0; i < count; ++i) {
+      const fpx_job& d = dj[i];
+      if (d.status != FPX_OK) continue;
+      if (d.out && d.out_len) segs.push_back(ReprSeg{d.p, d.out, d.out_len, 1});
+      if (d.out2 && d.out2_len) segs.push_back(ReprSeg{d.p, d.out2, d.out2_len, 1});
+    }
+    convert_repr(segs);
+  }
+  if (out_words) check(cudaMemcpyAsync(hout, dout, out_words * 4, cudaMemcpyDeviceToHost, stream_), "D2H");
+  sync();
+  qo = 0;
+  for (size_t i = 0; i < count; ++i) {
+    fpx_job& j = jobs[i];
+    const fpx_job& d = dj[i];
+    j.status = d.status;
+    j.out_len = d.out_len;
+    j.out2_len = d.out2_len;
+    if (d.status == FPX_OK) {
+      if (j.out && d.out_len) std::memcpy(j.out, hout + qo, std::min(d.out_len, wo[i]) * 4);
+      if (j.out2 && d.out2_len) std::memcpy(j.out2, hout + qo + wo[i], std::min(d.out2_len, wo2[i]) * 4);
+    }
+    qo += wo[i] + wo2[i];
+  }
+}
+
+}  // namespace fpx

@@ -209,6 +209,7 @@ Engine::~Engine() {
   primes_.clear();
   bigs_.clear();
   inv_tabs_.clear();
+  free_stages();
   for (auto& r : prof_recs_) { cudaEventDestroy(r.b); cudaEventDestroy(r.e); }
   for (auto ev : ev_free_) cudaEventDestroy(ev);
   if (scratch_ull_) cudaFree(scratch_ull_);

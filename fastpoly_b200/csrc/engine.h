@@ -15,6 +15,7 @@
 
 #include <cuda_runtime.h>
 
+#include "fpx_b200.h"
 #include "kernels.h"
 
 namespace fpx {
@@ -42,6 +43,8 @@ class Pool {
 };
 
 class Engine;
+class BatchRec;
+struct ExtJob;
 
 // RAII scratch buffer from the pool.
 class Buf {
@@ -110,6 +113,17 @@ class Engine {
               uint32_t* r, size_t* lr, bool want_q, bool want_r);
   void ntt(uint32_t p, uint32_t* data, uint32_t n, bool inverse);
 
+  // Many independent operations (device pointers) with shared launches:
+  // products of all jobs in one launch set per transform size, the Newton loops
+  // of inv / log / exp in lockstep.  Sets each job's status and lengths.
+  void batch(fpx_job* jobs, size_t count);
+  // The same with host buffers (blocking): inputs packed into one pinned
+  // buffer and copied at once, outputs brought back in one copy; repr as the
+  // C ABI's (canonical or Montgomery limbs).
+  void batch_host(fpx_job* jobs, size_t count, int repr);
+  // In-place representation changes of many arrays in one launch.
+  void convert_repr(const std::vector<ReprSeg>& segs);
+
   void check(cudaError_t e, const char* what);
   void sync();
 
@@ -119,6 +133,7 @@ class Engine {
   uint64_t launches() const { return launches_; }
 
  private:
+  friend class BatchRec;
   // ---- plans
   const PrimePlan& prime_plan(uint32_t p);
   const BigPlan& big_plan(uint32_t p, int logN);
@@ -151,6 +166,27 @@ class Engine {
   void inv_into(uint32_t p, const uint32_t* a, size_t la, size_t n, uint32_t* out);
   void exp_into(uint32_t p, const uint32_t* a, size_t la, size_t n, uint32_t* out);
   void log_into(uint32_t p, const uint32_t* a, size_t la, size_t n, uint32_t* out);
+
+  // ---- batches (batch.cpp)
+  struct Stage {  // one slot of the descriptor staging ring
+    void* host = nullptr;  // pinned
+    size_t cap = 0;
+    Buf dev;
+    cudaEvent_t ev = nullptr;  // recorded after the slot's host->device copy
+  };
+  static constexpr int kStages = 4;
+  Stage stages_[kStages];
+  int stage_next_ = 0;
+  uint32_t* pin_ = nullptr;  // pinned packing buffer of batch_host
+  size_t pin_words_ = 0;
+  // Next ring slot, holding >= bytes, whose previous copy has completed.
+  Stage& stage(size_t bytes);
+  void free_stages();
+  void count_batch(const BatchPlan& b);
+  // host_out[i] = *ptrs[i] (0 for null), one launch, then synchronises.
+  void gather_first(const std::vector<const uint32_t*>& ptrs, uint32_t* host_out);
+  void ext_phase1(BatchRec& rec, const ExtJob& j);
+  void ext_phase2(BatchRec& rec, const ExtJob& j);
 
   // small device->host reads
   uint32_t read_word(const uint32_t* d);

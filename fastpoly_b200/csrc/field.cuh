@@ -31,7 +31,14 @@ __host__ __device__ inline uint32_t inv_mod_2_32(uint32_t a) {
 __host__ inline Fp make_fp(uint32_t p) { return Fp{p, 2u * p, inv_mod_2_32(p)}; }
 
 // min(x, x - m) over unsigned: subtract m once if x >= m (x < 2m required).
-__device__ __forceinline__ uint32_t red(uint32_t x, uint32_t m) { return min(x, x - m); }
+// One DPX add-min instruction on sm_90 and later.
+__device__ __forceinline__ uint32_t red(uint32_t x, uint32_t m) {
+#if defined(__CUDA_ARCH__) && __CUDA_ARCH__ >= 900
+  return __viaddmin_u32(x, 0u - m, x);
+#else
+  return min(x, x - m);
+#endif
+}
 
 // a*w mod p in [0, 2p) for any a < 2^32, w < p, wq = floor(w*2^32/p).
 __device__ __forceinline__ uint32_t shoup(uint32_t a, uint32_t w, uint32_t wq, uint32_t p) {

@@ -18,6 +18,10 @@
 //     reference's bit-reversed DIF order.
 #include <cuda_runtime.h>
 
+#include <algorithm>
+#include <cstring>
+#include <vector>
+
 #include "field.cuh"
 #include "kernels.h"
 #include "ntt_core.cuh"
@@ -95,7 +99,7 @@ struct SmallD {
   EpiD epi;
 };
 
-__global__ void __launch_bounds__(512) k_small(SmallD job, Ptab pt, int logN) {
+__device__ __forceinline__ void small_body(const SmallD& job, const Ptab& pt, int logN) {
   extern __shared__ uint32_t sm[];
   const int N = 1 << logN, tid = threadIdx.x, nt = blockDim.x;
   uint32_t* X = sm;
@@ -132,6 +136,8 @@ __global__ void __launch_bounds__(512) k_small(SmallD job, Ptab pt, int logN) {
   const uint32_t hi = job.epi.hi < (uint32_t)N ? job.epi.hi : (uint32_t)N;
   for (uint32_t i = job.epi.lo + tid; i < hi; i += nt) epi_store(job.epi, i, X[pad(i)], f);
 }
+
+__global__ void __launch_bounds__(512) k_small(SmallD job, Ptab pt, int logN) { small_body(job, pt, logN); }
 
 // ---------------------------------------------------------------------------
 // Pass A forward (columns).
@@ -262,8 +268,10 @@ struct GarnerC {
 
 __device__ __forceinline__ uint32_t redc_any(uint32_t x, uint32_t m) { return min(x, x - m); }
 
-__global__ void k_garner(GarnerC g, int primes, const uint32_t* c1, const uint32_t* c2, const uint32_t* c3,
-                         uint32_t* out, size_t n, int accumulate) {
+__device__ __forceinline__ void garner_body(const GarnerC& g, int primes, const uint32_t* c1, const uint32_t* c2,
+                                            const uint32_t* c3, uint32_t* out, size_t n, int accumulate,
+                                            const uint32_t* post_mont = nullptr, int negate = 0,
+                                            uint32_t tpinv = 0) {
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
     const uint32_t x1 = c1[i];
     uint32_t v = x1 - __umulhi(x1, g.t_q1) * g.t;
@@ -280,9 +288,19 @@ __global__ void k_garner(GarnerC g, int primes, const uint32_t* c1, const uint32
         v = redc_any(v + v3, g.t);
       }
     }
+    if (post_mont) {  // Montgomery table product in the target field (odd target)
+      const Fp ft{g.t, 2 * g.t, tpinv};
+      v = red(mont(v, __ldg(post_mont + i), ft), g.t);
+    }
+    if (negate && v) v = g.t - v;
     if (accumulate) v = redc_any(v + out[i], g.t);
     out[i] = v;
   }
+}
+
+__global__ void k_garner(GarnerC g, int primes, const uint32_t* c1, const uint32_t* c2, const uint32_t* c3,
+                         uint32_t* out, size_t n, int accumulate) {
+  garner_body(g, primes, c1, c2, c3, out, n, accumulate);
 }
 
 __global__ void k_from_mont(Fp f, const uint32_t* in, uint32_t* out, size_t n) {
@@ -328,8 +346,9 @@ __global__ void k_derivative(Fp f, uint32_t q1, uint2 r_sh, const uint32_t* a, u
 
 // Direct product window (short operand a, la <= 40):
 // out[i] = sum_j a[j] * b[i + off - j].
-__global__ void k_direct(uint32_t p, Fp f, uint2 r_sh, const uint32_t* a, int la, const uint32_t* b, size_t lb,
-                         size_t off, size_t cnt, uint32_t* out, int accumulate) {
+__device__ __forceinline__ void direct_body(uint32_t p, const Fp& f, const uint32_t* a, int la, const uint32_t* b,
+                                            size_t lb, size_t off, size_t cnt, uint32_t* out, int accumulate,
+                                            const uint32_t* post_mont = nullptr, int negate = 0) {
   __shared__ uint32_t am[64];
   if (threadIdx.x < la) {
     const uint32_t v = a[threadIdx.x];
@@ -348,12 +367,19 @@ __global__ void k_direct(uint32_t p, Fp f, uint2 r_sh, const uint32_t* a, int la
       else acc += mont(am[j], bv, f);
     }
     uint32_t v = (p == 2) ? (bits & 1u) : (uint32_t)(acc % p);
+    if (post_mont) v = red(mont(v, __ldg(post_mont + i), f), f.p);
+    if (negate && v) v = p - v;
     if (accumulate) {
       const uint64_t s = (uint64_t)v + out[i];
       v = (uint32_t)(s >= p ? s - p : s);
     }
     out[i] = v;
   }
+}
+
+__global__ void k_direct(uint32_t p, Fp f, uint2 r_sh, const uint32_t* a, int la, const uint32_t* b, size_t lb,
+                         size_t off, size_t cnt, uint32_t* out, int accumulate) {
+  direct_body(p, f, a, la, b, lb, off, cnt, out, accumulate);
 }
 
 int grid_for(size_t n, int threads) {
@@ -371,6 +397,7 @@ namespace fpx {
 int small_kernel_max_log() { return kSmallLog; }
 
 cudaError_t kernels_fast_init();
+cudaError_t kernels_batch_init();
 cudaError_t launch_rows_generic(const PrimeTables& pt, const BigTables& bt, uint32_t* x, const uint32_t* y, int ymode,
                                 uint32_t* y_spec_out, int forward, int inverse, cudaStream_t s);
 
@@ -386,7 +413,8 @@ cudaError_t kernels_init() {
   set((const void*)k_rows, 2 * padded_words(1 << 13) * 4);
   set((const void*)k_colinv, padded_words(1 << 14) * 4);
   const cudaError_t r = kernels_fast_init();
-  return e != cudaSuccess ? e : r;
+  const cudaError_t r2 = kernels_batch_init();
+  return e != cudaSuccess ? e : (r != cudaSuccess ? r : r2);
 }
 
 cudaError_t launch_small(const PrimeTables& pt, int logN, const SmallJob& job, cudaStream_t s) {
@@ -561,7 +589,8 @@ __device__ __forceinline__ uint32_t warp_sum_mod(uint32_t v, uint32_t p) {
 // kind 1: exp seed       b[i] = (sum_{j=1..min(i,la)} a[j-1] b[i-j]) / i,   b[0] = 1   (a = a')
 // kind 2: sqrt seed      b[i] = (u[i] - sum_{j=1..i-1} b[j] b[i-j]) * w,     b[0] = r0, w = 1/(2 r0)
 // One warp; n <= 64.  Writes out[0..n).
-__global__ void k_seed(int kind, uint32_t p, const uint32_t* a, size_t la, uint32_t* out, int n, uint32_t r0) {
+__device__ __forceinline__ void seed_body(int kind, uint32_t p, const uint32_t* a, size_t la, uint32_t* out, int n,
+                                          uint32_t r0) {
   __shared__ uint32_t c[64];
   const int lane = threadIdx.x;
   uint32_t w = 0;
@@ -593,6 +622,34 @@ __global__ void k_seed(int kind, uint32_t p, const uint32_t* a, size_t la, uint3
     __syncwarp();
   }
   for (int i = lane; i < n; i += 32) out[i] = c[i];
+}
+
+__global__ void k_seed(int kind, uint32_t p, const uint32_t* a, size_t la, uint32_t* out, int n, uint32_t r0) {
+  seed_body(kind, p, a, la, out, n, r0);
+}
+
+// exp / log preparation (exponential.hpp:85-139): out = out0 + 0x + ..., ap = a'
+// (first cnt coefficients of a); blockIdx.y = job.
+struct ExpPrepB {
+  Fp f;
+  uint32_t q1;
+  uint2 r_sh;
+  const uint32_t* a;
+  size_t cnt;  // min(la, n)
+  uint32_t* ap;
+  uint32_t* out;
+  size_t n;
+  uint32_t out0;
+};
+__global__ void k_exp_prep_b(const ExpPrepB* __restrict__ jobs) {
+  const ExpPrepB& j = jobs[blockIdx.y];
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < j.n; i += (size_t)gridDim.x * blockDim.x) {
+    j.out[i] = i == 0 ? j.out0 : 0u;
+    if (i + 1 < j.cnt) {
+      const uint32_t k = reduce_any((uint32_t)(i + 1), j.q1, j.f);
+      j.ap[i] = red(shoup(red(mont(j.a[i + 1], k, j.f), j.f.p), j.r_sh, j.f.p), j.f.p);
+    }
+  }
 }
 
 // First (mode 0) or last (mode 1) index in [0, n) with a[i] != 0; n if none.
@@ -691,13 +748,28 @@ namespace {
 // ymode == 1), pointwise product (ymode 1 raw y, 2 y spectrum, 3 square),
 // inverse (DIT).  The forward's last group, the product and the inverse's first
 // group all act on the same 16 positions per thread, in registers.
-__global__ void __launch_bounds__(256, 3) k_rows12(uint32_t* __restrict__ x, const uint32_t* __restrict__ y,
-                                                  int ymode, uint32_t* __restrict__ y_spec_out, int forward,
-                                                  int inverse, Ptab pt) {
-  __shared__ uint32_t sX[4096];
-  __shared__ uint32_t sY[4096];
+__device__ __forceinline__ void lds16(const uint32_t* p, uint32_t (&v)[16]) {
+  const uint4* q = reinterpret_cast<const uint4*>(p);
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const uint4 u = q[k];
+    v[4 * k] = u.x; v[4 * k + 1] = u.y; v[4 * k + 2] = u.z; v[4 * k + 3] = u.w;
+  }
+}
+__device__ __forceinline__ void sts16(uint32_t* p, const uint32_t (&v)[16]) {
+  uint4* q = reinterpret_cast<uint4*>(p);
+#pragma unroll
+  for (int k = 0; k < 4; ++k) q[k] = make_uint4(v[4 * k], v[4 * k + 1], v[4 * k + 2], v[4 * k + 3]);
+}
+
+__device__ __forceinline__ void rows12_body(uint32_t* __restrict__ x, const uint32_t* __restrict__ y, int ymode,
+                                            uint32_t* __restrict__ y_spec_out, int forward, int inverse,
+                                            const Ptab& pt, unsigned row_index) {
+  __shared__ __align__(16) uint32_t sX[kRowWords];
+  __shared__ __align__(16) uint32_t sY[kRowWords];
   const int t = threadIdx.x;
-  const size_t row = (size_t)blockIdx.x << 12;
+  const int bA = baseA(t), bB = baseB(t), bC = baseC(t);
+  const size_t row = (size_t)row_index << 12;
   const Fp f = pt.f;
   uint32_t v[2][16];
   if (forward) {
@@ -710,28 +782,25 @@ __global__ void __launch_bounds__(256, 3) k_rows12(uint32_t* __restrict__ x, con
       bf_group<4, 12, false, 2>(v, pt.fwd, t, f);
 #pragma unroll
       for (int i = 0; i < 16; ++i) {
-        sX[swz12(posA(t, i))] = v[0][i];
-        sY[swz12(posA(t, i))] = v[1][i];
+        sX[bA + offA(i)] = v[0][i];
+        sY[bA + offA(i)] = v[1][i];
       }
       __syncthreads();
 #pragma unroll
       for (int i = 0; i < 16; ++i) {
-        v[0][i] = sX[swz12(posB(t, i))];
-        v[1][i] = sY[swz12(posB(t, i))];
+        v[0][i] = sX[bB + offB(i)];
+        v[1][i] = sY[bB + offB(i)];
       }
       bf_group<4, 8, false, 2>(v, pt.fwd, t & 15, f);
 #pragma unroll
       for (int i = 0; i < 16; ++i) {
-        sX[swz12(posB(t, i))] = v[0][i];
-        sY[swz12(posB(t, i))] = v[1][i];
+        sX[bB + offB(i)] = v[0][i];
+        sY[bB + offB(i)] = v[1][i];
       }
       __syncthreads();
-#pragma unroll
-      for (int i = 0; i < 16; ++i) {
-        v[0][i] = sX[swz12(posC(t, i))];
-        v[1][i] = sY[swz12(posC(t, i))];
-      }
-      bf_group<4, 4, false, 2>(v, pt.fwd, 0, f);
+      lds16(sX + bC, v[0]);
+      lds16(sY + bC, v[1]);
+      bf_group<4, 4, false, 2, true>(v, pt.fwd, 0, f);
       if (y_spec_out) {
         uint4* o = reinterpret_cast<uint4*>(y_spec_out + row + posC(t, 0));
 #pragma unroll
@@ -744,17 +813,16 @@ __global__ void __launch_bounds__(256, 3) k_rows12(uint32_t* __restrict__ x, con
       for (int i = 0; i < 16; ++i) v[0][i] = x[row + posA(t, i)];
       bf_group<4, 12, false, 1>(v, pt.fwd, t, f);
 #pragma unroll
-      for (int i = 0; i < 16; ++i) sX[swz12(posA(t, i))] = v[0][i];
+      for (int i = 0; i < 16; ++i) sX[bA + offA(i)] = v[0][i];
       __syncthreads();
 #pragma unroll
-      for (int i = 0; i < 16; ++i) v[0][i] = sX[swz12(posB(t, i))];
+      for (int i = 0; i < 16; ++i) v[0][i] = sX[bB + offB(i)];
       bf_group<4, 8, false, 1>(v, pt.fwd, t & 15, f);
 #pragma unroll
-      for (int i = 0; i < 16; ++i) sX[swz12(posB(t, i))] = v[0][i];
+      for (int i = 0; i < 16; ++i) sX[bB + offB(i)] = v[0][i];
       __syncthreads();
-#pragma unroll
-      for (int i = 0; i < 16; ++i) v[0][i] = sX[swz12(posC(t, i))];
-      bf_group<4, 4, false, 1>(v, pt.fwd, 0, f);
+      lds16(sX + bC, v[0]);
+      bf_group<4, 4, false, 1, true>(v, pt.fwd, 0, f);
     }
   } else {
     const uint4* in = reinterpret_cast<const uint4*>(x + row + posC(t, 0));
@@ -789,21 +857,26 @@ __global__ void __launch_bounds__(256, 3) k_rows12(uint32_t* __restrict__ x, con
                         red(v[0][4 * q + 3], f.p));
     return;
   }
-  bf_group<4, 4, true, 1>(v, pt.inv, 0, f);
-#pragma unroll
-  for (int i = 0; i < 16; ++i) sX[swz12(posC(t, i))] = v[0][i];
+  bf_group<4, 4, true, 1, true>(v, pt.inv, 0, f);
+  sts16(sX + bC, v[0]);
   __syncthreads();
 #pragma unroll
-  for (int i = 0; i < 16; ++i) v[0][i] = sX[swz12(posB(t, i))];
+  for (int i = 0; i < 16; ++i) v[0][i] = sX[bB + offB(i)];
   bf_group<4, 8, true, 1>(v, pt.inv, t & 15, f);
 #pragma unroll
-  for (int i = 0; i < 16; ++i) sX[swz12(posB(t, i))] = v[0][i];
+  for (int i = 0; i < 16; ++i) sX[bB + offB(i)] = v[0][i];
   __syncthreads();
 #pragma unroll
-  for (int i = 0; i < 16; ++i) v[0][i] = sX[swz12(posA(t, i))];
+  for (int i = 0; i < 16; ++i) v[0][i] = sX[bA + offA(i)];
   bf_group<4, 12, true, 1>(v, pt.inv, t, f);
 #pragma unroll
   for (int i = 0; i < 16; ++i) x[row + posA(t, i)] = v[0][i];
+}
+
+__global__ void __launch_bounds__(256, 3) k_rows12(uint32_t* __restrict__ x, const uint32_t* __restrict__ y,
+                                                  int ymode, uint32_t* __restrict__ y_spec_out, int forward,
+                                                  int inverse, Ptab pt) {
+  rows12_body(x, y, ymode, y_spec_out, forward, inverse, pt, blockIdx.x);
 }
 
 template <int LOGR>
@@ -813,6 +886,8 @@ struct ColCfg {
   static constexpr int TE = 1 << (LOGR + LOGW);
   static constexpr int K = ColGroups<LOGR>::K;
   static constexpr int GL = ColGroups<LOGR>::size(K - 1);
+  using P = ColSwz<LOGR, LOGW, GL>;
+  static constexpr int SMEM_WORDS = TE;
 };
 
 // Loads the W x R column tile (rows t, columns j0..j0+W) into shared memory
@@ -823,7 +898,7 @@ __device__ __forceinline__ void col_tile_load(uint32_t* sm, const uint32_t* src,
                                               int tid) {
   using C = ColCfg<LOGR>;
   if (src == nullptr || count == 0) {
-    for (int e = tid; e < C::TE; e += 256) sm[e] = 0u;
+    for (int e = tid; e < C::SMEM_WORDS; e += 256) sm[e] = 0u;
     return;
   }
   if (((uintptr_t)src & 15u) == 0) {
@@ -833,7 +908,7 @@ __device__ __forceinline__ void col_tile_load(uint32_t* sm, const uint32_t* src,
       const int t = q / CPR, cc = (q % CPR) * 4;
       const uint32_t gi = ((uint32_t)t << logC) + j0 + cc;
       const int valid = gi < count ? (int)min(4u, count - gi) : 0;
-      cp_async16(sm + swz_col<LOGR, C::LOGW, C::GL>((t << C::LOGW) + cc), src + (valid ? gi : 0), valid * 4);
+      cp_async16(sm + C::P::at((t << C::LOGW) + cc), src + (valid ? gi : 0), valid * 4);
     }
   } else {
 #pragma unroll 4
@@ -841,7 +916,7 @@ __device__ __forceinline__ void col_tile_load(uint32_t* sm, const uint32_t* src,
       const int t = e >> C::LOGW, c = e & (C::W - 1);
       const uint32_t gi = ((uint32_t)t << logC) + j0 + c;
       const bool v = gi < count;
-      cp_async4(sm + swz_col<LOGR, C::LOGW, C::GL>(e), src + (v ? gi : 0), v ? 4 : 0);
+      cp_async4(sm + C::P::at(e), src + (v ? gi : 0), v ? 4 : 0);
     }
   }
   cp_async_wait_all();
@@ -865,12 +940,12 @@ __device__ __forceinline__ void col_group_smem(uint32_t* sm, const uint2* tw, co
     uint32_t v[2][1 << G];
 #pragma unroll
     for (int i = 0; i < (1 << G); ++i) {
-      const uint32_t x = sm[swz_col<LOGR, C::LOGW, C::GL>(((p0 + (i << S)) << C::LOGW) + c)];
+      const uint32_t x = sm[C::P::at(((p0 + (i << S)) << C::LOGW) + c)];
       v[0][i] = REDUCE ? reduce_any(x, q1, f) : x;
     }
     bf_group<G, T, INV, 1>(v, tw, base, f);
 #pragma unroll
-    for (int i = 0; i < (1 << G); ++i) sm[swz_col<LOGR, C::LOGW, C::GL>(((p0 + (i << S)) << C::LOGW) + c)] = v[0][i];
+    for (int i = 0; i < (1 << G); ++i) sm[C::P::at(((p0 + (i << S)) << C::LOGW) + c)] = v[0][i];
   }
 }
 
@@ -896,15 +971,13 @@ __device__ __forceinline__ void col_inv_groups(uint32_t* sm, const Ptab& pt, int
 }
 
 template <int LOGR>
-__global__ void __launch_bounds__(256, 3) k_colfwd_t(ColOps ops, BigD bt, Ptab pt) {
+__device__ __forceinline__ void colfwd_body(const InD& in, uint32_t* __restrict__ out, const BigD& bt, const Ptab& pt) {
   using C = ColCfg<LOGR>;
   constexpr int K = ColGroups<LOGR>::K;
   constexpr int G = C::GL;
   extern __shared__ uint32_t sm[];
   const int tid = threadIdx.x, logC = bt.logC;
   const int j0 = blockIdx.x << C::LOGW;
-  const InD in = blockIdx.y == 0 ? ops.in[0] : (blockIdx.y == 1 ? ops.in[1] : ops.in[2]);
-  uint32_t* out = blockIdx.y == 0 ? ops.out[0] : (blockIdx.y == 1 ? ops.out[1] : ops.out[2]);
   const Fp f = pt.f;
   col_tile_load<LOGR>(sm, in.ptr, in.count, j0, logC, tid);
   __syncthreads();
@@ -920,10 +993,10 @@ __global__ void __launch_bounds__(256, 3) k_colfwd_t(ColOps ops, BigD bt, Ptab p
     uint32_t v[2][1 << G];
 #pragma unroll
     for (int i = 0; i < (1 << G); ++i) {
-      const uint32_t x = sm[swz_col<LOGR, C::LOGW, C::GL>(((p0 + i) << C::LOGW) + c)];
+      const uint32_t x = sm[C::P::at(((p0 + i) << C::LOGW) + c)];
       v[0][i] = reduce_here ? reduce_any(x, pt.q1, f) : x;
     }
-    bf_group<G, G, false, 1>(v, pt.fwd, 0, f);
+    bf_group<G, G, false, 1, true>(v, pt.fwd, 0, f);
     const uint32_t j = j0 + c;
     const uint32_t eb = j * brev_c(b, LOGR - G);
     const uint32_t js = j << (LOGR - G);
@@ -937,7 +1010,15 @@ __global__ void __launch_bounds__(256, 3) k_colfwd_t(ColOps ops, BigD bt, Ptab p
 }
 
 template <int LOGR>
-__global__ void __launch_bounds__(256, 3) k_colinv_t(const uint32_t* __restrict__ in, BigD bt, Ptab pt, EpiD epi) {
+__global__ void __launch_bounds__(256, 3) k_colfwd_t(ColOps ops, BigD bt, Ptab pt) {
+  const InD in = blockIdx.y == 0 ? ops.in[0] : (blockIdx.y == 1 ? ops.in[1] : ops.in[2]);
+  uint32_t* out = blockIdx.y == 0 ? ops.out[0] : (blockIdx.y == 1 ? ops.out[1] : ops.out[2]);
+  colfwd_body<LOGR>(in, out, bt, pt);
+}
+
+template <int LOGR>
+__device__ __forceinline__ void colinv_body(const uint32_t* __restrict__ in, const BigD& bt, const Ptab& pt,
+                                            const EpiD& epi) {
   using C = ColCfg<LOGR>;
   constexpr int K = ColGroups<LOGR>::K;
   extern __shared__ uint32_t sm[];
@@ -962,16 +1043,16 @@ __global__ void __launch_bounds__(256, 3) k_colinv_t(const uint32_t* __restrict_
 #pragma unroll
       for (int i = 0; i < (1 << G); ++i) {
         const uint32_t ex = eb + js * brev_c(i, G);
-        uint32_t w = shoup(sm[swz_col<LOGR, C::LOGW, C::GL>(((p0 + i) << C::LOGW) + c)], __ldg(bt.lo + (ex & 4095u)), f.p);
+        uint32_t w = shoup(sm[C::P::at(((p0 + i) << C::LOGW) + c)], __ldg(bt.lo + (ex & 4095u)), f.p);
         v[0][i] = shoup(w, __ldg(bt.hi + (ex >> 12)), f.p);
       }
-      bf_group<G, G, true, 1>(v, pt.inv, 0, f);
+      bf_group<G, G, true, 1, true>(v, pt.inv, 0, f);
       if constexpr (K == 1) {
 #pragma unroll
         for (int i = 0; i < (1 << G); ++i) epi_store(epi, (uint32_t)(((p0 + i) << logC) + j), v[0][i], f);
       } else {
 #pragma unroll
-        for (int i = 0; i < (1 << G); ++i) sm[swz_col<LOGR, C::LOGW, C::GL>(((p0 + i) << C::LOGW) + c)] = v[0][i];
+        for (int i = 0; i < (1 << G); ++i) sm[C::P::at(((p0 + i) << C::LOGW) + c)] = v[0][i];
       }
     }
   }
@@ -988,7 +1069,7 @@ __global__ void __launch_bounds__(256, 3) k_colinv_t(const uint32_t* __restrict_
       const int base = inst >> C::LOGW;
       uint32_t v[2][1 << G];
 #pragma unroll
-      for (int i = 0; i < (1 << G); ++i) v[0][i] = sm[swz_col<LOGR, C::LOGW, C::GL>(((base + (i << S)) << C::LOGW) + c)];
+      for (int i = 0; i < (1 << G); ++i) v[0][i] = sm[C::P::at(((base + (i << S)) << C::LOGW) + c)];
       bf_group<G, LOGR, true, 1>(v, pt.inv, base, f);
 #pragma unroll
       for (int i = 0; i < (1 << G); ++i) epi_store(epi, (uint32_t)(((base + (i << S)) << logC) + j0 + c), v[0][i], f);
@@ -997,7 +1078,12 @@ __global__ void __launch_bounds__(256, 3) k_colinv_t(const uint32_t* __restrict_
 }
 
 template <int LOGR>
-int col_smem_bytes() { return ColCfg<LOGR>::TE * 4; }
+__global__ void __launch_bounds__(256, 3) k_colinv_t(const uint32_t* __restrict__ in, BigD bt, Ptab pt, EpiD epi) {
+  colinv_body<LOGR>(in, bt, pt, epi);
+}
+
+template <int LOGR>
+int col_smem_bytes() { return ColCfg<LOGR>::SMEM_WORDS * 4; }
 
 using ColFwdFn = void (*)(ColOps, BigD, Ptab);
 using ColInvFn = void (*)(const uint32_t*, BigD, Ptab, EpiD);
@@ -1016,7 +1102,7 @@ struct ColTable {
   }
   static int words(int logR) {
     int r = 0;
-    ((logR == L ? (r = ColCfg<L>::TE, 0) : 0), ...);
+    ((logR == L ? (r = ColCfg<L>::SMEM_WORDS, 0) : 0), ...);
     return r;
   }
   static int logw(int logR) {
@@ -1030,8 +1116,8 @@ struct ColTable {
       const cudaError_t r = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
       if (r != cudaSuccess) e = r;
     };
-    (set((const void*)k_colfwd_t<L>, ColCfg<L>::TE * 4), ...);
-    (set((const void*)k_colinv_t<L>, ColCfg<L>::TE * 4), ...);
+    (set((const void*)k_colfwd_t<L>, ColCfg<L>::SMEM_WORDS * 4), ...);
+    (set((const void*)k_colinv_t<L>, ColCfg<L>::SMEM_WORDS * 4), ...);
     return e;
   }
 };
@@ -1080,4 +1166,465 @@ cudaError_t launch_rows(const PrimeTables& pt, const BigTables& bt, uint32_t* x,
   return cudaGetLastError();
 }
 
+}  // namespace fpx
+
+// ===========================================================================
+// Batched execution: many independent products per launch.  Each CTA reads its
+// job's descriptor (prime tables, operands, scratch, epilogue) from device
+// memory, so one launch covers any mix of primes and polynomials of the same
+// transform size; different sizes go to different launches.
+// ===========================================================================
+namespace {
+
+struct SmallJobB {
+  SmallD d;
+  Ptab pt;
+};
+struct BigJobB {
+  Ptab pt;
+  BigD bf, bi;
+  InD in[2];
+  uint32_t* t[2];
+  int nops, ymode;
+  const uint32_t* yspec;
+  uint32_t* yspec_out;
+  EpiD epi;
+};
+struct DirectJobB {
+  uint32_t p;
+  Fp f;
+  const uint32_t* a;
+  int la;
+  const uint32_t* b;
+  size_t lb, off, cnt;
+  uint32_t* out;
+  int accumulate;
+  const uint32_t* post_mont;
+  int negate;
+};
+struct GarnerJobB {
+  GarnerC g;
+  int primes;
+  const uint32_t *c1, *c2, *c3;
+  uint32_t* out;
+  size_t n;
+  int accumulate;
+  const uint32_t* post_mont;
+  int negate;
+  uint32_t tpinv;
+};
+
+__global__ void __launch_bounds__(512) k_small_b(const SmallJobB* __restrict__ jobs, int logN) {
+  const SmallJobB& j = jobs[blockIdx.x];
+  small_body(j.d, j.pt, logN);
+}
+
+template <int LOGR>
+__global__ void __launch_bounds__(256, 3) k_colfwd_b(const BigJobB* __restrict__ jobs) {
+  const BigJobB& j = jobs[blockIdx.z];
+  if ((int)blockIdx.y >= j.nops) return;
+  colfwd_body<LOGR>(j.in[blockIdx.y], j.t[blockIdx.y], j.bf, j.pt);
+}
+
+__global__ void __launch_bounds__(256, 3) k_rows12_b(const BigJobB* __restrict__ jobs) {
+  const BigJobB& j = jobs[blockIdx.y];
+  rows12_body(j.t[0], j.ymode == 1 ? j.t[1] : j.yspec, j.ymode, j.yspec_out, 1, 1, j.pt, blockIdx.x);
+}
+
+template <int LOGR>
+__global__ void __launch_bounds__(256, 3) k_colinv_b(const BigJobB* __restrict__ jobs) {
+  const BigJobB& j = jobs[blockIdx.y];
+  colinv_body<LOGR>(j.t[0], j.bi, j.pt, j.epi);
+}
+
+__global__ void k_direct_b(const DirectJobB* __restrict__ jobs) {
+  const DirectJobB& j = jobs[blockIdx.y];
+  direct_body(j.p, j.f, j.a, j.la, j.b, j.lb, j.off, j.cnt, j.out, j.accumulate, j.post_mont, j.negate);
+}
+
+// Newton seeds for many jobs (k_seed per block): blockIdx.x = job.
+struct SeedJobB {
+  int kind;
+  uint32_t p;
+  const uint32_t* a;
+  size_t la;
+  uint32_t* out;
+  int n;
+  uint32_t r0;
+};
+__global__ void k_seed_b(const SeedJobB* __restrict__ jobs) {
+  const SeedJobB& j = jobs[blockIdx.x];
+  seed_body(j.kind, j.p, j.a, j.la, j.out, j.n, j.r0);
+}
+
+__global__ void k_garner_b(const GarnerJobB* __restrict__ jobs) {
+  const GarnerJobB& j = jobs[blockIdx.y];
+  garner_body(j.g, j.primes, j.c1, j.c2, j.c3, j.out, j.n, j.accumulate, j.post_mont, j.negate, j.tpinv);
+}
+
+using BatchFn = void (*)(const BigJobB*);
+
+template <int... L>
+struct ColBatch {
+  static BatchFn fwd(int logR) {
+    BatchFn r = nullptr;
+    ((logR == L ? (r = k_colfwd_b<L>, 0) : 0), ...);
+    return r;
+  }
+  static BatchFn inv(int logR) {
+    BatchFn r = nullptr;
+    ((logR == L ? (r = k_colinv_b<L>, 0) : 0), ...);
+    return r;
+  }
+  static cudaError_t launch(int logR, dim3 grid, const BigJobB* jobs, int smem, cudaStream_t s) {
+    BatchFn fn = fwd(logR);
+    if (!fn) return cudaErrorInvalidValue;
+    fn<<<grid, 256, smem, s>>>(jobs);
+    return cudaGetLastError();
+  }
+  static cudaError_t launch_inv(int logR, dim3 grid, const BigJobB* jobs, int smem, cudaStream_t s) {
+    BatchFn fn = inv(logR);
+    if (!fn) return cudaErrorInvalidValue;
+    fn<<<grid, 256, smem, s>>>(jobs);
+    return cudaGetLastError();
+  }
+  static cudaError_t init() {
+    cudaError_t e = cudaSuccess;
+    auto set = [&](const void* fn, int bytes) {
+      const cudaError_t r = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+      if (r != cudaSuccess) e = r;
+    };
+    (set((const void*)k_colfwd_b<L>, ColCfg<L>::SMEM_WORDS * 4), ...);
+    (set((const void*)k_colinv_b<L>, ColCfg<L>::SMEM_WORDS * 4), ...);
+    set((const void*)k_small_b, 2 * padded_words(1 << kSmallLog) * 4);
+    return e;
+  }
+};
+using ColsB = ColBatch<2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12>;
+
+
+GarnerC garner_consts(uint32_t target) {
+  const uint64_t P1 = 167772161u, P2 = 469762049u, P3 = 754974721u;
+  auto powm = [](uint64_t a, uint64_t e, uint64_t m) {
+    uint64_t r = 1 % m;
+    a %= m;
+    for (; e; e >>= 1, a = a * a % m)
+      if (e & 1) r = r * a % m;
+    return r;
+  };
+  GarnerC g;
+  g.P1 = (uint32_t)P1; g.P2 = (uint32_t)P2; g.P3 = (uint32_t)P3;
+  g.inv12 = shoup_const((uint32_t)powm(P1 % P2, P2 - 2, P2), (uint32_t)P2);
+  g.p1_in3 = shoup_const((uint32_t)(P1 % P3), (uint32_t)P3);
+  g.inv123 = shoup_const((uint32_t)powm((P1 * P2) % P3, P3 - 2, P3), (uint32_t)P3);
+  g.t = target;
+  g.t_q1 = (uint32_t)((((uint64_t)1) << 32) / target);
+  g.p1_t = shoup_const((uint32_t)(P1 % target), target);
+  g.p12_t = shoup_const((uint32_t)((P1 * P2) % target), target);
+  return g;
+}
+
+struct BatchGroup {
+  int logN;
+  bool big;
+  size_t off;
+  int count;
+};
+inline size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
+
+}  // namespace
+
+namespace fpx {
+
+cudaError_t kernels_batch_init() { return ColsB::init(); }
+
+size_t batch_descriptor_bytes(const BatchPlan& b) {
+  return b.xjobs.size() * std::max(sizeof(SmallJobB), sizeof(BigJobB)) + b.direct.size() * sizeof(DirectJobB) +
+         b.garner.size() * sizeof(GarnerJobB) + 256 * 40;  // every section starts 256-byte aligned
+}
+
+cudaError_t launch_batch(const BatchPlan& b, void* host_staging, void* dev_desc, cudaStream_t s,
+                         cudaEvent_t staged) {
+  // Layout: [small jobs by logN][big jobs by logN][direct][garner], each section 256-byte aligned.
+  std::vector<int> order;
+  order.reserve(b.xjobs.size());
+  for (int lg = 0; lg <= 31; ++lg)  // stable bucket order by transform size
+    for (size_t i = 0; i < b.xjobs.size(); ++i)
+      if (b.xjobs[i].logN == lg) order.push_back((int)i);
+  char* h = static_cast<char*>(host_staging);
+  char* d = static_cast<char*>(dev_desc);
+  size_t off = 0;
+  std::vector<BatchGroup> groups;
+  for (size_t k = 0; k < order.size();) {
+    const int logN = b.xjobs[order[k]].logN;
+    size_t e = k;
+    while (e < order.size() && b.xjobs[order[e]].logN == logN) ++e;
+    const bool big = logN > kSmallLog;
+    off = align256(off);
+    BatchGroup grp;
+    grp.logN = logN;
+    grp.big = big;
+    grp.off = off;
+    grp.count = (int)(e - k);
+    groups.push_back(grp);
+    for (size_t q = k; q < e; ++q) {
+      const XJob& x = b.xjobs[order[q]];
+      const Ptab pt = dev_tab(*x.pt);
+      if (!big) {
+        SmallJobB j{};
+        j.pt = pt;
+        j.d.x = dev_in(x.x);
+        j.d.y = dev_in(x.y);
+        j.d.forward = 1;
+        j.d.ymode = x.ymode;
+        j.d.inverse = 1;
+        j.d.yspec = x.yspec;
+        j.d.yspec_out = x.yspec_out;
+        j.d.spec_x = nullptr;
+        j.d.epi = dev_epi(x.epi);
+        std::memcpy(h + off, &j, sizeof j);
+        off += sizeof j;
+      } else {
+        const BigTables& bt = *x.bt;
+        BigJobB j{};
+        j.pt = pt;
+        j.bf = BigD{bt.logR, bt.logC, Cols::logw(bt.logR), reinterpret_cast<const uint2*>(bt.lo_fwd),
+                    reinterpret_cast<const uint2*>(bt.hi_fwd)};
+        j.bi = BigD{bt.logR, bt.logC, Cols::logw(bt.logR),
+                    reinterpret_cast<const uint2*>(x.ymode != 0 ? bt.lo_inv_r : bt.lo_inv),
+                    reinterpret_cast<const uint2*>(bt.hi_inv)};
+        j.in[0] = dev_in(x.x);
+        j.in[1] = dev_in(x.y);
+        j.t[0] = x.t1;
+        j.t[1] = x.t2;
+        j.nops = x.ymode == 1 ? 2 : 1;
+        j.ymode = x.ymode;
+        j.yspec = x.yspec;
+        j.yspec_out = x.yspec_out;
+        j.epi = dev_epi(x.epi);
+        std::memcpy(h + off, &j, sizeof j);
+        off += sizeof j;
+      }
+    }
+    k = e;
+  }
+  off = align256(off);
+  const size_t off_direct = off;
+  for (const DirectJob& x : b.direct) {
+    DirectJobB j;
+    j.p = x.p;
+    if (x.p & 1u) {
+      j.f = make_fp(x.p);
+    } else {
+      j.f.p = x.p;
+      j.f.p2 = 2 * x.p;
+      j.f.pinv = 1;
+    }
+    j.a = x.a;
+    j.la = (int)x.la;
+    j.b = x.b;
+    j.lb = x.lb;
+    j.off = x.off;
+    j.cnt = x.cnt;
+    j.out = x.out;
+    j.accumulate = x.accumulate;
+    j.post_mont = x.post_mont;
+    j.negate = x.negate;
+    std::memcpy(h + off, &j, sizeof j);
+    off += sizeof j;
+  }
+  off = align256(off);
+  const size_t off_garner = off;
+  for (const GarnerJob& x : b.garner) {
+    GarnerJobB j;
+    j.g = garner_consts(x.target);
+    j.primes = x.primes;
+    j.c1 = x.c1;
+    j.c2 = x.c2;
+    j.c3 = x.c3;
+    j.out = x.out;
+    j.n = x.n;
+    j.accumulate = x.accumulate;
+    j.post_mont = x.post_mont;
+    j.negate = x.negate;
+    j.tpinv = 1u;
+    if (x.target & 1u) j.tpinv = inv_mod_2_32(x.target);
+    std::memcpy(h + off, &j, sizeof j);
+    off += sizeof j;
+  }
+  if (off == 0) return cudaSuccess;
+  cudaError_t e = cudaMemcpyAsync(d, h, off, cudaMemcpyHostToDevice, s);
+  if (e != cudaSuccess) return e;
+  if (staged && (e = cudaEventRecord(staged, s)) != cudaSuccess) return e;
+  // grid.y / grid.z hold at most 65535 jobs per launch
+  constexpr size_t kMaxY = 65535;
+  if (!b.direct.empty()) {
+    size_t maxcnt = 0;
+    for (const DirectJob& x : b.direct) maxcnt = std::max(maxcnt, x.cnt);
+    for (size_t k = 0; k < b.direct.size(); k += kMaxY) {
+      dim3 grid((unsigned)std::min<size_t>((maxcnt + 255) / 256, 1024),
+                (unsigned)std::min(kMaxY, b.direct.size() - k));
+      k_direct_b<<<grid, 256, 0, s>>>(reinterpret_cast<const DirectJobB*>(d + off_direct) + k);
+      if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    }
+  }
+  for (const BatchGroup& g : groups) {
+    const uint32_t N = 1u << g.logN;
+    if (!g.big) {
+      int nt = (int)(N / 16);
+      nt = nt < 32 ? 32 : (nt > 512 ? 512 : nt);
+      k_small_b<<<g.count, nt, 2 * padded_words(N) * 4, s>>>(reinterpret_cast<const SmallJobB*>(d + g.off), g.logN);
+      if ((e = cudaGetLastError()) != cudaSuccess) return e;
+      continue;
+    }
+    const int logC = 12, logR = g.logN - logC;
+    const int logW = Cols::logw(logR);
+    const int smem = Cols::words(logR) * 4;
+    for (size_t k = 0; k < (size_t)g.count; k += kMaxY) {
+      const BigJobB* jobs = reinterpret_cast<const BigJobB*>(d + g.off) + k;
+      const unsigned cnt = (unsigned)std::min(kMaxY, (size_t)g.count - k);
+      e = ColsB::launch(logR, dim3(1u << (logC - logW), 2, cnt), jobs, smem, s);
+      if (e != cudaSuccess) return e;
+      k_rows12_b<<<dim3(1u << logR, cnt), 256, 0, s>>>(jobs);
+      if ((e = cudaGetLastError()) != cudaSuccess) return e;
+      e = ColsB::launch_inv(logR, dim3(1u << (logC - logW), cnt), jobs, smem, s);
+      if (e != cudaSuccess) return e;
+    }
+  }
+  if (!b.garner.empty()) {
+    size_t maxn = 0;
+    for (const GarnerJob& x : b.garner) maxn = std::max(maxn, x.n);
+    for (size_t k = 0; k < b.garner.size(); k += kMaxY) {
+      dim3 grid((unsigned)std::min<size_t>((maxn + 255) / 256, 1024), (unsigned)std::min(kMaxY, b.garner.size() - k));
+      k_garner_b<<<grid, 256, 0, s>>>(reinterpret_cast<const GarnerJobB*>(d + off_garner) + k);
+      if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    }
+  }
+  return cudaSuccess;
+}
+
+}  // namespace fpx
+
+namespace fpx {
+
+cudaError_t launch_seeds_batch(const std::vector<SeedJob>& jobs, void* host_staging, void* dev_desc, cudaStream_t s,
+                               cudaEvent_t staged) {
+  if (jobs.empty()) return cudaSuccess;
+  std::vector<SeedJobB> v;
+  v.reserve(jobs.size());
+  for (const SeedJob& x : jobs) v.push_back(SeedJobB{x.kind, x.p, x.a, x.la, x.out, x.n, x.r0});
+  std::memcpy(host_staging, v.data(), v.size() * sizeof(SeedJobB));
+  cudaError_t e = cudaMemcpyAsync(dev_desc, host_staging, v.size() * sizeof(SeedJobB), cudaMemcpyHostToDevice, s);
+  if (e != cudaSuccess) return e;
+  if (staged && (e = cudaEventRecord(staged, s)) != cudaSuccess) return e;
+  k_seed_b<<<(unsigned)v.size(), 32, 0, s>>>(static_cast<const SeedJobB*>(dev_desc));
+  return cudaGetLastError();
+}
+
+cudaError_t launch_exp_prep_batch(const std::vector<ExpPrep>& jobs, void* host_staging, void* dev_desc,
+                                  cudaStream_t s, cudaEvent_t staged) {
+  if (jobs.empty()) return cudaSuccess;
+  std::vector<ExpPrepB> v;
+  size_t maxn = 0;
+  for (const ExpPrep& x : jobs) {
+    const uint32_t r = (uint32_t)((((uint64_t)1) << 32) % x.p);
+    v.push_back(ExpPrepB{make_fp(x.p), (uint32_t)((((uint64_t)1) << 32) / x.p), shoup_const(r, x.p), x.a, x.cnt,
+                         x.ap, x.out, x.n, x.out0});
+    maxn = std::max(maxn, x.n);
+  }
+  std::memcpy(host_staging, v.data(), v.size() * sizeof(ExpPrepB));
+  cudaError_t e = cudaMemcpyAsync(dev_desc, host_staging, v.size() * sizeof(ExpPrepB), cudaMemcpyHostToDevice, s);
+  if (e != cudaSuccess) return e;
+  if (staged && (e = cudaEventRecord(staged, s)) != cudaSuccess) return e;
+  dim3 grid((unsigned)std::min<size_t>((maxn + 255) / 256, 256), (unsigned)v.size());
+  k_exp_prep_b<<<grid, 256, 0, s>>>(static_cast<const ExpPrepB*>(dev_desc));
+  return cudaGetLastError();
+}
+
+size_t batch_aux_bytes(size_t jobs) { return jobs * std::max(sizeof(SeedJobB), sizeof(ExpPrepB)) + 256; }
+
+}  // namespace fpx
+
+namespace {
+__global__ void k_gather_first(const uint32_t* const* __restrict__ ptrs, uint32_t* __restrict__ out, int n) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) out[i] = ptrs[i] ? *ptrs[i] : 0u;
+}
+
+struct ReprSegB {
+  Fp f;
+  uint2 r_sh;  // 2^32 mod p as a Shoup constant
+  uint32_t* ptr;
+  size_t n;
+  int to_mont;
+};
+__global__ void k_repr_b(const ReprSegB* __restrict__ segs) {
+  const ReprSegB& g = segs[blockIdx.y];
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < g.n; i += (size_t)gridDim.x * blockDim.x) {
+    const uint32_t x = g.ptr[i];
+    uint32_t y;
+    if (g.f.p == 2) y = x & 1u;
+    else if (g.to_mont) y = redc_any(shoup(x, g.r_sh, g.f.p), g.f.p);
+    else y = red(mont(x, 1u, g.f), g.f.p);
+    g.ptr[i] = y;
+  }
+}
+}  // namespace
+
+namespace fpx {
+size_t repr_batch_bytes(size_t segs) { return segs * sizeof(ReprSegB) + 256; }
+
+cudaError_t launch_repr_batch(const std::vector<ReprSeg>& segs, void* host_staging, void* dev_desc, cudaStream_t s,
+                              cudaEvent_t staged) {
+  std::vector<ReprSegB> v;
+  size_t maxn = 0;
+  for (const ReprSeg& x : segs) {
+    if (x.n == 0) continue;
+    ReprSegB b{};
+    if (x.p == 2) {
+      b.f.p = 2;
+      b.f.p2 = 4;
+      b.f.pinv = 1;
+    } else {
+      b.f = make_fp(x.p);
+      b.r_sh = shoup_const((uint32_t)((((uint64_t)1) << 32) % x.p), x.p);
+    }
+    b.ptr = x.ptr;
+    b.n = x.n;
+    b.to_mont = x.to_mont;
+    v.push_back(b);
+    maxn = std::max(maxn, x.n);
+  }
+  if (v.empty()) return cudaSuccess;
+  std::memcpy(host_staging, v.data(), v.size() * sizeof(ReprSegB));
+  cudaError_t e = cudaMemcpyAsync(dev_desc, host_staging, v.size() * sizeof(ReprSegB), cudaMemcpyHostToDevice, s);
+  if (e != cudaSuccess) return e;
+  if (staged && (e = cudaEventRecord(staged, s)) != cudaSuccess) return e;
+  for (size_t k = 0; k < v.size(); k += 65535) {  // grid.y limit
+    const unsigned cnt = (unsigned)std::min<size_t>(65535, v.size() - k);
+    dim3 grid((unsigned)std::min<size_t>((maxn + 255) / 256, 128), cnt);
+    k_repr_b<<<grid, 256, 0, s>>>(static_cast<const ReprSegB*>(dev_desc) + k);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+}  // namespace fpx
+
+namespace fpx {
+// out_host[i] = *ptrs[i] (0 for null) for many device pointers: one H2D of the
+// pointer list, one kernel, one D2H; the caller synchronises the stream.
+cudaError_t launch_gather_first(const std::vector<const uint32_t*>& ptrs, void* host_staging, void* dev_buf,
+                                uint32_t* host_out, cudaStream_t s) {
+  if (ptrs.empty()) return cudaSuccess;
+  const size_t bytes = ptrs.size() * sizeof(void*);
+  std::memcpy(host_staging, ptrs.data(), bytes);
+  char* d = static_cast<char*>(dev_buf);
+  cudaError_t e = cudaMemcpyAsync(d, host_staging, bytes, cudaMemcpyHostToDevice, s);
+  if (e != cudaSuccess) return e;
+  uint32_t* dout = reinterpret_cast<uint32_t*>(d + ((bytes + 255) & ~size_t(255)));
+  k_gather_first<<<(unsigned)((ptrs.size() + 255) / 256), 256, 0, s>>>(reinterpret_cast<const uint32_t* const*>(d),
+                                                                         dout, (int)ptrs.size());
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  return cudaMemcpyAsync(host_out, dout, ptrs.size() * 4, cudaMemcpyDeviceToHost, s);
+}
 }  // namespace fpx

@@ -120,3 +120,97 @@ cudaError_t launch_sqrt_char2(const uint32_t* a, size_t cnt, uint32_t* out, unsi
 cudaError_t launch_mul_mont_tab(uint32_t p, const uint32_t* a, const uint32_t* tab, uint32_t* out, size_t n,
                                 cudaStream_t s);
 }  // namespace fpx
+
+#include <vector>
+namespace fpx {
+// ---- batched execution --------------------------------------------------------
+// One cyclic product of size 2^logN on a native prime (logN <= 13: one CTA per
+// job; 14 <= logN <= 23: the two-pass kernels with t1/t2 as N-word scratch).
+// ymode as in SmallJob; the inverse always runs; epi.scale must already hold
+// the full inverse scale for one-CTA jobs (1/N, times 2^32 after a product).
+struct XJob {
+  const PrimeTables* pt = nullptr;
+  const BigTables* bt = nullptr;
+  int logN = 0;
+  InOp x, y;
+  int ymode = 0;
+  const uint32_t* yspec = nullptr;
+  uint32_t* yspec_out = nullptr;
+  uint32_t *t1 = nullptr, *t2 = nullptr;
+  Epi epi;
+};
+// out[i] = (+)= [-] (sum_j a[j] b[i+off-j]) [* post_mont[i]], i < cnt
+struct DirectJob {
+  uint32_t p;
+  const uint32_t* a;  // the short operand (<= 40 terms)
+  size_t la;
+  const uint32_t* b;
+  size_t lb, off, cnt;
+  uint32_t* out;
+  int accumulate = 0;
+  const uint32_t* post_mont = nullptr;
+  int negate = 0;
+};
+struct GarnerJob {
+  uint32_t target;
+  int primes;
+  const uint32_t *c1, *c2, *c3;
+  uint32_t* out;
+  size_t n;
+  int accumulate = 0;
+  const uint32_t* post_mont = nullptr;  // Montgomery table, odd target only
+  int negate = 0;
+};
+struct BatchPlan {
+  std::vector<XJob> xjobs;
+  std::vector<DirectJob> direct;
+  std::vector<GarnerJob> garner;  // run after every xjob
+};
+size_t batch_descriptor_bytes(const BatchPlan& b);
+// Serialises the descriptors into host_staging (pinned, batch_descriptor_bytes),
+// copies them to dev_desc and launches: direct jobs, then one launch set per
+// transform size, then the Garner reconstructions.
+cudaError_t launch_batch(const BatchPlan& b, void* host_staging, void* dev_desc, cudaStream_t s,
+                         cudaEvent_t staged = nullptr);
+// Newton seeds (kind as launch_seed) and exp preparations for many jobs at once.
+struct SeedJob {
+  int kind;
+  uint32_t p;
+  const uint32_t* a;
+  size_t la;
+  uint32_t* out;
+  int n;
+  uint32_t r0;
+};
+struct ExpPrep {
+  uint32_t p;          // odd
+  const uint32_t* a;
+  size_t cnt;          // min(la, n)
+  uint32_t* ap;        // cnt - 1 words: a'
+  uint32_t* out;       // n words: out0, 0, 0, ...
+  size_t n;
+  uint32_t out0 = 1;   // 1 for exp, 0 for log
+};
+size_t batch_aux_bytes(size_t jobs);
+cudaError_t launch_seeds_batch(const std::vector<SeedJob>& jobs, void* host_staging, void* dev_desc, cudaStream_t s,
+                               cudaEvent_t staged = nullptr);
+cudaError_t launch_exp_prep_batch(const std::vector<ExpPrep>& jobs, void* host_staging, void* dev_desc,
+                                  cudaStream_t s, cudaEvent_t staged = nullptr);
+cudaError_t kernels_batch_init();
+}  // namespace fpx
+namespace fpx {
+// In-place representation change of many arrays: Montgomery limbs -> canonical
+// (to_mont = 0) or back (to_mont = 1); p = 2 keeps the bit.
+struct ReprSeg {
+  uint32_t p;
+  uint32_t* ptr;
+  size_t n;
+  int to_mont;
+};
+size_t repr_batch_bytes(size_t segs);
+cudaError_t launch_repr_batch(const std::vector<ReprSeg>& segs, void* host_staging, void* dev_desc, cudaStream_t s,
+                              cudaEvent_t staged = nullptr);
+// host_out[i] = *ptrs[i]; dev_buf needs ptrs.size() * 12 + 256 bytes.
+cudaError_t launch_gather_first(const std::vector<const uint32_t*>& ptrs, void* host_staging, void* dev_buf,
+                                uint32_t* host_out, cudaStream_t s);
+}  // namespace fpx

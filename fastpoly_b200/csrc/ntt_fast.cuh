@@ -19,20 +19,20 @@ namespace fpx_dev {
 // mod s.  Forward: levels len = 2^LL .. 2^(LL-G+1); inverse: the reverse.
 // Twiddle index for level l, pair j: (len/2) + base + j*s.
 // ---------------------------------------------------------------------------
-template <int G, int LL, bool INV, int NA>
+template <int G, int LL, bool INV, int NA, bool ZB = false>
 __device__ __forceinline__ void bf_group(uint32_t (&x)[2][1 << G], const uint2* __restrict__ tw, int base,
                                          const Fp& f) {
+  // ZB: base == 0 (the last group of a transform), so every j == 0 twiddle is 1
+  // and its butterfly needs no multiplication.
   constexpr int E = 1 << G;
   constexpr int S = LL - G;
-  // all twiddles of the group up front: more loads in flight
-  uint2 w[E];  // w[hs + j] for level with pair distance hs (hs = 1, 2, 4, 8)
+  uint2 w[E];  // w[hs + j]: twiddle of pair j at the level with pair distance hs
 #pragma unroll
   for (int hs = 1; hs < E; hs <<= 1) {
-    // level with pair distance hs: len = 2^(S + log2(hs) + 1), half = 2^(S + log2 hs)
 #pragma unroll
     for (int j = 0; j < hs; ++j) {
-      const int half = hs << S;
-      w[hs + j] = __ldg(&tw[half + base + (j << S)]);
+      if (ZB && j == 0) continue;
+      w[hs + j] = __ldg(&tw[(hs << S) + base + (j << S)]);
     }
   }
   if (!INV) {
@@ -41,8 +41,12 @@ __device__ __forceinline__ void bf_group(uint32_t (&x)[2][1 << G], const uint2* 
 #pragma unroll
       for (int i = 0; i < E; ++i)
         if (!(i & hs)) {
+          const int j = i & (hs - 1);
 #pragma unroll
-          for (int a = 0; a < NA; ++a) dif_bf(x[a][i], x[a][i + hs], w[hs + (i & (hs - 1))], f);
+          for (int a = 0; a < NA; ++a) {
+            if (ZB && j == 0) dif_bf1(x[a][i], x[a][i + hs], f);
+            else dif_bf(x[a][i], x[a][i + hs], w[hs + j], f);
+          }
         }
     }
   } else {
@@ -51,8 +55,12 @@ __device__ __forceinline__ void bf_group(uint32_t (&x)[2][1 << G], const uint2* 
 #pragma unroll
       for (int i = 0; i < E; ++i)
         if (!(i & hs)) {
+          const int j = i & (hs - 1);
 #pragma unroll
-          for (int a = 0; a < NA; ++a) dit_bf(x[a][i], x[a][i + hs], w[hs + (i & (hs - 1))], f);
+          for (int a = 0; a < NA; ++a) {
+            if (ZB && j == 0) dit_bf1(x[a][i], x[a][i + hs], f);
+            else dit_bf(x[a][i], x[a][i + hs], w[hs + j], f);
+          }
         }
     }
   }
@@ -64,29 +72,40 @@ __device__ __forceinline__ uint32_t brev_c(uint32_t t, int logn) { return logn ?
 // Row pass, C = 2^12, 256 threads, 16 points per thread per group.
 //   group A: len 4096..512, thread t holds t + 256 i
 //   group B: len 256..32,   thread t holds 256 (t>>4) + (t&15) + 16 i
-//   group C: len 16..2,     thread t holds 16 t + i
-// smem word for row position a: a ^ g(a >> 5), g(r) = (r & 15) | ((r >> 3 & 1) << 4)
-// (conflict-free for all three patterns).
+//   group C: len 16..2,     thread t holds 16 t + i      (contiguous)
+// Padded layout pad12(a) = a + 4 (a >> 5) + 16 (a >> 8): every pattern is free
+// of bank conflicts, patterns A and B are a per-thread base plus compile-time
+// offsets (304 i and 16 i + 4 (i >> 1)), and pattern C stays contiguous, so it
+// moves with 128-bit accesses.
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ int swz12(int a) {
-  const int r = a >> 5;
-  return a ^ ((r & 15) | (((r >> 3) & 1) << 4));
-}
+constexpr int kRowWords = 4096 + 512 + 256;
+__device__ __forceinline__ int pad12(int a) { return a + 4 * (a >> 5) + 16 * (a >> 8); }
+__device__ __forceinline__ int baseA(int t) { return pad12(t); }
+__device__ __forceinline__ int baseB(int t) { return 304 * (t >> 4) + (t & 15); }
+__device__ __forceinline__ int baseC(int t) { return pad12(t << 4); }
+__host__ __device__ constexpr int offA(int i) { return 304 * i; }
+__host__ __device__ constexpr int offB(int i) { return 16 * i + 4 * (i >> 1); }
 __device__ __forceinline__ int posA(int t, int i) { return t + (i << 8); }
-__device__ __forceinline__ int posB(int t, int i) { return ((t >> 4) << 8) + (t & 15) + (i << 4); }
 __device__ __forceinline__ int posC(int t, int i) { return (t << 4) + i; }
 
 // Column pass tile: W = 2^LOGW adjacent columns x R = 2^LOGR rows, element
-// (row t, col c) at smem word a = t*W + c, swizzled for the last group's
-// pattern (instances one group-length apart): a ^ ((a >> (GL+LOGW)) & (32/W-1)) << LOGW.
+// (row t, col c) at smem word a = t*W + c, XOR-swizzled for the last group's
+// pattern (instances one group-length apart):
+//   a ^ (((a >> (GL+LOGW)) & (32/W - 1)) << LOGW).
+// A padded layout would make every offset a compile-time constant, but its
+// extra 1/8 of shared memory moves three resident CTAs past the 196 KB carveout
+// and halves the L1 left for the twiddle tables, which costs more than the
+// address arithmetic saves.
 template <int LOGR, int LOGW, int GL>
-__device__ __forceinline__ int swz_col(int a) {
-  if constexpr (GL + LOGW >= 5 && LOGW < 5) {
-    return a ^ (((a >> (GL + LOGW)) & ((32 >> LOGW) - 1)) << LOGW);
-  } else {
-    return a;
+struct ColSwz {
+  __host__ __device__ static constexpr int at(int a) {
+    if constexpr (GL + LOGW >= 5 && LOGW < 5) {
+      return a ^ (((a >> (GL + LOGW)) & ((32 >> LOGW) - 1)) << LOGW);
+    } else {
+      return a;
+    }
   }
-}
+};
 
 // Asynchronous global -> shared copies (cp.async), zero-filling past src_bytes.
 __device__ __forceinline__ void cp_async16(uint32_t* smem, const uint32_t* gmem, int src_bytes) {

@@ -37,7 +37,8 @@ enum fpx_status {
   FPX_ETIMEDOUT = 5,    /* a bounded device wait gave up */
   FPX_ECUDA = 6,        /* CUDA runtime error (see fpx_last_error_message) */
   FPX_EINVAL = 7,       /* bad argument (null pointer, modulus not prime < 2^31, ...) */
-  FPX_EUNSUPPORTED = 8  /* no usable CUDA device */
+  FPX_EUNSUPPORTED = 8, /* no usable CUDA device */
+  FPX_EPENDING = 9      /* fpx_serve_poll: the request has not completed yet */
 };
 
 enum fpx_repr { FPX_REPR_CANONICAL = 0, FPX_REPR_MONTGOMERY = 1 };
@@ -117,6 +118,96 @@ int fpx_div(fpx_ctx* ctx, uint32_t p, const uint32_t* a, size_t la, const uint32
             size_t* q_len, int repr);
 int fpx_mod(fpx_ctx* ctx, uint32_t p, const uint32_t* a, size_t la, const uint32_t* b, size_t lb, uint32_t* r,
             size_t* r_len, int repr);
+
+/* ---- batches (no counterpart in the reference, whose callers loop over the
+ *      single-operation functions above on one or more host threads) -----------
+ * One fpx_job per operation; the jobs are independent and may mix moduli and
+ * sizes.  Results, lengths and error conditions are those of the single-job
+ * functions, job by job.  The batch shares launches between jobs: all products
+ * of a stage run as one launch set per transform size (mixed primes and CRT
+ * lifts included), and the Newton loops of inv, log and exp advance in
+ * lockstep.  sqrt, pow and divmod jobs, and transforms past 2^23 points, run
+ * one after another inside the same call. */
+enum fpx_op {
+  FPX_OP_CONV = 0,   /* out = conv(a, b, n)                     (convolution.hpp:145) */
+  FPX_OP_INV = 1,    /* out = inv(a, n)                         (inverse.hpp:163) */
+  FPX_OP_LOG = 2,    /* out = log(a, n)                         (exponential.hpp:85) */
+  FPX_OP_EXP = 3,    /* out = exp(a, n)                         (exponential.hpp:107) */
+  FPX_OP_SQRT = 4,   /* out = sqrt(a, n)                        (square_root.hpp:12) */
+  FPX_OP_POW = 5,    /* out = pow(a, k, n)                      (power.hpp:17) */
+  FPX_OP_DIVMOD = 6  /* out = quotient, out2 = remainder        (division.hpp:86) */
+};
+
+typedef struct fpx_job {
+  int op;              /* enum fpx_op */
+  uint32_t p;          /* modulus: a prime 2 <= p < 2^31 */
+  const uint32_t* a;   /* first operand, la words */
+  size_t la;
+  const uint32_t* b;   /* conv: second factor; divmod: divisor (lb words) */
+  size_t lb;
+  uint64_t k;          /* pow: exponent */
+  size_t n;            /* conv: truncation (SIZE_MAX = full product); inv/log/exp/sqrt/pow: length */
+  uint32_t* out;       /* conv: min(la+lb-1, n) words; series: n words; divmod: quotient, la words */
+  uint32_t* out2;      /* divmod: remainder, lb words (NULL: not wanted) */
+  size_t out_len;      /* set: result length (conv, divmod quotient; n for series) */
+  size_t out2_len;     /* set: divmod remainder length */
+  int status;          /* set: this job's fpx status; nothing is written for a failed job */
+} fpx_job;
+
+/* Device pointers, canonical residues, queued on the context's stream.  Returns
+ * when every job's status and lengths are set (the domain checks of inv, log and
+ * exp read one word per job: one small device->host copy for the whole batch);
+ * the results are complete when the stream reaches the point of the call
+ * (fpx_batch_wait or fpx_ctx_synchronize).  Returns FPX_OK when every job
+ * succeeded, else the first failing job's status (or a CUDA / memory error for
+ * the whole batch). */
+int fpx_batch_submit(fpx_ctx* ctx, fpx_job* jobs, size_t count);
+int fpx_batch_wait(fpx_ctx* ctx);
+/* Host buffers (blocking): every input is packed into one pinned buffer and
+ * copied to the device at once, the batch runs, and every output comes back in
+ * one copy.  repr as for the single-job functions. */
+int fpx_batch_run(fpx_ctx* ctx, fpx_job* jobs, size_t count, int repr);
+
+/* ---- serving (no counterpart in the reference) --------------------------------
+ * A request loop on one GPU.  Requests are fpx_job records with HOST buffers;
+ * the job record and its buffers must stay valid until fpx_serve_poll reports
+ * completion.  Worker threads, each with its own stream and device pool, form
+ * micro-batches from whatever is queued when they become free (continuous
+ * batching): requests are admitted in arrival order while the sum of their
+ * planned device bytes (operands, results and transform scratch) fits the HBM
+ * budget (a request larger than the budget runs alone), and each micro-batch
+ * runs as fpx_batch_run.  Every request's result is the one the single-job
+ * function gives it, whatever it was batched with. */
+typedef struct fpx_serve_config {
+  size_t hbm_budget_bytes; /* planned device bytes per micro-batch; 0 = 8 GiB */
+  size_t max_batch_jobs;   /* 0 = 4096 */
+  int workers;             /* micro-batches in flight; 0 = 2 */
+  int repr;                /* FPX_REPR_CANONICAL or FPX_REPR_MONTGOMERY for every request */
+} fpx_serve_config;
+
+typedef struct fpx_serve_stats {
+  uint64_t submitted, completed, batches;
+  uint64_t max_batch_jobs_seen;     /* largest micro-batch formed */
+  uint64_t max_batch_bytes_seen;    /* largest planned device bytes admitted in one micro-batch */
+  uint64_t oversize_requests;       /* requests that alone exceeded the budget (ran alone) */
+} fpx_serve_stats;
+
+typedef struct fpx_server fpx_server;
+
+int fpx_serve_start(int device, const fpx_serve_config* cfg, fpx_server** out);
+/* Queues one request; *ticket identifies it for fpx_serve_poll. */
+int fpx_serve_submit(fpx_server* srv, fpx_job* job, uint64_t* ticket);
+/* wait = 0: returns FPX_EPENDING until the request is complete; wait != 0:
+ * blocks until it is.  When complete, returns the job's status (also in
+ * job->status) and, if latency_ns is not NULL, the time from submission to
+ * completion (results in the host buffers).  A ticket is released once its
+ * completion has been reported. */
+int fpx_serve_poll(fpx_server* srv, uint64_t ticket, int wait, uint64_t* latency_ns);
+int fpx_serve_stats_get(fpx_server* srv, fpx_serve_stats* out);
+/* Finishes every queued request, then stops the workers and frees the server. */
+int fpx_serve_stop(fpx_server* srv);
+/* Planned device bytes of one request (the admission measure), 0 for an invalid job. */
+size_t fpx_serve_plan_bytes(const fpx_job* job);
 
 /* ---- allocation-free convolution (no counterpart in the reference) ------------
  * For callers that cannot allocate device memory when they need a product: code

@@ -52,3 +52,29 @@ def test_null_context_rejected():
     lib = F.load_library()
     assert lib.fpx_ctx_destroy(None) == F.EINVAL
     assert lib.fpx_conv(None, 998244353, None, 0, None, 0, 0, None, None, 0) == F.EINVAL
+
+
+def test_job_struct_layout_matches_header(tmp_path):
+    """fastpoly_b200.Job (ctypes) has the layout of struct fpx_job in include/fpx_b200.h."""
+    import shutil
+    import subprocess
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no C compiler")
+    fields = [f for f, _ in F.Job._fields_]
+    src = tmp_path / "layout.c"
+    src.write_text("#include <stdio.h>\n#include <stddef.h>\n#include \"fpx_b200.h\"\nint main(void) {\n"
+                   "  printf(\"%zu\\n\", sizeof(fpx_job));\n"
+                   + "".join(f"  printf(\"%zu\\n\", offsetof(fpx_job, {f}));\n" for f in fields)
+                   + "  return 0;\n}\n")
+    exe = tmp_path / "layout"
+    subprocess.run([cc, "-I" + os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
+    got = [int(x) for x in subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split()]
+    assert got[0] == ctypes.sizeof(F.Job)
+    assert got[1:] == [getattr(F.Job, f).offset for f in fields]
+
+
+def test_batch_rejects_null_context():
+    lib = F.load_library()
+    assert lib.fpx_batch_run(None, None, 0, 0) == F.EINVAL
+    assert lib.fpx_batch_submit(None, None, 0) == F.EINVAL

@@ -1,0 +1,235 @@
+"""Parity of the batched path (fpx_batch_run / fpx_batch_submit) against the
+oracle and against the single-operation calls.
+
+A batch must give every job exactly the result, length and error the
+single-job function gives it, whatever else is in the batch: mixed moduli
+(native primes, CRT-only moduli, p = 2), mixed sizes (direct products, one-CTA
+and two-pass transforms), mixed operations, failing jobs next to good ones."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+import fastpoly_b200 as F
+from test_gpu_parity import eq, rnd
+from oracle.oracle import DomainError as OracleDomainError
+
+pytestmark = pytest.mark.gpu
+
+MODULI = [998244353, 167772161, 754974721, 1000000007, 2147483647, 7340033, 97, 2]
+
+
+def _oracle_job(O, jb):
+    op, p = jb[0], jb[1]
+    try:
+        if op == "conv":
+            return O.conv(p, jb[2], jb[3], None if len(jb) < 5 else jb[4])
+        if op == "pow":
+            return O.pow(p, jb[2], jb[3], jb[4])
+        if op == "divmod":
+            return O.divmod(p, jb[2], jb[3])
+        return getattr(O, op)(p, jb[2], jb[3])
+    except OracleDomainError as e:
+        return e
+
+
+def _check(res, want, what):
+    if isinstance(want, Exception):
+        assert isinstance(res, F.DomainError), (what, res)
+    elif isinstance(want, tuple):
+        assert not isinstance(res, Exception), (what, res)
+        eq(res[0], want[0], what + " q")
+        eq(res[1], want[1], what + " r")
+    else:
+        assert not isinstance(res, Exception), (what, res)
+        eq(res, want, what)
+
+
+def _conv_jobs(rng):
+    jobs = []
+    for p in MODULI:
+        for la, lb, n in [(1, 1, None), (3, 50, None), (40, 41, None), (41, 41, None), (100, 300, None),
+                          (1000, 1000, 1500), (3000, 5000, None), (4097, 4096, None), (20000, 30000, None),
+                          (70000, 1 << 16, 100000)]:
+            jobs.append(("conv", p, rnd(rng, p, la), rnd(rng, p, lb), n))
+    a = rnd(rng, 998244353, 5000)
+    jobs.append(("conv", 998244353, a, a, None))   # square
+    jobs.append(("conv", 998244353, a, a, 7))      # square, truncated
+    jobs.append(("conv", 1000000007, a, a, None))  # CRT square
+    jobs.append(("conv", 998244353, a, [], None))  # empty operand
+    jobs.append(("conv", 998244353, a, a, 0))      # n = 0
+    return jobs
+
+
+def test_batch_conv_mixed(fpx, oracle):
+    rng = np.random.default_rng(41)
+    jobs = _conv_jobs(rng)
+    res = fpx.batch(jobs)
+    for i, jb in enumerate(jobs):
+        _check(res[i], _oracle_job(oracle, jb), f"job {i} conv p={jb[1]} {len(jb[2])}x{len(jb[3])}")
+
+
+SERIES_N = [1, 2, 5, 31, 32, 33, 64, 100, 1000, 4096, 5000, 8193, 20000, 65536 + 3]
+
+
+@pytest.mark.parametrize("op", ["inv", "log", "exp"])
+def test_batch_series_mixed(fpx, oracle, op):
+    rng = np.random.default_rng({"inv": 1, "log": 2, "exp": 3}[op])
+    jobs = []
+    for p in [998244353, 167772161, 754974721, 1000000007, 7340033, 97]:
+        for n in SERIES_N:
+            if op == "log" and n > p:
+                continue
+            if op == "exp" and n - 1 >= p:
+                continue
+            for la in (1, 3, n + 7):
+                a = rnd(rng, p, la, nonzero0=True)
+                if op == "log":
+                    a[0] = 1
+                if op == "exp":
+                    a[0] = 0
+                jobs.append((op, p, a, n))
+    res = fpx.batch(jobs)
+    for i, jb in enumerate(jobs):
+        _check(res[i], _oracle_job(oracle, jb), f"job {i} {op} p={jb[1]} n={jb[3]} la={len(jb[2])}")
+
+
+def test_batch_everything_and_errors(fpx, oracle):
+    """All operations in one batch, with failing jobs among them."""
+    rng = np.random.default_rng(7)
+    p = 998244353
+    jobs = []
+    for q in (998244353, 1000000007, 97):
+        a = rnd(rng, q, 3000, nonzero0=True)
+        b = rnd(rng, q, 1200)
+        b[-1] = b[-1] or 1
+        sq = oracle.conv(q, a, a, 2000)
+        e0 = a.copy(); e0[0] = 0
+        l1 = a.copy(); l1[0] = 1
+        jobs += [("conv", q, a, b), ("inv", q, a, 2500), ("exp", q, e0, 90 if q == 97 else 2500),
+                 ("log", q, l1, 97 if q == 97 else 2600), ("sqrt", q, sq, 2000), ("pow", q, a[:500], 1000003, 2200),
+                 ("pow", q, a[:500], 3, 2200), ("divmod", q, a, b)]
+    jobs += [("inv", p, [0, 1, 2], 10), ("log", p, [2, 1], 5), ("exp", p, [1, 1], 5), ("sqrt", p, [0, 4], 5),
+             ("divmod", p, [1, 2], [0, 0]), ("log", 3, [1, 1], 4), ("exp", 3, [0, 1], 4), ("inv", p, [], 4)]
+    res = fpx.batch(jobs)
+    for i, jb in enumerate(jobs):
+        _check(res[i], _oracle_job(oracle, jb), f"job {i} {jb[0]} p={jb[1]}")
+
+
+def test_batch_matches_single_calls(fpx):
+    """Same result alone as in the mix (the serving contract)."""
+    rng = np.random.default_rng(99)
+    jobs = []
+    for p in (998244353, 1000000007, 167772161, 2147483647):
+        for n in (300, 5000, 40000):
+            a = rnd(rng, p, n, nonzero0=True)
+            b = rnd(rng, p, n // 2 + 1)
+            b[-1] = b[-1] or 1
+            e0 = a.copy(); e0[0] = 0
+            l1 = a.copy(); l1[0] = 1
+            jobs += [("conv", p, a, b), ("inv", p, a, n), ("exp", p, e0, n), ("log", p, l1, n), ("divmod", p, a, b)]
+    res = fpx.batch(jobs)
+    for i, jb in enumerate(jobs):
+        op, p = jb[0], jb[1]
+        if op == "conv":
+            alone = fpx.conv(p, jb[2], jb[3])
+        elif op == "divmod":
+            alone = fpx.divmod(p, jb[2], jb[3])
+        else:
+            alone = getattr(fpx, op)(p, jb[2], jb[3])
+        _check(res[i], alone, f"job {i} {op} p={p}")
+
+
+def test_batch_reference_vectors(fpx, ref_vectors):
+    """All 1332 reference vectors as one batch."""
+    jobs, want = [], []
+    for case in ref_vectors:
+        p, op = case["p"], case["op"]
+        if op == "conv":
+            jobs.append(("conv", p, case["a"], case["b"], case["n"]))
+        elif op == "pow":
+            jobs.append(("pow", p, case["a"], case["k"], case["n"]))
+        elif op == "divmod":
+            jobs.append(("divmod", p, case["a"], case["b"]))
+        else:
+            jobs.append((op, p, case["a"], case["n"]))
+        if case["status"] == "domain_error":
+            want.append(OracleDomainError(1, op))
+        elif op == "divmod":
+            want.append((np.asarray(case["q"], np.uint32), np.asarray(case["r"], np.uint32)))
+        else:
+            want.append(np.asarray(case["out"], np.uint32))
+    res = fpx.batch(jobs)
+    for i in range(len(jobs)):
+        _check(res[i], want[i], f"vector {i} {jobs[i][0]} p={jobs[i][1]}")
+
+
+def test_batch_montgomery(fpx, oracle):
+    rng = np.random.default_rng(5)
+    jobs, want = [], []
+    for p in (998244353, 1000000007, 2):
+        a, b = rnd(rng, p, 3000, nonzero0=True), rnd(rng, p, 2000)
+        ma = np.array([oracle.to_mont(p, int(x)) for x in a], np.uint32)
+        mb = np.array([oracle.to_mont(p, int(x)) for x in b], np.uint32)
+        jobs += [("conv", p, ma, mb), ("inv", p, ma, 4000)]
+        want += [oracle.conv(p, a, b), oracle.inv(p, a, 4000)]
+    res = fpx.batch(jobs, repr=F.MONTGOMERY)
+    for i, w in enumerate(want):
+        p = jobs[i][1]
+        eq(res[i], np.array([oracle.to_mont(p, int(x)) for x in w], np.uint32), f"mont job {i}")
+
+
+def test_batch_device_submit(fpx, oracle):
+    import torch
+    rng = np.random.default_rng(8)
+    p = 998244353
+    specs = [(OP, n) for OP in (F.OP_CONV, F.OP_INV, F.OP_EXP) for n in (100, 3000, 50000)]
+    jobs = (F.Job * len(specs))()
+    keep, host = [], []
+    for i, (op, n) in enumerate(specs):
+        a = rnd(rng, p, n, nonzero0=True)
+        if op == F.OP_EXP:
+            a[0] = 0
+        b = rnd(rng, p, n // 3 + 1)
+        da = torch.from_numpy(a.view(np.int32)).cuda()
+        db = torch.from_numpy(b.view(np.int32)).cuda()
+        cap = n + b.size - 1 if op == F.OP_CONV else n
+        do = torch.empty(cap, dtype=torch.int32, device="cuda")
+        keep += [da, db, do]
+        j = jobs[i]
+        j.op, j.p, j.a, j.la, j.n, j.out = op, p, da.data_ptr(), n, n if op != F.OP_CONV else F.SIZE_MAX, do.data_ptr()
+        if op == F.OP_CONV:
+            j.b, j.lb = db.data_ptr(), b.size
+        host.append((op, a, b, do))
+    torch.cuda.synchronize()
+    assert fpx.batch_submit(jobs) == F.OK
+    fpx.batch_wait()
+    for i, (op, a, b, do) in enumerate(host):
+        got = do.cpu().numpy().view(np.uint32)[: jobs[i].out_len]
+        if op == F.OP_CONV:
+            want = oracle.conv(p, a, b)
+        elif op == F.OP_INV:
+            want = oracle.inv(p, a, a.size)
+        else:
+            want = oracle.exp(p, a, a.size)
+        eq(got, want, f"device job {i}")
+
+
+def test_batch_empty_and_invalid(fpx):
+    assert fpx.batch([]) == []
+    res = fpx.batch([("conv", 4, [1], [1]), ("inv", 998244353, [1, 2], 3)])
+    assert isinstance(res[0], F.FpxError) and res[0].code == F.EINVAL
+    eq(res[1], [1, 998244351, 4], "inv next to an invalid job")
+
+
+def test_batch_launch_sharing(fpx):
+    """512 inverses of mixed sizes share launches: far fewer than one set per job."""
+    rng = np.random.default_rng(12)
+    p = 998244353
+    jobs = [("inv", p, rnd(rng, p, int(n), nonzero0=True), int(n))
+            for n in np.exp2(rng.uniform(8, 14, 512)).astype(int)]
+    fpx.batch(jobs[:4])
+    before = fpx.launch_count()
+    fpx.batch(jobs)
+    used = fpx.launch_count() - before
+    assert used < 200, used
