@@ -48,6 +48,14 @@ L2_FLUSH_BYTES = 512 << 20
 # fused row pass = forward a, forward b and inverse = 3 passes, inverse column = 1.
 ALG_BYTES = {"colfwd": 2 * 8 * N_FFT, "rows": 3 * 8 * N_FFT, "colinv": 8 * N_FFT}
 STEP_ALG_BYTES = sum(ALG_BYTES.values())
+# Algorithmic multiply instructions per launch: (N/2) log2(points) butterflies per
+# transform at 3 (Shoup: mul.hi + 2 mul.lo), the pointwise product at 4 (Montgomery);
+# columns are 2^11-point transforms, rows 2^12-point ones (2^11 x 2^12 = N).
+LOG_R, LOG_C = 11, 12
+ALG_MULS = {"colfwd": 2 * (N_FFT // 2) * LOG_R * 3,
+            "rows": 3 * (N_FFT // 2) * LOG_C * 3 + N_FFT * 4,
+            "colinv": (N_FFT // 2) * LOG_R * 3}
+STEP_ALG_MULS = sum(ALG_MULS.values())
 
 
 def env_rank():
@@ -274,8 +282,10 @@ def run_fpx(args):
     total_ms, e2e_s = max_over_ranks(dist, [total_ms, e2e_s], device="cuda")
     ms_per_step, value, e2e_value = whole_job_rates(world, args.steps, total_ms, e2e_steps, e2e_s)
 
-    # roofline of the dominant kernel
+    # roofline of the dominant kernel: the slower of bytes over HBM bandwidth and
+    # multiply instructions over the measured 32-bit multiply rate
     peak, peak_kind = measured_peak_hbm()
+    imad = F.measure_imad_rate(local)
     dom = max((k for k in prof if k in ALG_BYTES), key=lambda k: prof[k][1], default=None)
     roof = None
     if dom:
@@ -287,8 +297,17 @@ def run_fpx(args):
                 "alg_bytes_per_launch": ALG_BYTES[dom], "avg_launch_us": round(avg_s * 1e6, 2),
                 "traffic": ncu_traffic(dom),
                 "step": {"alg_bytes": STEP_ALG_BYTES, "achieved": round(STEP_ALG_BYTES / (ms_per_step * 1e-3) / 1e9, 1),
-                         "frac": round(STEP_ALG_BYTES / (ms_per_step * 1e-3) / 1e9 / peak, 4)},
-                "kernels_ms": {k: round(v[1] / v[0] * 1e3, 2) for k, v in prof.items()}}
+                         "frac": round(STEP_ALG_BYTES / (ms_per_step * 1e-3) / 1e9 / peak, 4),
+                         "alg_mul_instr": STEP_ALG_MULS,
+                         "t_roof_us": round(1e6 * max(STEP_ALG_BYTES / (peak * 1e9), STEP_ALG_MULS / imad), 2),
+                         "frac_of_roofline": round(max(STEP_ALG_BYTES / (peak * 1e9), STEP_ALG_MULS / imad)
+                                                   / (ms_per_step * 1e-3), 4)},
+                "int_mul": {"alg_mul_instr_per_launch": ALG_MULS[dom],
+                            "achieved_per_s": round(ALG_MULS[dom] / avg_s, 1), "peak_per_s": round(imad, 1),
+                            "frac": round(ALG_MULS[dom] / avg_s / imad, 4),
+                            "peak_source": "measured in this run (fpx_measure_imad_rate)"},
+                "frac_of_roofline": round(max(ALG_BYTES[dom] / (peak * 1e9), ALG_MULS[dom] / imad) / avg_s, 4),
+                "kernels_us": {k: round(v[1] / v[0] * 1e3, 2) for k, v in prof.items()}}
 
     line = None
     if rank == 0:
@@ -311,15 +330,410 @@ def run_fpx(args):
     return 0
 
 
+# ============================================================================
+# Secondary workloads (--workload batch | serve)
+# ============================================================================
+BATCH_MODULI = [998244353, 1000000007]
+SERVE_MODULI = [998244353, 167772161, 1000000007, 2147483647]
+NAIVE = 40
+
+
+def batch_mix(seed: int = 4):
+    """4096 convs (operand lengths floor(2^U), U ~ Uniform[6, 16] per operand) and
+    512 inv / exp (n log-uniform in [2^8, 2^14]); moduli 50/50 998244353 / 1e9+7."""
+    rng = np.random.default_rng(seed)
+    specs = []
+    for _ in range(4096):
+        p = BATCH_MODULI[rng.integers(0, 2)]
+        la, lb = int(2 ** rng.uniform(6, 16)), int(2 ** rng.uniform(6, 16))
+        specs.append(("conv", p, rng.integers(0, p, la, dtype=np.uint64).astype(np.uint32),
+                      rng.integers(0, p, lb, dtype=np.uint64).astype(np.uint32)))
+    for _ in range(512):
+        p = BATCH_MODULI[rng.integers(0, 2)]
+        n = int(2 ** rng.uniform(8, 14))
+        a = rng.integers(0, p, n, dtype=np.uint64).astype(np.uint32)
+        if rng.integers(0, 2) == 0:
+            a[0] = a[0] or 1
+            specs.append(("inv", p, a, n))
+        else:
+            a[0] = 0
+            specs.append(("exp", p, a, n))
+    return specs
+
+
+def serve_mix(count: int, seed: int = 5, max_log: int = 22):
+    """conv 40 %, inv 20 %, exp 15 %, sqrt 10 %, divmod 10 %, pow 5 % (k uniform u64);
+    sizes log-uniform in [2^8, 2^max_log]; moduli uniform over four."""
+    rng = np.random.default_rng(seed)
+    ops = ["conv"] * 8 + ["inv"] * 4 + ["exp"] * 3 + ["sqrt"] * 2 + ["divmod"] * 2 + ["pow"]
+    specs = []
+    for _ in range(count):
+        op = ops[rng.integers(0, len(ops))]
+        p = SERVE_MODULI[rng.integers(0, len(SERVE_MODULI))]
+        n = int(2 ** rng.uniform(8, max_log))
+        a = rng.integers(0, p, n, dtype=np.uint64).astype(np.uint32)
+        if op == "conv":
+            m = int(2 ** rng.uniform(8, max_log))
+            specs.append(("conv", p, a, rng.integers(0, p, m, dtype=np.uint64).astype(np.uint32)))
+        elif op == "divmod":
+            b = rng.integers(0, p, (n + 1) // 2, dtype=np.uint64).astype(np.uint32)
+            b[-1] = b[-1] or 1
+            specs.append(("divmod", p, a, b))
+        elif op == "pow":
+            specs.append(("pow", p, a, int(rng.integers(0, 2**63, dtype=np.uint64)) * 2 + int(rng.integers(0, 2)), n))
+        else:
+            a[0] = {"inv": a[0] or 1, "exp": 0, "sqrt": 1}[op]
+            specs.append((op, p, a, n))
+    return specs
+
+
+def _native(p: int, log_n: int) -> bool:
+    return p % 2 == 1 and p < (1 << 30) and 1 <= log_n <= ((p - 1) & -(p - 1)).bit_length() - 1
+
+
+def _tbytes(n_pts: int) -> int:
+    """Algorithmic bytes of one transform: 16 N past 2^15 points (two HBM passes), else 8 N."""
+    return 16 * n_pts if n_pts > (1 << 15) else 8 * n_pts
+
+
+def _product_bytes(p: int, la: int, lb: int, out: int, log_n: int | None = None) -> int:
+    if min(la, lb) <= NAIVE or out <= 0:
+        return 4 * (la + lb + out)
+    if log_n is None:
+        log_n = (la + lb - 2).bit_length()
+    n_pts = 1 << log_n
+    if _native(p, log_n):
+        return 3 * _tbytes(n_pts)
+    return 3 * 3 * _tbytes(n_pts) + 16 * out
+
+
+def alg_bytes(spec) -> int:
+    """The job's algorithmic HBM bytes under the transform byte rule (a batched
+    product with a reusable spectrum counts its transforms once)."""
+    op, p = spec[0], spec[1]
+    if op == "conv":
+        la, lb = len(spec[2]), len(spec[3])
+        return _product_bytes(p, la, lb, la + lb - 1) if la and lb else 0
+    n = spec[3]
+    total, m = 0, 32
+    if op == "inv":
+        while m < n:
+            k = (2 * m - 1).bit_length()
+            total += 5 * _tbytes(1 << k) if _native(p, k) else 2 * (9 * _tbytes(1 << k) + 16 * m)
+            m *= 2
+        return total
+    # exp: extension of the running inverse plus eight transforms per doubling
+    csize = 16
+    while m < n:
+        k = (2 * m - 1).bit_length()
+        hlen = min(2 * m, n) - m
+        if csize < hlen:
+            kc = (2 * csize - 1).bit_length()
+            total += 5 * _tbytes(1 << kc) if _native(p, kc) else 2 * (9 * _tbytes(1 << kc) + 16 * hlen)
+            csize = hlen
+        total += 8 * _tbytes(1 << k) if _native(p, k) else 3 * (9 * _tbytes(1 << k) + 16 * hlen)
+        m *= 2
+    return total
+
+
+def _device_jobs(F, torch, specs):
+    """Job array with device copies of every operand (one upload) and outputs."""
+    words_in = sum(len(s[2]) + (len(s[3]) if s[0] in ("conv", "divmod") else 0) for s in specs)
+    caps = []
+    for s in specs:
+        if s[0] == "conv":
+            caps.append(max(len(s[2]) + len(s[3]) - 1, 1))
+        elif s[0] == "divmod":
+            caps.append(len(s[2]) + len(s[3]))
+        else:
+            caps.append(s[-1])
+    host = np.concatenate([np.concatenate([s[2], s[3]]) if s[0] in ("conv", "divmod") else s[2] for s in specs])
+    din = torch.from_numpy(host.view(np.int32)).cuda()
+    dout = torch.empty(sum(caps), dtype=torch.int32, device="cuda")
+    jobs = (F.Job * len(specs))()
+    qi = qo = 0
+    base_in, base_out = din.data_ptr(), dout.data_ptr()
+    for i, s in enumerate(specs):
+        j = jobs[i]
+        j.op, j.p = F._OPS[s[0]], s[1]
+        j.a, j.la = base_in + 4 * qi, len(s[2])
+        qi += len(s[2])
+        if s[0] in ("conv", "divmod"):
+            j.b, j.lb = base_in + 4 * qi, len(s[3])
+            qi += len(s[3])
+        j.n = F.SIZE_MAX if s[0] == "conv" else (0 if s[0] == "divmod" else s[-1])
+        if s[0] == "pow":
+            j.k = s[3]
+        j.out = base_out + 4 * qo
+        if s[0] == "divmod":
+            j.out2 = base_out + 4 * (qo + len(s[2]))
+        qo += caps[i]
+    assert qi == words_in
+    return jobs, din, dout
+
+
+def run_batch_fpx(args):
+    import torch
+    import fastpoly_b200 as F
+
+    rank, local, world = env_rank()
+    torch.cuda.set_device(local)
+    ctx = F.Context(local)
+    stream = torch.cuda.Stream()
+    ctx.set_stream(stream.cuda_stream)
+    torch.cuda.set_stream(stream)
+    specs = batch_mix()
+    jobs, din, dout = _device_jobs(F, torch, specs)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.int32, device="cuda")
+    step_bytes = sum(alg_bytes(s) for s in specs)
+
+    def step():
+        rc = ctx.batch_submit(jobs)
+        assert rc == F.OK, rc
+
+    for _ in range(args.warmup):
+        flush.zero_()
+        step()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(0.3)
+    steps = max(3, min(args.steps, 50))
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    launches0 = ctx.launch_count()
+    torch.cuda.synchronize()
+    for i in range(steps):
+        flush.zero_()
+        ev[i][0].record(stream)
+        step()
+        ev[i][1].record(stream)
+    torch.cuda.synchronize()
+    launches = (ctx.launch_count() - launches0) // steps
+    ms = float(np.median([s.elapsed_time(e) for s, e in ev]))
+    value = len(specs) / (ms * 1e-3)
+
+    # the plain per-call path on the same device buffers (one call per job)
+    def plain():
+        for i, s in enumerate(specs):
+            j = jobs[i]
+            if s[0] == "conv":
+                ctx.conv_device(s[1], j.a, j.la, j.b, j.lb, None, j.out)
+            elif s[0] == "inv":
+                ctx.inv_device(s[1], j.a, j.la, j.n, j.out)
+            else:
+                ctx.exp_device(s[1], j.a, j.la, j.n, j.out)
+        ctx.synchronize()
+
+    plain()
+    t0 = time.perf_counter()
+    plain()
+    plain_s = time.perf_counter() - t0
+
+    # end to end: host buffers through fpx_batch_run
+    ctx.batch(specs)
+    e2e_steps = 5
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        res = ctx.batch(specs)
+    e2e_s = (time.perf_counter() - t0) / e2e_steps
+    clk = clocks.stop()
+    bad = sum(isinstance(r, Exception) for r in res)
+    assert bad == 0, f"{bad} failed jobs"
+    h2d = 4 * sum(len(s[2]) + (len(s[3]) if s[0] == "conv" else 0) for s in specs)
+    d2h = 4 * sum(r.size for r in res)
+    peak, peak_kind = measured_peak_hbm()
+    achieved = step_bytes / (ms * 1e-3) / 1e9
+    line = {"metric": "polys/s, mixed batch (4096 conv + 512 inv/exp)", "value": round(value, 1), "unit": "polys/s",
+            "n_gpus": 1, "steps": steps, "warmup": args.warmup, "ms_per_step": round(ms, 4), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+            "config": {"workload": "4096 conv (lengths 2^U, U~U[6,16]) + 512 inv/exp (n log-uniform 2^8..2^14), "
+                                   "moduli 50/50 998244353 / 1000000007, fixed seed", "jobs": len(specs),
+                       "l2": "flushed between steps (512 MiB write)"},
+            "plain_per_call": {"value": round(len(specs) / plain_s, 1), "unit": "polys/s",
+                               "api": "fpx_conv_device / fpx_inv_device / fpx_exp_device, one call per job"},
+            "batch_speedup": round(value / (len(specs) / plain_s), 2),
+            "e2e": {"value": round(len(specs) / e2e_s, 1), "unit": "polys/s", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h, "api": "fpx_batch_run (host buffers)"},
+            "gpu_launches": int(launches),
+            "roofline": {"bound": "hbm", "kernel": "whole batch step", "achieved": round(achieved, 1), "peak": peak,
+                         "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": None,
+                         "alg_bytes_per_step": step_bytes, "peak_source": peak_kind},
+            "clocks": clk}
+    if not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_mix_sample(specs, budget_s=20.0)
+    print(json.dumps(line))
+    ctx.close()
+    return 0
+
+
+def _ref_call(ref, spec):
+    from oracle.oracle import OP_CONV, OP_INV, OP_LOG, OP_EXP, OP_SQRT, OP_POW, OP_DIVMOD
+    op, p = spec[0], spec[1]
+    code = {"conv": OP_CONV, "inv": OP_INV, "log": OP_LOG, "exp": OP_EXP, "sqrt": OP_SQRT, "pow": OP_POW,
+            "divmod": OP_DIVMOD}[op]
+    if op == "conv":
+        return ref.run(code, p, spec[2], spec[3], cap=len(spec[2]) + len(spec[3]))[2][0]
+    if op == "divmod":
+        return ref.run(code, p, spec[2], spec[3], cap=len(spec[2]) + len(spec[3]))[2][0]
+    if op == "pow":
+        return ref.run(code, p, spec[2], n=spec[4], k=spec[3], cap=spec[4])[2][0]
+    try:
+        return ref.run(code, p, spec[2], n=spec[3], cap=spec[3])[2][0]
+    except Exception:
+        return 0.0
+
+
+def cpu_mix_sample(specs, budget_s: float = 20.0, threads: int | None = None):
+    """The reference on this host's cores: one worker thread per core pulling jobs
+    of the mix (the library is thread-safe across calls), until the job list or
+    the time budget runs out; polys/s over the jobs finished."""
+    from concurrent.futures import ThreadPoolExecutor
+    from oracle.oracle import Reference
+    ref = Reference.load()
+    if ref is None:
+        return {"value": None, "unavailable": "reference build (oracle/_ref) missing"}
+    threads = threads or max(1, min(os.cpu_count() or 1, 64))
+    deadline = time.perf_counter() + budget_s
+    done = [0]
+
+    def work(s):
+        if time.perf_counter() > deadline:
+            return
+        _ref_call(ref, s)
+        done[0] += 1
+
+    t0 = time.perf_counter()
+    with ThreadPoolExecutor(threads) as ex:
+        list(ex.map(work, specs))
+    el = time.perf_counter() - t0
+    return {"value": round(done[0] / el, 1), "unit": "polys/s", "cores": threads, "kind": "reference",
+            "sample": f"{done[0]} of {len(specs)} jobs of the mix on {threads} threads in {el:.1f} s ({ref.backend})"}
+
+
+def run_batch_reference(args):
+    rank, _, world = env_rank()
+    if rank != 0:
+        return 0
+    specs = batch_mix()
+    threads = max(1, min(os.cpu_count() or 1, 64))
+    for _ in range(min(args.warmup, 1)):
+        cpu_mix_sample(specs[:256], budget_s=5.0, threads=threads)
+    vals = [cpu_mix_sample(specs, budget_s=20.0, threads=threads) for _ in range(max(1, min(args.steps, 3)))]
+    v = float(np.median([x["value"] for x in vals]))
+    line = {"impl": "reference", "metric": "polys/s, mixed batch (4096 conv + 512 inv/exp)", "value": v,
+            "unit": "polys/s", "n_gpus": world, "steps": len(vals), "warmup": args.warmup,
+            "ms_per_step": round(1e3 * len(specs) / v, 3), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+            "config": {"workload": "batch mix (same as --workload batch)", "threads": threads},
+            "cpu_baseline": dict(vals[0], value=v),
+            "e2e": {"value": v, "unit": "polys/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+def run_serve_fpx(args):
+    import threading
+    import torch
+    import fastpoly_b200 as F
+
+    rank, local, world = env_rank()
+    torch.cuda.set_device(local)
+    count = args.requests
+    specs = serve_mix(count, max_log=args.serve_max_log)
+    srv = F.Server(local, workers=args.workers)
+    try:
+        # warm-up: plans, pools, pinned buffers
+        for t in [srv.submit(s) for s in serve_mix(64, seed=9, max_log=args.serve_max_log)]:
+            srv.poll(t)
+        # saturation: everything offered at once
+        t0 = time.perf_counter()
+        tickets = [srv.submit(s) for s in specs]
+        lat = []
+        fails = 0
+        for t in tickets:
+            r, l = srv.poll(t)
+            fails += isinstance(r, Exception)
+            lat.append(l)
+        sat_s = time.perf_counter() - t0
+        sat_rate = count / sat_s
+        loads = {}
+        for frac in (0.5, 0.8, 1.0):
+            rate = frac * sat_rate
+            rng = np.random.default_rng(int(frac * 100))
+            gaps = rng.exponential(1.0 / rate, count)
+            arrivals = np.cumsum(gaps)
+            tickets = [None] * count
+
+            def submitter():
+                start = time.perf_counter()
+                for i in range(count):
+                    d = start + arrivals[i] - time.perf_counter()
+                    if d > 0:
+                        time.sleep(d)
+                    tickets[i] = srv.submit(specs[i])
+
+            th = threading.Thread(target=submitter)
+            t0 = time.perf_counter()
+            th.start()
+            lats = []
+            for i in range(count):
+                while tickets[i] is None:
+                    time.sleep(0.0002)
+                r, l = srv.poll(tickets[i])
+                lats.append(l)
+            th.join()
+            el = time.perf_counter() - t0
+            loads[f"{int(frac * 100)}%"] = {"offered_req_s": round(rate, 2), "achieved_req_s": round(count / el, 2),
+                                            "p50_ms": round(1e3 * float(np.percentile(lats, 50)), 3),
+                                            "p99_ms": round(1e3 * float(np.percentile(lats, 99)), 3)}
+        st = srv.stats()
+    finally:
+        srv.stop()
+    in_bytes = 4 * sum(len(s[2]) + (len(s[3]) if s[0] in ("conv", "divmod") else 0) for s in specs)
+    line = {"metric": "served requests/s at saturation (mixed ops, sizes 2^8..2^%d)" % args.serve_max_log,
+            "value": round(sat_rate, 2), "unit": "req/s", "n_gpus": 1, "steps": count, "warmup": 64,
+            "ms_per_step": round(1e3 / sat_rate, 3), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+            "config": {"workload": "conv 40 / inv 20 / exp 15 / sqrt 10 / divmod 10 / pow 5 %, sizes log-uniform "
+                                   f"2^8..2^{args.serve_max_log}, moduli 998244353 / 167772161 / 1e9+7 / 2^31-1",
+                       "requests": count, "workers": args.workers, "failed": int(fails)},
+            "latency": loads, "server": st,
+            "e2e": {"value": round(sat_rate, 2), "unit": "req/s", "h2d_bytes_per_step": in_bytes // count,
+                    "d2h_bytes_per_step": None, "api": "fpx_serve_submit / fpx_serve_poll (host buffers)"}}
+    if not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_mix_sample(specs, budget_s=30.0)
+    print(json.dumps(line))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="fpx", choices=["fpx", "reference"])
+    ap.add_argument("--workload", default="conv", choices=["conv", "batch", "serve"],
+                    help="conv: the headline 2^23 conv (default); batch: mixed batch; serve: request loop")
+    ap.add_argument("--requests", type=int, default=300, help="serve: requests per load level")
+    ap.add_argument("--serve-max-log", type=int, default=22, help="serve: largest size 2^k")
+    ap.add_argument("--workers", type=int, default=2, help="serve: micro-batches in flight")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
+    if args.workload == "batch":
+        return run_batch_reference(args) if args.impl == "reference" else run_batch_fpx(args)
+    if args.workload == "serve":
+        if args.impl == "reference":
+            rank, _, world = env_rank()
+            if rank == 0:
+                specs = serve_mix(args.requests, max_log=args.serve_max_log)
+                b = cpu_mix_sample(specs, budget_s=60.0)
+                print(json.dumps({"impl": "reference", "metric": "served requests/s at saturation", "value": b["value"],
+                                  "unit": "req/s", "n_gpus": world, "higher_is_better": True, "cpu_baseline": b,
+                                  "e2e": {"value": b["value"], "unit": "req/s", "h2d_bytes_per_step": 0,
+                                          "d2h_bytes_per_step": 0}}))
+            return 0
+        return run_serve_fpx(args)
     if args.impl == "reference":
         return run_reference(args)
     return run_fpx(args)

@@ -22,7 +22,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libfpx_b200.so")
 
-OK, EDOMAIN, ESIZE, ELENGTH, ENOMEM, ETIMEDOUT, ECUDA, EINVAL, EUNSUPPORTED = range(9)
+OK, EDOMAIN, ESIZE, ELENGTH, ENOMEM, ETIMEDOUT, ECUDA, EINVAL, EUNSUPPORTED, EPENDING = range(10)
 CANONICAL, MONTGOMERY = 0, 1
 SIZE_MAX = 2**64 - 1
 
@@ -91,9 +91,17 @@ def load_library(path: str = LIB_PATH):
     L.fpx_divmod.argtypes = [vp, u32, _u32p, sz, _u32p, sz, _u32p, _szp, _u32p, _szp, i32]
     L.fpx_div.argtypes = [vp, u32, _u32p, sz, _u32p, sz, _u32p, _szp, i32]
     L.fpx_mod.argtypes = [vp, u32, _u32p, sz, _u32p, sz, _u32p, _szp, i32]
+    L.fpx_measure_imad_rate.argtypes = [i32, C.POINTER(C.c_double)]
     L.fpx_batch_submit.argtypes = [vp, vp, sz]
     L.fpx_batch_wait.argtypes = [vp]
     L.fpx_batch_run.argtypes = [vp, vp, sz, i32]
+    L.fpx_serve_start.argtypes = [i32, vp, C.POINTER(vp)]
+    L.fpx_serve_submit.argtypes = [vp, vp, C.POINTER(u64)]
+    L.fpx_serve_poll.argtypes = [vp, u64, i32, C.POINTER(u64)]
+    L.fpx_serve_stats_get.argtypes = [vp, vp]
+    L.fpx_serve_stop.argtypes = [vp]
+    L.fpx_serve_plan_bytes.argtypes = [vp]
+    L.fpx_serve_plan_bytes.restype = sz
     _lib = L
     return L
 
@@ -108,6 +116,116 @@ class Job(C.Structure):
     _fields_ = [("op", C.c_int), ("p", C.c_uint32), ("a", C.c_void_p), ("la", C.c_size_t), ("b", C.c_void_p),
                 ("lb", C.c_size_t), ("k", C.c_uint64), ("n", C.c_size_t), ("out", C.c_void_p),
                 ("out2", C.c_void_p), ("out_len", C.c_size_t), ("out2_len", C.c_size_t), ("status", C.c_int)]
+
+
+class ServeConfig(C.Structure):
+    """struct fpx_serve_config."""
+    _fields_ = [("hbm_budget_bytes", C.c_size_t), ("max_batch_jobs", C.c_size_t), ("workers", C.c_int),
+                ("repr", C.c_int)]
+
+
+class ServeStats(C.Structure):
+    """struct fpx_serve_stats."""
+    _fields_ = [("submitted", C.c_uint64), ("completed", C.c_uint64), ("batches", C.c_uint64),
+                ("max_batch_jobs_seen", C.c_uint64), ("max_batch_bytes_seen", C.c_uint64),
+                ("oversize_requests", C.c_uint64)]
+
+
+def make_job(spec, keep: list) -> tuple:
+    """Fills a Job from a tuple spec (see Context.batch) with host buffers; returns
+    (job, out, out2).  Arrays the job points into are appended to `keep`."""
+    op, p = _OPS[spec[0]], int(spec[1])
+    a = _arr(spec[2])
+    b = np.zeros(0, np.uint32)
+    k, n = 0, 0
+    o2 = None
+    if op == OP_CONV:
+        b = _arr(spec[3])
+        n = SIZE_MAX if len(spec) < 5 or spec[4] is None else int(spec[4])
+        cap = min(a.size, n) + min(b.size, n) - 1 if a.size and b.size and n else 0
+        o1 = np.empty(max(min(cap, n), 1), np.uint32)
+    elif op == OP_POW:
+        k, n = int(spec[3]), int(spec[4])
+        o1 = np.empty(max(n, 1), np.uint32)
+    elif op == OP_DIVMOD:
+        b = _arr(spec[3])
+        o1, o2 = np.empty(max(a.size, 1), np.uint32), np.empty(max(b.size, 1), np.uint32)
+    else:
+        n = int(spec[3])
+        o1 = np.empty(max(n, 1), np.uint32)
+    j = Job()
+    j.op, j.p, j.la, j.lb, j.k, j.n = op, p, a.size, b.size, k, n
+    j.a = a.ctypes.data if a.size else None
+    j.b = b.ctypes.data if b.size else None
+    j.out = o1.ctypes.data
+    j.out2 = o2.ctypes.data if o2 is not None else None
+    keep += [a, b, o1, o2]
+    return j, o1, o2
+
+
+def job_result(j, o1, o2, what=""):
+    """The result of a finished Job: the array ((q, r) for divmod) or the exception the single call raises."""
+    if j.status != OK:
+        return _ERRORS.get(j.status, FpxError)(j.status, what)
+    if j.op == OP_DIVMOD:
+        return o1[: j.out_len], o2[: j.out2_len]
+    return o1[: j.out_len]
+
+
+class Server:
+    """The request loop (fpx_serve_*): HBM-budget admission, continuous micro-batching."""
+
+    def __init__(self, device: int = 0, hbm_budget_bytes: int = 0, max_batch_jobs: int = 0, workers: int = 0,
+                 repr: int = CANONICAL):
+        self._L = load_library()
+        cfg = ServeConfig(hbm_budget_bytes, max_batch_jobs, workers, repr)
+        h = C.c_void_p()
+        rc = self._L.fpx_serve_start(device, C.byref(cfg), C.byref(h))
+        if rc != OK:
+            raise FpxError(rc, "fpx_serve_start failed")
+        self._h = h
+        self._live = {}
+
+    def submit(self, spec) -> int:
+        """Queues one request (tuple spec as in Context.batch); returns its ticket."""
+        keep = []
+        j, o1, o2 = make_job(spec, keep)
+        t = C.c_uint64(0)
+        rc = self._L.fpx_serve_submit(self._h, C.byref(j), C.byref(t))
+        if rc != OK:
+            raise FpxError(rc, "fpx_serve_submit failed")
+        self._live[t.value] = (j, o1, o2, keep, spec[0])
+        return t.value
+
+    def poll(self, ticket: int, wait: bool = True):
+        """None while pending; else (result, latency_seconds)."""
+        lat = C.c_uint64(0)
+        rc = self._L.fpx_serve_poll(self._h, ticket, 1 if wait else 0, C.byref(lat))
+        if rc == EPENDING:
+            return None
+        j, o1, o2, keep, op = self._live.pop(ticket)
+        return job_result(j, o1, o2, f"served {op}"), lat.value * 1e-9
+
+    def stats(self) -> dict:
+        st = ServeStats()
+        self._L.fpx_serve_stats_get(self._h, C.byref(st))
+        return {k: getattr(st, k) for k, _ in ServeStats._fields_}
+
+    def plan_bytes(self, spec) -> int:
+        keep = []
+        j, _, _ = make_job(spec, keep)
+        return int(self._L.fpx_serve_plan_bytes(C.byref(j)))
+
+    def stop(self):
+        if getattr(self, "_h", None):
+            self._L.fpx_serve_stop(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.stop()
+        except Exception:
+            pass
 
 
 class PoolStats(C.Structure):
@@ -315,45 +433,14 @@ class Context:
         arr = (Job * max(len(jobs), 1))()
         keep, outs = [], []
         for i, jb in enumerate(jobs):
-            op, p = _OPS[jb[0]], int(jb[1])
-            a = _arr(jb[2])
-            b = np.zeros(0, np.uint32)
-            k, n = 0, 0
-            if op == OP_CONV:
-                b = _arr(jb[3])
-                n = SIZE_MAX if len(jb) < 5 or jb[4] is None else int(jb[4])
-                cap = min(a.size, n) + min(b.size, n) - 1 if a.size and b.size and n else 0
-                o1, o2 = np.empty(max(min(cap, n), 1), np.uint32), None
-            elif op == OP_POW:
-                k, n = int(jb[3]), int(jb[4])
-                o1, o2 = np.empty(max(n, 1), np.uint32), None
-            elif op == OP_DIVMOD:
-                b = _arr(jb[3])
-                o1, o2 = np.empty(max(a.size, 1), np.uint32), np.empty(max(b.size, 1), np.uint32)
-            else:
-                n = int(jb[3])
-                o1, o2 = np.empty(max(n, 1), np.uint32), None
-            j = arr[i]
-            j.op, j.p, j.la, j.lb, j.k, j.n = op, p, a.size, b.size, k, n
-            j.a = a.ctypes.data if a.size else None
-            j.b = b.ctypes.data if b.size else None
-            j.out = o1.ctypes.data
-            j.out2 = o2.ctypes.data if o2 is not None else None
-            keep += [a, b]
+            j, o1, o2 = make_job(jb, keep)
+            arr[i] = j
             outs.append((o1, o2))
         rc = self._L.fpx_batch_run(self._h, C.cast(arr, C.c_void_p), len(jobs), repr)
         if rc not in (OK, EDOMAIN, ESIZE, ELENGTH, EINVAL):
             self._check(rc, "batch")
-        res = []
-        for i in range(len(jobs)):
-            j = arr[i]
-            if j.status != OK:
-                res.append(_ERRORS.get(j.status, FpxError)(j.status, f"batch job {i} ({jobs[i][0]})"))
-            elif j.op == OP_DIVMOD:
-                res.append((outs[i][0][: j.out_len], outs[i][1][: j.out2_len]))
-            else:
-                res.append(outs[i][0][: j.out_len])
-        return res
+        return [job_result(arr[i], outs[i][0], outs[i][1], f"batch job {i} ({jobs[i][0]})")
+                for i in range(len(jobs))]
 
     def batch_submit(self, jobs) -> int:
         """fpx_batch_submit on a ctypes array of Job with device pointers; returns the call's status
@@ -364,10 +451,19 @@ class Context:
         self._check(self._L.fpx_batch_wait(self._h), "batch_wait")
 
 
+def measure_imad_rate(device: int = 0) -> float:
+    """Measured thread-level 32-bit multiply instructions per second of the GPU."""
+    r = C.c_double(0)
+    rc = load_library().fpx_measure_imad_rate(device, C.byref(r))
+    if rc != OK:
+        raise FpxError(rc, "fpx_measure_imad_rate failed")
+    return r.value
+
+
 def ntt_max_log(p: int) -> int:
     return load_library().fpx_ntt_max_log(p)
 
 
 __all__ = ["Context", "DomainError", "NttSizeError", "LengthError", "FpxError", "CANONICAL", "MONTGOMERY",
-           "load_library", "ntt_max_log", "LIB_PATH", "Job", "OP_CONV", "OP_INV", "OP_LOG", "OP_EXP", "OP_SQRT",
+           "load_library", "ntt_max_log", "LIB_PATH", "Job", "Server", "make_job", "job_result", "OP_CONV", "OP_INV", "OP_LOG", "OP_EXP", "OP_SQRT",
            "OP_POW", "OP_DIVMOD"]

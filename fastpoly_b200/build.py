@@ -24,7 +24,7 @@ CUDA_HOME = os.environ.get("CUDA_HOME", "/usr/local/cuda")
 NVCC = os.path.join(CUDA_HOME, "bin", "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
-CU_SOURCES = ["kernels.cu", "noalloc.cu"]
+CU_SOURCES = ["kernels.cu", "noalloc.cu", "peaks.cu"]
 CPP_SOURCES = ["engine.cpp", "batch.cpp", "serve.cpp", "api.cpp"]
 HEADERS = ["field.cuh", "ntt_core.cuh", "ntt_fast.cuh", "kernels.h", "engine.h"]
 

@@ -322,9 +322,14 @@ struct HostTables {
 };
 }  // namespace
 
+// Plans are uploaded on the engine's stream and waited for: the engine's stream
+// does not synchronise with the legacy default stream, and a plan outlives
+// stream changes (set_stream), so the tables must be complete before any use.
 static uint32_t* upload(Engine& eng, Buf& dst, const std::vector<Tw2>& v) {
   dst = Buf(&eng.pool(), v.size() * 2);
-  eng.check(cudaMemcpy(dst.get(), v.data(), v.size() * sizeof(Tw2), cudaMemcpyHostToDevice), "plan upload");
+  eng.check(cudaMemcpyAsync(dst.get(), v.data(), v.size() * sizeof(Tw2), cudaMemcpyHostToDevice, eng.stream()),
+            "plan upload");
+  eng.sync();
   return dst.get();
 }
 

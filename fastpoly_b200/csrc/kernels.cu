@@ -85,6 +85,21 @@ __device__ __forceinline__ void epi_store(const EpiD& e, uint32_t gi, uint32_t x
   e.out[j] = v;
 }
 
+// The plain epilogue (no scale, table, negation, subtraction or accumulation):
+// canonical value into the window.
+template <bool PLAIN>
+__device__ __forceinline__ void epi_store_t(const EpiD& e, uint32_t gi, uint32_t x, const Fp& f) {
+  if constexpr (PLAIN) {
+    if (gi < e.lo || gi >= e.hi) return;
+    e.out[gi - e.lo] = red(red(x, f.p2), f.p);
+  } else {
+    epi_store(e, gi, x, f);
+  }
+}
+bool host_epi_plain(const fpx::Epi& e) {
+  return e.scale.w == 0 && !e.mul_mont && !e.negate && !e.sub_from && !e.accumulate;
+}
+
 __device__ __forceinline__ int brev_n(int t, int logn) { return logn ? (int)(__brev((unsigned)t) >> (32 - logn)) : 0; }
 
 // ---------------------------------------------------------------------------
@@ -893,10 +908,12 @@ struct ColCfg {
 // Loads the W x R column tile (rows t, columns j0..j0+W) into shared memory
 // with cp.async: all copies in flight at once, no register staging, zero
 // beyond `count`.  16-byte copies when the source is 16-byte aligned.
-template <int LOGR>
+template <int LOGR, bool HALF = false>
 __device__ __forceinline__ void col_tile_load(uint32_t* sm, const uint32_t* src, uint32_t count, int j0, int logC,
                                               int tid) {
+  // HALF: only rows t < R/2 (the rest are known zeros, never read as such)
   using C = ColCfg<LOGR>;
+  constexpr int TL = HALF ? C::TE / 2 : C::TE;
   if (src == nullptr || count == 0) {
     for (int e = tid; e < C::SMEM_WORDS; e += 256) sm[e] = 0u;
     return;
@@ -904,7 +921,7 @@ __device__ __forceinline__ void col_tile_load(uint32_t* sm, const uint32_t* src,
   if (((uintptr_t)src & 15u) == 0) {
     constexpr int CPR = C::W / 4;  // 16-byte chunks per row segment
 #pragma unroll 4
-    for (int q = tid; q < C::TE / 4; q += 256) {
+    for (int q = tid; q < TL / 4; q += 256) {
       const int t = q / CPR, cc = (q % CPR) * 4;
       const uint32_t gi = ((uint32_t)t << logC) + j0 + cc;
       const int valid = gi < count ? (int)min(4u, count - gi) : 0;
@@ -912,7 +929,7 @@ __device__ __forceinline__ void col_tile_load(uint32_t* sm, const uint32_t* src,
     }
   } else {
 #pragma unroll 4
-    for (int e = tid; e < C::TE; e += 256) {
+    for (int e = tid; e < TL; e += 256) {
       const int t = e >> C::LOGW, c = e & (C::W - 1);
       const uint32_t gi = ((uint32_t)t << logC) + j0 + c;
       const bool v = gi < count;
@@ -924,7 +941,7 @@ __device__ __forceinline__ void col_tile_load(uint32_t* sm, const uint32_t* src,
 
 // One group over the tile, shared -> registers -> shared.  REDUCE: inputs may be
 // any 32-bit value (CRT lift), reduce them on the way in (first forward group).
-template <int LOGR, int KG, bool INV, bool REDUCE>
+template <int LOGR, int KG, bool INV, bool REDUCE, bool ZH = false>
 __device__ __forceinline__ void col_group_smem(uint32_t* sm, const uint2* tw, const Fp& f, uint32_t q1, int tid) {
   using C = ColCfg<LOGR>;
   constexpr int G = ColGroups<LOGR>::size(KG);
@@ -939,22 +956,23 @@ __device__ __forceinline__ void col_group_smem(uint32_t* sm, const uint2* tw, co
     const int p0 = ((rest >> S) << T) + base;
     uint32_t v[2][1 << G];
 #pragma unroll
-    for (int i = 0; i < (1 << G); ++i) {
+    for (int i = 0; i < (ZH ? (1 << G) / 2 : (1 << G)); ++i) {
       const uint32_t x = sm[C::P::at(((p0 + (i << S)) << C::LOGW) + c)];
       v[0][i] = REDUCE ? reduce_any(x, q1, f) : x;
     }
-    bf_group<G, T, INV, 1>(v, tw, base, f);
+    bf_group<G, T, INV, 1, false, ZH>(v, tw, base, f);
 #pragma unroll
     for (int i = 0; i < (1 << G); ++i) sm[C::P::at(((p0 + (i << S)) << C::LOGW) + c)] = v[0][i];
   }
 }
 
 // Forward groups 0 .. K-2 (the last group is the caller's).
-template <int LOGR, int KG>
+template <int LOGR, int KG, bool ZH = false>
 __device__ __forceinline__ void col_fwd_groups(uint32_t* sm, const Ptab& pt, bool reduce, int tid) {
   if constexpr (KG < ColGroups<LOGR>::K - 1) {
-    if (KG == 0 && reduce) col_group_smem<LOGR, KG, false, true>(sm, pt.fwd, pt.f, pt.q1, tid);
-    else col_group_smem<LOGR, KG, false, false>(sm, pt.fwd, pt.f, pt.q1, tid);
+    constexpr bool Z = ZH && KG == 0;
+    if (KG == 0 && reduce) col_group_smem<LOGR, KG, false, true, Z>(sm, pt.fwd, pt.f, pt.q1, tid);
+    else col_group_smem<LOGR, KG, false, false, Z>(sm, pt.fwd, pt.f, pt.q1, tid);
     __syncthreads();
     col_fwd_groups<LOGR, KG + 1>(sm, pt, reduce, tid);
   }
@@ -979,9 +997,18 @@ __device__ __forceinline__ void colfwd_body(const InD& in, uint32_t* __restrict_
   const int tid = threadIdx.x, logC = bt.logC;
   const int j0 = blockIdx.x << C::LOGW;
   const Fp f = pt.f;
-  col_tile_load<LOGR>(sm, in.ptr, in.count, j0, logC, tid);
-  __syncthreads();
-  col_fwd_groups<LOGR, 0>(sm, pt, in.reduce != 0, tid);
+  // zero-padded input (count <= N/2, every conv operand): the lower half of
+  // each column is never loaded and the first level needs no additions
+  const bool half = K > 1 && in.ptr != nullptr && in.count != 0 && in.count <= (1u << (LOGR - 1 + logC));
+  if (half) {
+    col_tile_load<LOGR, true>(sm, in.ptr, in.count, j0, logC, tid);
+    __syncthreads();
+    col_fwd_groups<LOGR, 0, true>(sm, pt, in.reduce != 0, tid);
+  } else {
+    col_tile_load<LOGR>(sm, in.ptr, in.count, j0, logC, tid);
+    __syncthreads();
+    col_fwd_groups<LOGR, 0>(sm, pt, in.reduce != 0, tid);
+  }
   // last group: shared -> registers -> Bailey twiddle -> global
   constexpr int NINST = C::TE >> G;
   const bool reduce_here = K == 1 && in.reduce;
@@ -1016,7 +1043,7 @@ __global__ void __launch_bounds__(256, 3) k_colfwd_t(ColOps ops, BigD bt, Ptab p
   colfwd_body<LOGR>(in, out, bt, pt);
 }
 
-template <int LOGR>
+template <int LOGR, bool PLAIN>
 __device__ __forceinline__ void colinv_body(const uint32_t* __restrict__ in, const BigD& bt, const Ptab& pt,
                                             const EpiD& epi) {
   using C = ColCfg<LOGR>;
@@ -1049,7 +1076,7 @@ __device__ __forceinline__ void colinv_body(const uint32_t* __restrict__ in, con
       bf_group<G, G, true, 1, true>(v, pt.inv, 0, f);
       if constexpr (K == 1) {
 #pragma unroll
-        for (int i = 0; i < (1 << G); ++i) epi_store(epi, (uint32_t)(((p0 + i) << logC) + j), v[0][i], f);
+        for (int i = 0; i < (1 << G); ++i) epi_store_t<PLAIN>(epi, (uint32_t)(((p0 + i) << logC) + j), v[0][i], f);
       } else {
 #pragma unroll
         for (int i = 0; i < (1 << G); ++i) sm[C::P::at(((p0 + i) << C::LOGW) + c)] = v[0][i];
@@ -1072,14 +1099,15 @@ __device__ __forceinline__ void colinv_body(const uint32_t* __restrict__ in, con
       for (int i = 0; i < (1 << G); ++i) v[0][i] = sm[C::P::at(((base + (i << S)) << C::LOGW) + c)];
       bf_group<G, LOGR, true, 1>(v, pt.inv, base, f);
 #pragma unroll
-      for (int i = 0; i < (1 << G); ++i) epi_store(epi, (uint32_t)(((base + (i << S)) << logC) + j0 + c), v[0][i], f);
+      for (int i = 0; i < (1 << G); ++i)
+        epi_store_t<PLAIN>(epi, (uint32_t)(((base + (i << S)) << logC) + j0 + c), v[0][i], f);
     }
   }
 }
 
-template <int LOGR>
+template <int LOGR, bool PLAIN>
 __global__ void __launch_bounds__(256, 3) k_colinv_t(const uint32_t* __restrict__ in, BigD bt, Ptab pt, EpiD epi) {
-  colinv_body<LOGR>(in, bt, pt, epi);
+  colinv_body<LOGR, PLAIN>(in, bt, pt, epi);
 }
 
 template <int LOGR>
@@ -1095,9 +1123,9 @@ struct ColTable {
     ((logR == L ? (r = k_colfwd_t<L>, 0) : 0), ...);
     return r;
   }
-  static ColInvFn inv(int logR) {
+  static ColInvFn inv(int logR, bool plain) {
     ColInvFn r = nullptr;
-    ((logR == L ? (r = k_colinv_t<L>, 0) : 0), ...);
+    ((logR == L ? (r = plain ? k_colinv_t<L, true> : k_colinv_t<L, false>, 0) : 0), ...);
     return r;
   }
   static int words(int logR) {
@@ -1117,7 +1145,8 @@ struct ColTable {
       if (r != cudaSuccess) e = r;
     };
     (set((const void*)k_colfwd_t<L>, ColCfg<L>::SMEM_WORDS * 4), ...);
-    (set((const void*)k_colinv_t<L>, ColCfg<L>::SMEM_WORDS * 4), ...);
+    (set((const void*)k_colinv_t<L, true>, ColCfg<L>::SMEM_WORDS * 4), ...);
+    (set((const void*)k_colinv_t<L, false>, ColCfg<L>::SMEM_WORDS * 4), ...);
     return e;
   }
 };
@@ -1153,7 +1182,7 @@ cudaError_t launch_colinv(const PrimeTables& pt, const BigTables& bt, const uint
   BigD d{bt.logR, bt.logC, Cols::logw(bt.logR),
          reinterpret_cast<const uint2*>(mont_scaled ? bt.lo_inv_r : bt.lo_inv),
          reinterpret_cast<const uint2*>(bt.hi_inv)};
-  ColInvFn fn = Cols::inv(bt.logR);
+  ColInvFn fn = Cols::inv(bt.logR, host_epi_plain(epi));
   if (!fn || d.logW > bt.logC) return cudaErrorInvalidValue;
   fn<<<1u << (bt.logC - d.logW), 256, Cols::words(bt.logR) * 4, s>>>(in, d, dev_tab(pt), dev_epi(epi));
   return cudaGetLastError();
@@ -1231,10 +1260,10 @@ __global__ void __launch_bounds__(256, 3) k_rows12_b(const BigJobB* __restrict__
   rows12_body(j.t[0], j.ymode == 1 ? j.t[1] : j.yspec, j.ymode, j.yspec_out, 1, 1, j.pt, blockIdx.x);
 }
 
-template <int LOGR>
+template <int LOGR, bool PLAIN>
 __global__ void __launch_bounds__(256, 3) k_colinv_b(const BigJobB* __restrict__ jobs) {
   const BigJobB& j = jobs[blockIdx.y];
-  colinv_body<LOGR>(j.t[0], j.bi, j.pt, j.epi);
+  colinv_body<LOGR, PLAIN>(j.t[0], j.bi, j.pt, j.epi);
 }
 
 __global__ void k_direct_b(const DirectJobB* __restrict__ jobs) {
@@ -1271,9 +1300,9 @@ struct ColBatch {
     ((logR == L ? (r = k_colfwd_b<L>, 0) : 0), ...);
     return r;
   }
-  static BatchFn inv(int logR) {
+  static BatchFn inv(int logR, bool plain) {
     BatchFn r = nullptr;
-    ((logR == L ? (r = k_colinv_b<L>, 0) : 0), ...);
+    ((logR == L ? (r = plain ? k_colinv_b<L, true> : k_colinv_b<L, false>, 0) : 0), ...);
     return r;
   }
   static cudaError_t launch(int logR, dim3 grid, const BigJobB* jobs, int smem, cudaStream_t s) {
@@ -1282,8 +1311,8 @@ struct ColBatch {
     fn<<<grid, 256, smem, s>>>(jobs);
     return cudaGetLastError();
   }
-  static cudaError_t launch_inv(int logR, dim3 grid, const BigJobB* jobs, int smem, cudaStream_t s) {
-    BatchFn fn = inv(logR);
+  static cudaError_t launch_inv(int logR, bool plain, dim3 grid, const BigJobB* jobs, int smem, cudaStream_t s) {
+    BatchFn fn = inv(logR, plain);
     if (!fn) return cudaErrorInvalidValue;
     fn<<<grid, 256, smem, s>>>(jobs);
     return cudaGetLastError();
@@ -1295,7 +1324,8 @@ struct ColBatch {
       if (r != cudaSuccess) e = r;
     };
     (set((const void*)k_colfwd_b<L>, ColCfg<L>::SMEM_WORDS * 4), ...);
-    (set((const void*)k_colinv_b<L>, ColCfg<L>::SMEM_WORDS * 4), ...);
+    (set((const void*)k_colinv_b<L, true>, ColCfg<L>::SMEM_WORDS * 4), ...);
+    (set((const void*)k_colinv_b<L, false>, ColCfg<L>::SMEM_WORDS * 4), ...);
     set((const void*)k_small_b, 2 * padded_words(1 << kSmallLog) * 4);
     return e;
   }
@@ -1329,6 +1359,7 @@ struct BatchGroup {
   bool big;
   size_t off;
   int count;
+  bool plain;  // every job's epilogue is plain
 };
 inline size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
 
@@ -1366,6 +1397,8 @@ cudaError_t launch_batch(const BatchPlan& b, void* host_staging, void* dev_desc,
     grp.big = big;
     grp.off = off;
     grp.count = (int)(e - k);
+    grp.plain = true;
+    for (size_t q = k; q < e; ++q) grp.plain = grp.plain && host_epi_plain(b.xjobs[order[q]].epi);
     groups.push_back(grp);
     for (size_t q = k; q < e; ++q) {
       const XJob& x = b.xjobs[order[q]];
@@ -1487,7 +1520,7 @@ cudaError_t launch_batch(const BatchPlan& b, void* host_staging, void* dev_desc,
       if (e != cudaSuccess) return e;
       k_rows12_b<<<dim3(1u << logR, cnt), 256, 0, s>>>(jobs);
       if ((e = cudaGetLastError()) != cudaSuccess) return e;
-      e = ColsB::launch_inv(logR, dim3(1u << (logC - logW), cnt), jobs, smem, s);
+      e = ColsB::launch_inv(logR, g.plain, dim3(1u << (logC - logW), cnt), jobs, smem, s);
       if (e != cudaSuccess) return e;
     }
   }

@@ -19,11 +19,13 @@ namespace fpx_dev {
 // mod s.  Forward: levels len = 2^LL .. 2^(LL-G+1); inverse: the reverse.
 // Twiddle index for level l, pair j: (len/2) + base + j*s.
 // ---------------------------------------------------------------------------
-template <int G, int LL, bool INV, int NA, bool ZB = false>
+template <int G, int LL, bool INV, int NA, bool ZB = false, bool ZH = false>
 __device__ __forceinline__ void bf_group(uint32_t (&x)[2][1 << G], const uint2* __restrict__ tw, int base,
                                          const Fp& f) {
   // ZB: base == 0 (the last group of a transform), so every j == 0 twiddle is 1
   // and its butterfly needs no multiplication.
+  // ZH (forward only): the upper half x[E/2..E) is zero (zero-padded input), so
+  // the first level is u' = u, v' = u * w and x[E/2..E) need not hold anything.
   constexpr int E = 1 << G;
   constexpr int S = LL - G;
   uint2 w[E];  // w[hs + j]: twiddle of pair j at the level with pair distance hs
@@ -36,8 +38,14 @@ __device__ __forceinline__ void bf_group(uint32_t (&x)[2][1 << G], const uint2* 
     }
   }
   if (!INV) {
+    if constexpr (ZH) {
 #pragma unroll
-    for (int hs = E / 2; hs >= 1; hs >>= 1) {
+      for (int i = 0; i < E / 2; ++i)
+#pragma unroll
+        for (int a = 0; a < NA; ++a) x[a][i + E / 2] = (ZB && i == 0) ? x[a][i] : shoup(x[a][i], w[E / 2 + i], f.p);
+    }
+#pragma unroll
+    for (int hs = ZH ? E / 4 : E / 2; hs >= 1; hs >>= 1) {
 #pragma unroll
       for (int i = 0; i < E; ++i)
         if (!(i & hs)) {

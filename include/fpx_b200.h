@@ -76,6 +76,10 @@ int fpx_release_pool(fpx_ctx* ctx);
 int fpx_profile(fpx_ctx* ctx, int enable);
 int fpx_profile_report(fpx_ctx* ctx, char* buf, size_t cap, size_t* needed);
 uint64_t fpx_launch_count(fpx_ctx* ctx);
+/* The GPU's measured 32-bit integer multiply rate (thread-level mul.hi.u32 and
+ * mad.lo.u32 instructions per second, all SMs busy, CUDA-event timed): the
+ * compute denominator of the transform roofline.  No context needed. */
+int fpx_measure_imad_rate(int device, double* per_second);
 
 /* ---- transforms (NttPlan<M>::forward / inverse, ntt.hpp:140-192) -------------
  * In place, n a power of two with 2 <= n <= 2^v2(p-1), p < 2^30 odd.  forward

@@ -78,3 +78,20 @@ def test_batch_rejects_null_context():
     lib = F.load_library()
     assert lib.fpx_batch_run(None, None, 0, 0) == F.EINVAL
     assert lib.fpx_batch_submit(None, None, 0) == F.EINVAL
+
+
+def test_serve_plan_bytes_without_device():
+    """The admission measure needs no GPU: native products plan two N-word
+    buffers, CRT products three primes' worth plus their residues."""
+    import numpy as np
+    keep = []
+    a = np.ones(1 << 16, np.uint32)
+    native, _, _ = F.make_job(("conv", 998244353, a, a), keep)
+    crt, _, _ = F.make_job(("conv", 1000000007, a, a), keep)
+    lib = F.load_library()
+    nb = lib.fpx_serve_plan_bytes(ctypes.byref(native))
+    cb = lib.fpx_serve_plan_bytes(ctypes.byref(crt))
+    N = 1 << 17
+    assert nb >= 4 * (2 * N) and nb < 4 * (6 * N)
+    assert cb > 2.5 * nb
+    assert lib.fpx_serve_plan_bytes(None) == 0
