@@ -642,8 +642,8 @@ def run_serve_fpx(args):
     specs = serve_mix(count, max_log=args.serve_max_log)
     srv = F.Server(local, workers=args.workers)
     try:
-        # warm-up: plans, pools, pinned buffers
-        for t in [srv.submit(s) for s in serve_mix(64, seed=9, max_log=args.serve_max_log)]:
+        # warm-up: plans, pools and pinned buffers of every worker, on the same mix
+        for t in [srv.submit(s) for s in specs]:
             srv.poll(t)
         # saturation: everything offered at once
         t0 = time.perf_counter()
@@ -691,7 +691,7 @@ def run_serve_fpx(args):
         srv.stop()
     in_bytes = 4 * sum(len(s[2]) + (len(s[3]) if s[0] in ("conv", "divmod") else 0) for s in specs)
     line = {"metric": "served requests/s at saturation (mixed ops, sizes 2^8..2^%d)" % args.serve_max_log,
-            "value": round(sat_rate, 2), "unit": "req/s", "n_gpus": 1, "steps": count, "warmup": 64,
+            "value": round(sat_rate, 2), "unit": "req/s", "n_gpus": 1, "steps": count, "warmup": count,
             "ms_per_step": round(1e3 / sat_rate, 3), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "u32", "data": "synthetic",
             "config": {"workload": "conv 40 / inv 20 / exp 15 / sqrt 10 / divmod 10 / pow 5 %, sizes log-uniform "
@@ -706,14 +706,119 @@ def run_serve_fpx(args):
     return 0
 
 
+def ops_cases():
+    """Single operations of the reference's configs 1-3 (seeded uniform residues)."""
+    rng = np.random.default_rng(6)
+
+    def r(p, n, a0=None):
+        a = rng.integers(0, p, n, dtype=np.uint64).astype(np.uint32)
+        if a0 is not None:
+            a[0] = a0
+        return a
+
+    p, q = 998244353, 1000000007
+    n22 = 1 << 22
+    sq = None
+    return [
+        ("C1 conv 2^18 x 2^18", "conv", p, (r(p, 1 << 18), r(p, 1 << 18)), None),
+        ("H1 conv 2^22 x 2^22", "conv", p, (r(p, n22), r(p, n22)), None),
+        ("H2 conv 2^23 x 2^23 (CRT)", "conv", p, (r(p, 1 << 23), r(p, 1 << 23)), None),
+        ("C2 inv 2^22", "inv", p, (r(p, n22, 1),), n22),
+        ("C2 log 2^22", "log", p, (r(p, n22, 1),), n22),
+        ("C2 exp 2^22", "exp", p, (r(p, n22, 0),), n22),
+        ("C2 sqrt 2^22", "sqrt", p, (r(p, n22, 1),), n22),
+        ("C2 pow k=1000003 2^22", "pow", p, (r(p, n22), 1000003), n22),
+        ("C3 conv 2^23 x 2^23 mod 1e9+7", "conv", q, (r(q, 1 << 23), r(q, 1 << 23)), None),
+        ("C3 inv 2^22 mod 1e9+7", "inv", q, (r(q, n22, int(rng.integers(1, q))),), n22),
+        ("C3 conv 2^25 x 2^25 mod 1e9+7", "conv", q, (r(q, 1 << 25), r(q, 1 << 25)), None),
+    ]
+
+
+def run_ops_fpx(args):
+    """Device-resident time of each single operation (CUDA events, median of
+    `reps`), output Mcoeff/s; the reference's single-threaded time beside it
+    where one call takes under ~3 s on the host."""
+    import torch
+    import fastpoly_b200 as F
+    from oracle.oracle import Reference, OP_CONV, OP_INV, OP_LOG, OP_EXP, OP_SQRT, OP_POW
+
+    rank, local, world = env_rank()
+    torch.cuda.set_device(local)
+    ctx = F.Context(local)
+    stream = torch.cuda.Stream()
+    ctx.set_stream(stream.cuda_stream)
+    torch.cuda.set_stream(stream)
+    ref = None if args.no_cpu_baseline else Reference.load()
+    codes = {"conv": OP_CONV, "inv": OP_INV, "log": OP_LOG, "exp": OP_EXP, "sqrt": OP_SQRT, "pow": OP_POW}
+    rows = []
+    for name, op, p, ins, n in ops_cases():
+        a = ins[0]
+        da = torch.from_numpy(a.view(np.int32)).cuda()
+        if op == "conv":
+            b = ins[1]
+            db = torch.from_numpy(b.view(np.int32)).cuda()
+            outn = a.size + b.size - 1
+        else:
+            outn = n
+        dout = torch.empty(outn, dtype=torch.int32, device="cuda")
+
+        def call():
+            if op == "conv":
+                ctx.conv_device(p, da, a.size, db, b.size, None, dout)
+            elif op == "pow":
+                ctx.pow_device(p, da, a.size, ins[1], n, dout)
+            else:
+                getattr(ctx, op + "_device")(p, da, a.size, n, dout)
+
+        call()
+        torch.cuda.synchronize()
+        reps = 5
+        ts = []
+        for _ in range(reps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            call()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ts.append(e0.elapsed_time(e1))
+        ms = float(np.median(ts))
+        row = {"case": name, "p": p, "out_terms": outn, "gpu_ms": round(ms, 3),
+               "gpu_mcoeff_s": round(outn / (ms * 1e-3) / 1e6, 1)}
+        if ref is not None and outn <= (1 << 24) and not (op == "conv" and p != 998244353 and outn > (1 << 24)):
+            if op == "conv":
+                _, _, t = ref.run(OP_CONV, p, a, b, cap=outn + 1)
+            elif op == "pow":
+                _, _, t = ref.run(OP_POW, p, a, n=n, k=ins[1], cap=n)
+            else:
+                _, _, t = ref.run(codes[op], p, a, n=n, cap=n)
+            row["cpu_ref_1thread_ms"] = round(1e3 * float(t[0]), 1)
+            row["speedup_vs_1_core"] = round(1e3 * float(t[0]) / ms, 1)
+        rows.append(row)
+        del da, dout
+        if op == "conv":
+            del db
+        torch.cuda.empty_cache()
+    line = {"metric": "single-operation Mcoeff/s, configs 1-3", "value": rows[1]["gpu_mcoeff_s"], "unit": "Mcoeff/s",
+            "n_gpus": 1, "higher_is_better": True, "dtype": "u32", "data": "synthetic",
+            "config": {"workload": "configs 1-3 single operations, device-resident, CUDA events, median of 5"},
+            "ops": rows}
+    if ref is not None:
+        line["cpu_baseline"] = {"kind": "reference", "cores": 1, "backend": ref.backend,
+                                "sample": "one call per case (cases whose output exceeds 2^24 terms skipped)"}
+    print(json.dumps(line))
+    ctx.close()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="fpx", choices=["fpx", "reference"])
-    ap.add_argument("--workload", default="conv", choices=["conv", "batch", "serve"],
-                    help="conv: the headline 2^23 conv (default); batch: mixed batch; serve: request loop")
+    ap.add_argument("--workload", default="conv", choices=["conv", "batch", "serve", "ops"],
+                    help="conv: the headline 2^23 conv (default); batch: mixed batch; serve: request loop; "
+                         "ops: single operations of configs 1-3")
     ap.add_argument("--requests", type=int, default=300, help="serve: requests per load level")
     ap.add_argument("--serve-max-log", type=int, default=22, help="serve: largest size 2^k")
     ap.add_argument("--workers", type=int, default=2, help="serve: micro-batches in flight")
@@ -722,6 +827,8 @@ def main():
     args.warmup = max(args.warmup, 3)
     if args.workload == "batch":
         return run_batch_reference(args) if args.impl == "reference" else run_batch_fpx(args)
+    if args.workload == "ops":
+        return run_ops_fpx(args)
     if args.workload == "serve":
         if args.impl == "reference":
             rank, _, world = env_rank()

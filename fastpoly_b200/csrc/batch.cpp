@@ -216,9 +216,11 @@ Engine::Stage& Engine::stage(size_t bytes) {
 }
 
 void Engine::free_stages() {
-  if (pin_) cudaFreeHost(pin_);
-  pin_ = nullptr;
-  pin_words_ = 0;
+  for (Pin& q : pins_) {
+    if (q.host) cudaFreeHost(q.host);
+    if (q.ev) cudaEventDestroy(q.ev);
+    q = Pin();
+  }
   for (Stage& s : stages_) {
     if (s.host) cudaFreeHost(s.host);
     if (s.ev) cudaEventDestroy(s.ev);
@@ -698,30 +700,21 @@ void Engine::batch_host(fpx_job* jobs, size_t count, int repr) {
     out_words += o + o2;
   }
   const size_t total = in_words + out_words;
-  if (total > pin_words_) {
-    if (pin_) cudaFreeHost(pin_);
-    pin_ = nullptr;
-    pin_words_ = 0;
-    const size_t want = total + total / 4 + 1024;
-    check(cudaMallocHost(&pin_, want * 4), "cudaMallocHost");
-    pin_words_ = want;
-  }
-  uint32_t* hin = pin_;
-  uint32_t* hout = pin_ + in_words;
   Buf dbuf(&pool_, total ? total : 1);
   uint32_t* din = dbuf.get();
   uint32_t* dout = din + in_words;
   std::vector<fpx_job> dj(jobs, jobs + count);
   std::vector<ReprSeg> segs;
+  std::vector<HostSpan> ins;
   size_t qi = 0, qo = 0;
   for (size_t i = 0; i < count; ++i) {
     const fpx_job& j = jobs[i];
     fpx_job& d = dj[i];
-    if (wa[i]) std::memcpy(hin + qi, j.a, wa[i] * 4);
+    if (wa[i]) ins.push_back(HostSpan{j.a, nullptr, wa[i]});
     d.a = j.a ? din + qi : nullptr;
     if (wa[i]) segs.push_back(ReprSeg{j.p, din + qi, wa[i], 0});
     qi += wa[i];
-    if (wb[i]) std::memcpy(hin + qi, j.b, wb[i] * 4);
+    if (wb[i]) ins.push_back(HostSpan{j.b, nullptr, wb[i]});
     d.b = j.b ? din + qi : nullptr;
     if (wb[i]) segs.push_back(ReprSeg{j.p, din + qi, wb[i], 0});
     qi += wb[i];
@@ -732,7 +725,7 @@ void Engine::batch_host(fpx_job* jobs, size_t count, int repr) {
     d.out2 = j.out2 ? dout + qo : nullptr;
     qo += wo2[i];
   }
-  if (in_words) check(cudaMemcpyAsync(din, hin, in_words * 4, cudaMemcpyHostToDevice, stream_), "H2D");
+  copy_in(ins, din);
   if (repr == FPX_REPR_MONTGOMERY) convert_repr(segs);
   batch(dj.data(), count);
   if (repr == FPX_REPR_MONTGOMERY) {
@@ -745,21 +738,99 @@ void Engine::batch_host(fpx_job* jobs, size_t count, int repr) {
     }
     convert_repr(segs);
   }
-  if (out_words) check(cudaMemcpyAsync(hout, dout, out_words * 4, cudaMemcpyDeviceToHost, stream_), "D2H");
-  sync();
-  qo = 0;
+  // every job's output region, in device order: its result words go to the
+  // caller's buffer, the rest of the region is skipped
+  std::vector<HostSpan> outs;
   for (size_t i = 0; i < count; ++i) {
     fpx_job& j = jobs[i];
     const fpx_job& d = dj[i];
     j.status = d.status;
     j.out_len = d.out_len;
     j.out2_len = d.out2_len;
-    if (d.status == FPX_OK) {
-      if (j.out && d.out_len) std::memcpy(j.out, hout + qo, std::min(d.out_len, wo[i]) * 4);
-      if (j.out2 && d.out2_len) std::memcpy(j.out2, hout + qo + wo[i], std::min(d.out2_len, wo2[i]) * 4);
-    }
-    qo += wo[i] + wo2[i];
+    const bool ok = d.status == FPX_OK;
+    const size_t n1 = ok && j.out ? std::min(d.out_len, wo[i]) : 0;
+    const size_t n2 = ok && j.out2 ? std::min(d.out2_len, wo2[i]) : 0;
+    if (n1) outs.push_back(HostSpan{nullptr, j.out, n1});
+    if (wo[i] > n1) outs.push_back(HostSpan{nullptr, nullptr, wo[i] - n1});
+    if (n2) outs.push_back(HostSpan{nullptr, j.out2, n2});
+    if (wo2[i] > n2) outs.push_back(HostSpan{nullptr, nullptr, wo2[i] - n2});
   }
+  copy_out(dout, outs);
+}
+
+// --------------------------------------------------------- pinned staging
+
+namespace {
+constexpr size_t kPinWords = size_t(8) << 20;  // 32 MiB per slot
+}
+
+uint32_t* Engine::pin_slot(int k) {
+  Pin& q = pins_[k];
+  if (!q.host) {
+    check(cudaMallocHost(&q.host, kPinWords * 4), "cudaMallocHost");
+    check(cudaEventCreateWithFlags(&q.ev, cudaEventDisableTiming), "cudaEventCreate");
+  } else {
+    check(cudaEventSynchronize(q.ev), "staging wait");
+  }
+  return q.host;
+}
+
+void Engine::copy_in(const std::vector<HostSpan>& spans, uint32_t* dst) {
+  size_t si = 0, so = 0;
+  int k = 0;
+  while (si < spans.size()) {
+    uint32_t* h = pin_slot(k);
+    size_t filled = 0;
+    while (si < spans.size() && filled < kPinWords) {
+      const size_t take = std::min(spans[si].words - so, kPinWords - filled);
+      std::memcpy(h + filled, spans[si].src + so, take * 4);
+      filled += take;
+      so += take;
+      if (so == spans[si].words) {
+        ++si;
+        so = 0;
+      }
+    }
+    check(cudaMemcpyAsync(dst, h, filled * 4, cudaMemcpyHostToDevice, stream_), "H2D");
+    check(cudaEventRecord(pins_[k].ev, stream_), "event");
+    dst += filled;
+    k ^= 1;
+  }
+}
+
+void Engine::copy_out(const uint32_t* src, const std::vector<HostSpan>& spans) {
+  size_t total = 0;
+  for (const HostSpan& s : spans) total += s.words;
+  const size_t chunks = (total + kPinWords - 1) / kPinWords;
+  size_t si = 0, so = 0;
+  auto issue = [&](size_t c) {  // D2H of chunk c into slot c % 2
+    const int k = (int)(c & 1);
+    uint32_t* h = pin_slot(k);
+    const size_t off = c * kPinWords, w = std::min(kPinWords, total - off);
+    check(cudaMemcpyAsync(h, src + off, w * 4, cudaMemcpyDeviceToHost, stream_), "D2H");
+    check(cudaEventRecord(pins_[k].ev, stream_), "event");
+  };
+  if (chunks > 0) issue(0);
+  if (chunks > 1) issue(1);
+  for (size_t c = 0; c < chunks; ++c) {
+    const int k = (int)(c & 1);
+    check(cudaEventSynchronize(pins_[k].ev), "D2H wait");
+    const uint32_t* h = pins_[k].host;
+    const size_t w = std::min(kPinWords, total - c * kPinWords);
+    size_t used = 0;
+    while (used < w) {
+      const size_t take = std::min(spans[si].words - so, w - used);
+      if (spans[si].dst) std::memcpy(spans[si].dst + so, h + used, take * 4);
+      used += take;
+      so += take;
+      if (so == spans[si].words) {
+        ++si;
+        so = 0;
+      }
+    }
+    if (c + 2 < chunks) issue(c + 2);
+  }
+  sync();
 }
 
 }  // namespace fpx

@@ -177,8 +177,23 @@ class Engine {
   static constexpr int kStages = 4;
   Stage stages_[kStages];
   int stage_next_ = 0;
-  uint32_t* pin_ = nullptr;  // pinned packing buffer of batch_host
-  size_t pin_words_ = 0;
+  // Two pinned staging slots of batch_host: host copies into one slot overlap
+  // the DMA of the other.
+  struct Pin {
+    uint32_t* host = nullptr;
+    cudaEvent_t ev = nullptr;  // recorded after the slot's last copy
+  };
+  Pin pins_[2];
+  uint32_t* pin_slot(int k);  // waits for the slot's last copy
+  struct HostSpan {
+    const uint32_t* src;  // copy_in: host source
+    uint32_t* dst;        // copy_out: host destination (null: skip)
+    size_t words;
+  };
+  // Host spans, concatenated, -> dst (device), through the pinned slots.
+  void copy_in(const std::vector<HostSpan>& spans, uint32_t* dst);
+  // Device region [src, src + sum(words)) -> host spans (null ones skipped).
+  void copy_out(const uint32_t* src, const std::vector<HostSpan>& spans);
   // Next ring slot, holding >= bytes, whose previous copy has completed.
   Stage& stage(size_t bytes);
   void free_stages();
