@@ -668,12 +668,32 @@ __global__ void k_exp_prep_b(const ExpPrepB* __restrict__ jobs) {
 }
 
 // First (mode 0) or last (mode 1) index in [0, n) with a[i] != 0; n if none.
-__global__ void k_find_nonzero(const uint32_t* a, size_t n, int mode, unsigned long long* res) {
-  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+// Each thread keeps its own first / last hit, the block reduces them, and one
+// atomic per block updates *res (dense inputs would otherwise serialise on a
+// single address).  Mode 1 reports 0 both for "index 0" and "none"; the caller
+// tells them apart.
+__global__ void __launch_bounds__(256) k_find_nonzero(const uint32_t* a, size_t n, int mode, unsigned long long* res) {
+  unsigned long long hit = 0;  // index + 1, 0 = none
+  const size_t stride = (size_t)gridDim.x * blockDim.x;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += stride) {
     if (a[i]) {
-      if (mode == 0) atomicMin(res, (unsigned long long)i);
-      else atomicMax(res, (unsigned long long)i);
+      hit = i + 1;
+      if (mode == 0) break;  // a thread's indices only grow
     }
+  }
+  __shared__ unsigned long long red_sm[8];
+  unsigned long long v = hit ? hit - 1 : (mode == 0 ? ~0ull : 0ull);
+  for (int o = 16; o; o >>= 1) {
+    const unsigned long long u = __shfl_xor_sync(0xffffffffu, v, o);
+    v = mode == 0 ? (u < v ? u : v) : (u > v ? u : v);
+  }
+  if ((threadIdx.x & 31) == 0) red_sm[threadIdx.x >> 5] = v;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int w = 1; w < (int)(blockDim.x >> 5); ++w)
+      v = mode == 0 ? (red_sm[w] < v ? red_sm[w] : v) : (red_sm[w] > v ? red_sm[w] : v);
+    if (mode == 0 && v != ~0ull) atomicMin(res, v);
+    if (mode == 1 && v != 0) atomicMax(res, v);
   }
 }
 
@@ -954,15 +974,18 @@ __device__ __forceinline__ void col_group_smem(uint32_t* sm, const uint2* tw, co
     const int rest = inst >> C::LOGW;
     const int base = rest & ((1 << S) - 1);
     const int p0 = ((rest >> S) << T) + base;
+    using A = typename C::P::template Group<S + C::LOGW, G>;
+    int ab[A::P];
+    A::bases((p0 << C::LOGW) + c, ab);
     uint32_t v[2][1 << G];
 #pragma unroll
     for (int i = 0; i < (ZH ? (1 << G) / 2 : (1 << G)); ++i) {
-      const uint32_t x = sm[C::P::at(((p0 + (i << S)) << C::LOGW) + c)];
+      const uint32_t x = sm[A::addr(ab, i)];
       v[0][i] = REDUCE ? reduce_any(x, q1, f) : x;
     }
     bf_group<G, T, INV, 1, false, ZH>(v, tw, base, f);
 #pragma unroll
-    for (int i = 0; i < (1 << G); ++i) sm[C::P::at(((p0 + (i << S)) << C::LOGW) + c)] = v[0][i];
+    for (int i = 0; i < (1 << G); ++i) sm[A::addr(ab, i)] = v[0][i];
   }
 }
 
@@ -1017,10 +1040,13 @@ __device__ __forceinline__ void colfwd_body(const InD& in, uint32_t* __restrict_
     const int c = inst & (C::W - 1);
     const int b = inst >> C::LOGW;
     const int p0 = b << G;
+    using A = typename C::P::template Group<C::LOGW, G>;
+    int ab[A::P];
+    A::bases((p0 << C::LOGW) + c, ab);
     uint32_t v[2][1 << G];
 #pragma unroll
     for (int i = 0; i < (1 << G); ++i) {
-      const uint32_t x = sm[C::P::at(((p0 + i) << C::LOGW) + c)];
+      const uint32_t x = sm[A::addr(ab, i)];
       v[0][i] = reduce_here ? reduce_any(x, pt.q1, f) : x;
     }
     bf_group<G, G, false, 1, true>(v, pt.fwd, 0, f);
@@ -1066,11 +1092,14 @@ __device__ __forceinline__ void colinv_body(const uint32_t* __restrict__ in, con
       const uint32_t j = j0 + c;
       const uint32_t eb = j * brev_c(b, LOGR - G);
       const uint32_t js = j << (LOGR - G);
+      using A = typename C::P::template Group<C::LOGW, G>;
+      int ab[A::P];
+      A::bases((p0 << C::LOGW) + c, ab);
       uint32_t v[2][1 << G];
 #pragma unroll
       for (int i = 0; i < (1 << G); ++i) {
         const uint32_t ex = eb + js * brev_c(i, G);
-        uint32_t w = shoup(sm[C::P::at(((p0 + i) << C::LOGW) + c)], __ldg(bt.lo + (ex & 4095u)), f.p);
+        uint32_t w = shoup(sm[A::addr(ab, i)], __ldg(bt.lo + (ex & 4095u)), f.p);
         v[0][i] = shoup(w, __ldg(bt.hi + (ex >> 12)), f.p);
       }
       bf_group<G, G, true, 1, true>(v, pt.inv, 0, f);
@@ -1079,7 +1108,7 @@ __device__ __forceinline__ void colinv_body(const uint32_t* __restrict__ in, con
         for (int i = 0; i < (1 << G); ++i) epi_store_t<PLAIN>(epi, (uint32_t)(((p0 + i) << logC) + j), v[0][i], f);
       } else {
 #pragma unroll
-        for (int i = 0; i < (1 << G); ++i) sm[C::P::at(((p0 + i) << C::LOGW) + c)] = v[0][i];
+        for (int i = 0; i < (1 << G); ++i) sm[A::addr(ab, i)] = v[0][i];
       }
     }
   }
@@ -1094,9 +1123,12 @@ __device__ __forceinline__ void colinv_body(const uint32_t* __restrict__ in, con
     for (int inst = tid; inst < NINST; inst += 256) {
       const int c = inst & (C::W - 1);
       const int base = inst >> C::LOGW;
+      using A = typename C::P::template Group<S + C::LOGW, G>;
+      int ab[A::P];
+      A::bases((base << C::LOGW) + c, ab);
       uint32_t v[2][1 << G];
 #pragma unroll
-      for (int i = 0; i < (1 << G); ++i) v[0][i] = sm[C::P::at(((base + (i << S)) << C::LOGW) + c)];
+      for (int i = 0; i < (1 << G); ++i) v[0][i] = sm[A::addr(ab, i)];
       bf_group<G, LOGR, true, 1>(v, pt.inv, base, f);
 #pragma unroll
       for (int i = 0; i < (1 << G); ++i)

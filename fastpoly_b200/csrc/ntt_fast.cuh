@@ -106,13 +106,30 @@ __device__ __forceinline__ int posC(int t, int i) { return (t << 4) + i; }
 // address arithmetic saves.
 template <int LOGR, int LOGW, int GL>
 struct ColSwz {
+  static constexpr bool ON = GL + LOGW >= 5 && LOGW < 5;
+  static constexpr int SH = GL + LOGW;         // the XOR key is a >> SH
+  static constexpr int MB = ON ? 5 - LOGW : 0;  // key bits
   __host__ __device__ static constexpr int at(int a) {
-    if constexpr (GL + LOGW >= 5 && LOGW < 5) {
-      return a ^ (((a >> (GL + LOGW)) & ((32 >> LOGW) - 1)) << LOGW);
+    if constexpr (ON) {
+      return a ^ (((a >> SH) & ((1 << MB) - 1)) << LOGW);
     } else {
       return a;
     }
   }
+  // Addresses of the 2^G points of one group instance, element i at unswizzled
+  // word a0 + (i << SS): the XOR key is periodic in i with period P, so
+  // at(a_{kP+r}) = at(a_r) + k (P << SS) and a thread computes P swizzled bases
+  // per instance, the rest being compile-time offsets.
+  template <int SS, int G>
+  struct Group {
+    static constexpr int P0 = !ON ? 1 : (SS >= SH + MB ? 1 : (SS >= SH ? 1 << (SH + MB - SS) : 1 << MB));
+    static constexpr int P = P0 < (1 << G) ? P0 : (1 << G);
+    __device__ __forceinline__ static void bases(int a0, int (&b)[P]) {
+#pragma unroll
+      for (int r = 0; r < P; ++r) b[r] = at(a0 + (r << SS));
+    }
+    __device__ __forceinline__ static int addr(const int (&b)[P], int i) { return b[i % P] + (i / P) * (P << SS); }
+  };
 };
 
 // Asynchronous global -> shared copies (cp.async), zero-filling past src_bytes.
