@@ -450,7 +450,8 @@ void Engine::cyc_product(uint32_t p, int logN, const CycOp& op) {
     if (epi.scale.w) s = s * epi.scale.w % p;
     epi.scale = shoup_pair((uint32_t)s, p);
     j.epi = epi;
-    kcheck(launch_small(pt, logN, j, stream_), "small");
+    if (logN == 12) kcheck(launch_cyc4096(pt, j, stream_), "cyc4096");
+    else kcheck(launch_cyc_small(pt, logN, j, stream_), "small");
     return;
   }
   const BigTables& bt = big_plan(p, logN).t;

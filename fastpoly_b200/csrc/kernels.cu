@@ -429,7 +429,8 @@ cudaError_t kernels_init() {
   set((const void*)k_colinv, padded_words(1 << 14) * 4);
   const cudaError_t r = kernels_fast_init();
   const cudaError_t r2 = kernels_batch_init();
-  return e != cudaSuccess ? e : (r != cudaSuccess ? r : r2);
+  const cudaError_t r3 = kernels_cyc_init();
+  return e != cudaSuccess ? e : (r != cudaSuccess ? r : (r2 != cudaSuccess ? r2 : r3));
 }
 
 cudaError_t launch_small(const PrimeTables& pt, int logN, const SmallJob& job, cudaStream_t s) {
@@ -592,47 +593,57 @@ __device__ uint32_t pow64(uint32_t a, uint64_t e, uint32_t p) {
 }
 __device__ __forceinline__ uint32_t inv64(uint32_t a, uint32_t p) { return p == 2 ? a : pow64(a, p - 2, p); }
 
-// Warp-wide sum mod p of per-lane values < p.
-__device__ __forceinline__ uint32_t warp_sum_mod(uint32_t v, uint32_t p) {
-  uint64_t s = v;
-#pragma unroll
-  for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-  return (uint32_t)(s % p);
-}
 
 // kind 0: inverse seed   c[i] = -(sum_{j=1..i, j<la} a[j] c[i-j]) * c[0], c[0] = 1/a[0]
 // kind 1: exp seed       b[i] = (sum_{j=1..min(i,la)} a[j-1] b[i-j]) / i,   b[0] = 1   (a = a')
 // kind 2: sqrt seed      b[i] = (u[i] - sum_{j=1..i-1} b[j] b[i-j]) * w,     b[0] = r0, w = 1/(2 r0)
-// One warp; n <= 64.  Writes out[0..n).
+// One warp; n <= 64.  Writes out[0..n).  The operands (in Montgomery form for
+// odd p) and, for exp, the inverses 1/i are staged in shared memory by all
+// lanes first; each step is then lane-parallel Montgomery products and a
+// 32-bit modular warp sum.
 __device__ __forceinline__ void seed_body(int kind, uint32_t p, const uint32_t* a, size_t la, uint32_t* out, int n,
                                           uint32_t r0) {
-  __shared__ uint32_t c[64];
+  __shared__ uint32_t c[64], cm[64], am[64], iv[64];
   const int lane = threadIdx.x;
+  const bool odd = (p & 1u) != 0;
+  const Fp f{p, 2 * p, odd ? inv_mod_2_32(p) : 1u};
+  const uint32_t R = (uint32_t)((((uint64_t)1) << 32) % p);
+  for (int i = lane; i < 64; i += 32) {
+    const uint32_t v = (size_t)i < la && i < n ? a[i] % p : 0u;
+    am[i] = odd ? mm64(v, R, p) : v;
+    iv[i] = (kind == 1 && i > 0 && i < n) ? inv64((uint32_t)i % p, p) : 0u;
+  }
   uint32_t w = 0;
   if (lane == 0) {
     if (kind == 0) c[0] = inv64(a[0] % p, p);
     else if (kind == 1) c[0] = 1 % p;
     else { c[0] = r0; w = inv64(mm64(2 % p, r0, p), p); }
+    cm[0] = odd ? mm64(c[0], R, p) : c[0];
   }
   w = __shfl_sync(0xffffffffu, w, 0);
   __syncwarp();
   for (int i = 1; i < n; ++i) {
     uint32_t part = 0;
     for (int j = 1 + lane; j <= i; j += 32) {
-      if (kind == 0) { if ((size_t)j < la) part = (uint32_t)((part + (uint64_t)mm64(a[j] % p, c[i - j], p)) % p); }
-      else if (kind == 1) { if ((size_t)j <= la) part = (uint32_t)((part + (uint64_t)mm64(a[j - 1] % p, c[i - j], p)) % p); }
-      else { if (j < i) part = (uint32_t)((part + (uint64_t)mm64(c[j], c[i - j], p)) % p); }
+      uint32_t t = 0;
+      if (kind == 0) t = (size_t)j < la ? (odd ? red(mont(am[j], c[i - j], f), p) : mm64(am[j], c[i - j], p)) : 0u;
+      else if (kind == 1) t = (size_t)j <= la ? (odd ? red(mont(am[j - 1], c[i - j], f), p) : mm64(am[j - 1], c[i - j], p)) : 0u;
+      else t = j < i ? (odd ? red(mont(cm[j], c[i - j], f), p) : mm64(c[j], c[i - j], p)) : 0u;
+      part = red(part + t, p);
     }
-    const uint32_t s = warp_sum_mod(part, p);
+#pragma unroll
+    for (int o = 16; o; o >>= 1) part = red(part + __shfl_xor_sync(0xffffffffu, part, o), p);
     if (lane == 0) {
+      const uint32_t sm_ = part;
       uint32_t v;
-      if (kind == 0) v = mm64(s ? p - s : 0u, c[0], p);
-      else if (kind == 1) v = mm64(s, inv64((uint32_t)i % p, p), p);
+      if (kind == 0) v = mm64(sm_ ? p - sm_ : 0u, c[0], p);
+      else if (kind == 1) v = mm64(sm_, iv[i], p);
       else {
         const uint32_t u = (size_t)i < la ? a[i] % p : 0u;
-        v = mm64(u >= s ? u - s : u + p - s, w, p);
+        v = mm64(u >= sm_ ? u - sm_ : u + p - sm_, w, p);
       }
       c[i] = v;
+      cm[i] = odd ? mm64(v, R, p) : v;
     }
     __syncwarp();
   }
@@ -1275,10 +1286,6 @@ struct GarnerJobB {
   uint32_t tpinv;
 };
 
-__global__ void __launch_bounds__(512) k_small_b(const SmallJobB* __restrict__ jobs, int logN) {
-  const SmallJobB& j = jobs[blockIdx.x];
-  small_body(j.d, j.pt, logN);
-}
 
 template <int LOGR>
 __global__ void __launch_bounds__(256, 3) k_colfwd_b(const BigJobB* __restrict__ jobs) {
@@ -1358,7 +1365,6 @@ struct ColBatch {
     (set((const void*)k_colfwd_b<L>, ColCfg<L>::SMEM_WORDS * 4), ...);
     (set((const void*)k_colinv_b<L, true>, ColCfg<L>::SMEM_WORDS * 4), ...);
     (set((const void*)k_colinv_b<L, false>, ColCfg<L>::SMEM_WORDS * 4), ...);
-    set((const void*)k_small_b, 2 * padded_words(1 << kSmallLog) * 4);
     return e;
   }
 };
@@ -1394,6 +1400,9 @@ struct BatchGroup {
   bool plain;  // every job's epilogue is plain
 };
 inline size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
+
+__global__ void __launch_bounds__(256) k_cyc4096_b(const SmallJobB* __restrict__ jobs);  // defined below
+cudaError_t launch_cyc_small_batch(int logN, unsigned count, const SmallJobB* jobs, cudaStream_t s);  // below
 
 }  // namespace
 
@@ -1534,12 +1543,14 @@ cudaError_t launch_batch(const BatchPlan& b, void* host_staging, void* dev_desc,
     }
   }
   for (const BatchGroup& g : groups) {
-    const uint32_t N = 1u << g.logN;
-    if (!g.big) {
-      int nt = (int)(N / 16);
-      nt = nt < 32 ? 32 : (nt > 512 ? 512 : nt);
-      k_small_b<<<g.count, nt, 2 * padded_words(N) * 4, s>>>(reinterpret_cast<const SmallJobB*>(d + g.off), g.logN);
+    if (!g.big && g.logN == 12) {
+      k_cyc4096_b<<<g.count, 256, 0, s>>>(reinterpret_cast<const SmallJobB*>(d + g.off));
       if ((e = cudaGetLastError()) != cudaSuccess) return e;
+      continue;
+    }
+    if (!g.big) {
+      e = launch_cyc_small_batch(g.logN, (unsigned)g.count, reinterpret_cast<const SmallJobB*>(d + g.off), s);
+      if (e != cudaSuccess) return e;
       continue;
     }
     const int logC = 12, logR = g.logN - logC;
@@ -1693,3 +1704,301 @@ cudaError_t launch_gather_first(const std::vector<const uint32_t*>& ptrs, void* 
   return cudaMemcpyAsync(host_out, dout, ptrs.size() * 4, cudaMemcpyDeviceToHost, s);
 }
 }  // namespace fpx
+
+// ===========================================================================
+// One cyclic product of exactly 4096 points in one CTA: the row pass's
+// register groups (three groups of four levels, padded conflict-free shared
+// layout, twiddles loaded per group up front) for the forward transform(s),
+// pointwise product and inverse, with the small-transform epilogue.  Replaces
+// the generic one-CTA kernel at this size (13.2 us against 16.4 us for the
+// generic kernel at half the size, one conv per call on B200).
+//
+// A thread-block-cluster version that spread 2^13..2^16-point products over
+// 2..16 CTAs, exchanging the cross-chunk butterfly levels through distributed
+// shared memory, was built and measured: 26 / 33 / 40 / 47 us against about
+// 25 us for the three two-pass launches (each cross-chunk level cost a remote
+// round trip and two cluster barriers), so those sizes stay two-pass.
+// ===========================================================================
+namespace {
+
+__device__ __forceinline__ void cyc4096_body(const SmallD& job, const Ptab& pt) {
+  __shared__ __align__(16) uint32_t sX[kRowWords];
+  __shared__ __align__(16) uint32_t sY[kRowWords];
+  const int t = threadIdx.x;
+  const int bA = baseA(t), bB = baseB(t), bC = baseC(t);
+  const Fp f = pt.f;
+  const int ymode = job.ymode;
+  uint32_t v[2][16];
+#pragma unroll
+  for (int i = 0; i < 16; ++i) {
+    v[0][i] = load_in(job.x, posA(t, i), f, pt.q1);
+    if (ymode == 1) v[1][i] = load_in(job.y, posA(t, i), f, pt.q1);
+  }
+  if (ymode == 1) {
+    bf_group<4, 12, false, 2>(v, pt.fwd, t, f);
+#pragma unroll
+    for (int i = 0; i < 16; ++i) {
+      sX[bA + offA(i)] = v[0][i];
+      sY[bA + offA(i)] = v[1][i];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < 16; ++i) {
+      v[0][i] = sX[bB + offB(i)];
+      v[1][i] = sY[bB + offB(i)];
+    }
+    bf_group<4, 8, false, 2>(v, pt.fwd, t & 15, f);
+#pragma unroll
+    for (int i = 0; i < 16; ++i) {
+      sX[bB + offB(i)] = v[0][i];
+      sY[bB + offB(i)] = v[1][i];
+    }
+    __syncthreads();
+    lds16(sX + bC, v[0]);
+    lds16(sY + bC, v[1]);
+    bf_group<4, 4, false, 2, true>(v, pt.fwd, 0, f);
+    if (job.yspec_out) {
+      uint4* o = reinterpret_cast<uint4*>(job.yspec_out + posC(t, 0));
+#pragma unroll
+      for (int q = 0; q < 4; ++q)
+        o[q] = make_uint4(red(v[1][4 * q], f.p), red(v[1][4 * q + 1], f.p), red(v[1][4 * q + 2], f.p),
+                          red(v[1][4 * q + 3], f.p));
+    }
+#pragma unroll
+    for (int i = 0; i < 16; ++i) v[0][i] = mont(v[0][i], v[1][i], f);
+  } else {
+    bf_group<4, 12, false, 1>(v, pt.fwd, t, f);
+#pragma unroll
+    for (int i = 0; i < 16; ++i) sX[bA + offA(i)] = v[0][i];
+    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < 16; ++i) v[0][i] = sX[bB + offB(i)];
+    bf_group<4, 8, false, 1>(v, pt.fwd, t & 15, f);
+#pragma unroll
+    for (int i = 0; i < 16; ++i) sX[bB + offB(i)] = v[0][i];
+    __syncthreads();
+    lds16(sX + bC, v[0]);
+    bf_group<4, 4, false, 1, true>(v, pt.fwd, 0, f);
+    if (ymode == 2) {
+      const uint4* ys = reinterpret_cast<const uint4*>(job.yspec + posC(t, 0));
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const uint4 u = __ldg(ys + q);
+        v[0][4 * q] = mont(v[0][4 * q], u.x, f);
+        v[0][4 * q + 1] = mont(v[0][4 * q + 1], u.y, f);
+        v[0][4 * q + 2] = mont(v[0][4 * q + 2], u.z, f);
+        v[0][4 * q + 3] = mont(v[0][4 * q + 3], u.w, f);
+      }
+    } else if (ymode == 3) {
+#pragma unroll
+      for (int i = 0; i < 16; ++i) v[0][i] = mont(v[0][i], v[0][i], f);
+    }
+  }
+  bf_group<4, 4, true, 1, true>(v, pt.inv, 0, f);
+  sts16(sX + bC, v[0]);
+  __syncthreads();
+#pragma unroll
+  for (int i = 0; i < 16; ++i) v[0][i] = sX[bB + offB(i)];
+  bf_group<4, 8, true, 1>(v, pt.inv, t & 15, f);
+#pragma unroll
+  for (int i = 0; i < 16; ++i) sX[bB + offB(i)] = v[0][i];
+  __syncthreads();
+#pragma unroll
+  for (int i = 0; i < 16; ++i) v[0][i] = sX[bA + offA(i)];
+  bf_group<4, 12, true, 1>(v, pt.inv, t, f);
+#pragma unroll
+  for (int i = 0; i < 16; ++i) epi_store(job.epi, posA(t, i), v[0][i], f);
+}
+
+__global__ void __launch_bounds__(256) k_cyc4096(SmallD job, Ptab pt) { cyc4096_body(job, pt); }
+// Batched: one CTA per job (descriptors as the batched one-CTA kernel's).
+__global__ void __launch_bounds__(256) k_cyc4096_b(const SmallJobB* __restrict__ jobs) {
+  const SmallJobB& j = jobs[blockIdx.x];
+  cyc4096_body(j.d, j.pt);
+}
+
+}  // namespace
+
+namespace fpx {
+
+cudaError_t launch_cyc4096(const PrimeTables& pt, const SmallJob& job, cudaStream_t s) {
+  SmallD d;
+  d.x = dev_in(job.x);
+  d.y = dev_in(job.y);
+  d.forward = 1;
+  d.ymode = job.ymode;
+  d.inverse = 1;
+  d.yspec = job.yspec;
+  d.yspec_out = job.yspec_out;
+  d.spec_x = nullptr;
+  d.epi = dev_epi(job.epi);
+  k_cyc4096<<<1, 256, 0, s>>>(d, dev_tab(pt));
+  return cudaGetLastError();
+}
+
+}  // namespace fpx
+
+// ===========================================================================
+// Cyclic products of N = 2^LOGN <= 2^13 points in one CTA with compile-time
+// structure: groups of at most four levels (sizes as the column passes'),
+// every group's twiddles loaded up front, both operands of a product in the
+// same register pass (twiddles shared), shared memory padded one word per 32.
+// Replaces the generic one-CTA kernel for products (the raw transform keeps
+// the generic one).
+// ===========================================================================
+namespace {
+
+template <int LOGN, int KG, bool INV, int NA>
+__device__ __forceinline__ void cyc_group(uint32_t* const (&S)[2], const uint2* __restrict__ tw, const Fp& f,
+                                          int tid, int nt) {
+  using Gs = ColGroups<LOGN>;
+  constexpr int G = Gs::size(KG);
+  constexpr int T = Gs::top(KG);
+  constexpr int SS = T - G;
+  constexpr int NINST = (1 << LOGN) >> G;
+#pragma unroll 1
+  for (int inst = tid; inst < NINST; inst += nt) {
+    const int base = inst & ((1 << SS) - 1);
+    const int p0 = ((inst >> SS) << T) + base;
+    uint32_t v[2][1 << G];
+#pragma unroll
+    for (int a = 0; a < NA; ++a)
+#pragma unroll
+      for (int i = 0; i < (1 << G); ++i) v[a][i] = S[a][pad(p0 + (i << SS))];
+    bf_group<G, T, INV, NA>(v, tw, base, f);
+#pragma unroll
+    for (int a = 0; a < NA; ++a)
+#pragma unroll
+      for (int i = 0; i < (1 << G); ++i) S[a][pad(p0 + (i << SS))] = v[a][i];
+  }
+}
+
+template <int LOGN, int KG, int NA>
+__device__ __forceinline__ void cyc_fwd(uint32_t* const (&S)[2], const uint2* tw, const Fp& f, int tid, int nt) {
+  if constexpr (KG < ColGroups<LOGN>::K) {
+    cyc_group<LOGN, KG, false, NA>(S, tw, f, tid, nt);
+    __syncthreads();
+    cyc_fwd<LOGN, KG + 1, NA>(S, tw, f, tid, nt);
+  }
+}
+
+template <int LOGN, int KG>
+__device__ __forceinline__ void cyc_inv(uint32_t* const (&S)[2], const uint2* tw, const Fp& f, int tid, int nt) {
+  if constexpr (KG >= 0) {
+    cyc_group<LOGN, KG, true, 1>(S, tw, f, tid, nt);
+    __syncthreads();
+    cyc_inv<LOGN, KG - 1>(S, tw, f, tid, nt);
+  }
+}
+
+template <int LOGN>
+__device__ __forceinline__ void cyc_small_body(const SmallD& job, const Ptab& pt) {
+  extern __shared__ uint32_t sm[];
+  constexpr int N = 1 << LOGN;
+  const int tid = threadIdx.x, nt = blockDim.x;
+  uint32_t* const S[2] = {sm, sm + padded_words(N)};
+  const Fp f = pt.f;
+  const int ymode = job.ymode;
+  for (int i = tid; i < N; i += nt) {
+    S[0][pad(i)] = load_in(job.x, i, f, pt.q1);
+    if (ymode == 1) S[1][pad(i)] = load_in(job.y, i, f, pt.q1);
+    else if (ymode == 2) S[1][pad(i)] = __ldg(job.yspec + i);
+  }
+  __syncthreads();
+  if (ymode == 1) {
+    cyc_fwd<LOGN, 0, 2>(S, pt.fwd, f, tid, nt);
+    if (job.yspec_out)
+      for (int i = tid; i < N; i += nt) job.yspec_out[i] = red(S[1][pad(i)], f.p);
+  } else {
+    cyc_fwd<LOGN, 0, 1>(S, pt.fwd, f, tid, nt);
+  }
+  if (ymode == 1 || ymode == 2) {
+    for (int i = tid; i < N; i += nt) S[0][pad(i)] = mont(S[0][pad(i)], S[1][pad(i)], f);
+  } else if (ymode == 3) {
+    for (int i = tid; i < N; i += nt) {
+      const uint32_t v = S[0][pad(i)];
+      S[0][pad(i)] = mont(v, v, f);
+    }
+  }
+  __syncthreads();
+  cyc_inv<LOGN, ColGroups<LOGN>::K - 1>(S, pt.inv, f, tid, nt);
+  const uint32_t hi = job.epi.hi < (uint32_t)N ? job.epi.hi : (uint32_t)N;
+  for (uint32_t i = job.epi.lo + tid; i < hi; i += nt) epi_store(job.epi, i, S[0][pad(i)], f);
+}
+
+template <int LOGN>
+__global__ void __launch_bounds__(512) k_cyc_small(SmallD job, Ptab pt) {
+  cyc_small_body<LOGN>(job, pt);
+}
+template <int LOGN>
+__global__ void __launch_bounds__(512) k_cyc_small_b(const SmallJobB* __restrict__ jobs) {
+  const SmallJobB& j = jobs[blockIdx.x];
+  cyc_small_body<LOGN>(j.d, j.pt);
+}
+
+using CycFn = void (*)(SmallD, Ptab);
+using CycBFn = void (*)(const SmallJobB*);
+
+template <int... L>
+struct CycTable {
+  static CycFn one(int logN) {
+    CycFn r = nullptr;
+    ((logN == L ? (r = k_cyc_small<L>, 0) : 0), ...);
+    return r;
+  }
+  static CycBFn batch(int logN) {
+    CycBFn r = nullptr;
+    ((logN == L ? (r = k_cyc_small_b<L>, 0) : 0), ...);
+    return r;
+  }
+  static cudaError_t init() {
+    cudaError_t e = cudaSuccess;
+    auto set = [&](const void* fn, int bytes) {
+      const cudaError_t r = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+      if (r != cudaSuccess) e = r;
+    };
+    (set((const void*)k_cyc_small<L>, 2 * padded_words(1 << L) * 4), ...);
+    (set((const void*)k_cyc_small_b<L>, 2 * padded_words(1 << L) * 4), ...);
+    return e;
+  }
+};
+using Cyc = CycTable<1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12, 13>;
+
+int cyc_threads(int logN) {
+  const int n = (1 << logN) / 16;
+  return n < 32 ? 32 : (n > 512 ? 512 : n);
+}
+
+}  // namespace
+
+namespace fpx {
+
+cudaError_t kernels_cyc_init() { return Cyc::init(); }
+
+cudaError_t launch_cyc_small(const PrimeTables& pt, int logN, const SmallJob& job, cudaStream_t s) {
+  CycFn fn = Cyc::one(logN);
+  if (!fn) return cudaErrorInvalidValue;
+  SmallD d;
+  d.x = dev_in(job.x);
+  d.y = dev_in(job.y);
+  d.forward = 1;
+  d.ymode = job.ymode;
+  d.inverse = 1;
+  d.yspec = job.yspec;
+  d.yspec_out = job.yspec_out;
+  d.spec_x = nullptr;
+  d.epi = dev_epi(job.epi);
+  fn<<<1, cyc_threads(logN), (size_t)2 * padded_words(1 << logN) * 4, s>>>(d, dev_tab(pt));
+  return cudaGetLastError();
+}
+
+}  // namespace fpx
+
+namespace {
+cudaError_t launch_cyc_small_batch(int logN, unsigned count, const SmallJobB* jobs, cudaStream_t s) {
+  CycBFn fn = Cyc::batch(logN);
+  if (!fn) return cudaErrorInvalidValue;
+  fn<<<count, cyc_threads(logN), (size_t)2 * padded_words(1 << logN) * 4, s>>>(jobs);
+  return cudaGetLastError();
+}
+}  // namespace

@@ -104,6 +104,13 @@ cudaError_t launch_direct_product(uint32_t p, const uint32_t* a, size_t la, cons
 int small_kernel_max_log();
 cudaError_t kernels_init();
 
+// One cyclic product of exactly 4096 points (as launch_small with forward =
+// inverse = 1; epi.scale holds the full inverse scale) in the row pass's layout.
+cudaError_t launch_cyc4096(const PrimeTables& pt, const SmallJob& job, cudaStream_t s);
+// One cyclic product of 2^logN <= 2^13 points in one CTA (same contract).
+cudaError_t launch_cyc_small(const PrimeTables& pt, int logN, const SmallJob& job, cudaStream_t s);
+cudaError_t kernels_cyc_init();
+
 }  // namespace fpx
 
 namespace fpx {

@@ -393,6 +393,111 @@ vec<M> integral(const vec<M>& a) {
 
 }  // namespace poly
 
+// ----------------------------------------------------------------- batches
+
+namespace gpu {
+
+/// Many fpx::poly operations in one call (fpx_batch_run).  No counterpart in
+/// the reference, whose callers loop over the single functions: queue the
+/// operations, run() once, then get() each result, which is exactly the single
+/// function's result, or throws exactly its exception.  The input vectors must
+/// stay alive and unchanged until run() returns.
+template <class M>
+class Batch {
+ public:
+  using vec = poly::vec<M>;
+  size_t conv(const vec& a, const vec& b, size_t n = SIZE_MAX) { return add(FPX_OP_CONV, a, &b, n, 0); }
+  size_t inv(const vec& a, size_t n) { return add(FPX_OP_INV, a, nullptr, n, 0); }
+  size_t log(const vec& a, size_t n) { return add(FPX_OP_LOG, a, nullptr, n, 0); }
+  size_t exp(const vec& a, size_t n) { return add(FPX_OP_EXP, a, nullptr, n, 0); }
+  size_t sqrt(const vec& a, size_t n) { return add(FPX_OP_SQRT, a, nullptr, n, 0); }
+  size_t pow(const vec& a, uint64_t k, size_t n) { return add(FPX_OP_POW, a, nullptr, n, k); }
+  size_t divmod(const vec& a, const vec& b) { return add(FPX_OP_DIVMOD, a, &b, 0, 0); }
+  size_t size() const { return items_.size(); }
+
+  /// Runs every queued operation; per-operation errors are kept for get().
+  void run() {
+    std::vector<fpx_job> jobs(items_.size());
+    for (size_t i = 0; i < items_.size(); ++i) {
+      Item& it = items_[i];
+      fpx_job& j = jobs[i];
+      j = fpx_job{};
+      j.op = it.op;
+      j.p = M::mod;
+      j.a = limbs(*it.a);
+      j.la = it.a->size();
+      if (it.b) {
+        j.b = limbs(*it.b);
+        j.lb = it.b->size();
+      }
+      j.k = it.k;
+      j.n = it.n;
+      size_t cap = it.n;
+      if (it.op == FPX_OP_CONV) {
+        const size_t la = std::min(j.la, it.n), lb = std::min(j.lb, it.n);
+        cap = la && lb ? (la > SIZE_MAX - lb ? it.n : std::min(la + lb - 1, it.n)) : 0;
+      } else if (it.op == FPX_OP_DIVMOD) {
+        cap = j.la;
+        it.out2.resize(j.lb);
+        j.out2 = limbs(it.out2);
+      }
+      it.out.resize(cap);
+      j.out = limbs(it.out);
+    }
+    const int rc = fpx_batch_run(context(), jobs.data(), jobs.size(), FPX_REPR_MONTGOMERY);
+    if (rc != FPX_OK && rc != FPX_EDOMAIN && rc != FPX_ESIZE && rc != FPX_ELENGTH && rc != FPX_EINVAL)
+      check(rc, "gpu::Batch::run");
+    for (size_t i = 0; i < items_.size(); ++i) {
+      Item& it = items_[i];
+      it.status = jobs[i].status;
+      it.out.resize(it.status == FPX_OK ? jobs[i].out_len : 0);
+      if (it.op == FPX_OP_DIVMOD) it.out2.resize(it.status == FPX_OK ? jobs[i].out2_len : 0);
+    }
+    ran_ = true;
+  }
+
+  /// Result of operation h (the quotient for divmod).
+  const vec& get(size_t h) const {
+    status_of(h);
+    return items_[h].out;
+  }
+  /// Remainder of divmod operation h.
+  const vec& remainder(size_t h) const {
+    status_of(h);
+    return items_[h].out2;
+  }
+
+ private:
+  struct Item {
+    int op;
+    const vec* a;
+    const vec* b;
+    size_t n;
+    uint64_t k;
+    vec out, out2;
+    int status = FPX_OK;
+  };
+  size_t add(int op, const vec& a, const vec* b, size_t n, uint64_t k) {
+    items_.push_back(Item{op, &a, b, n, k, {}, {}, FPX_OK});
+    ran_ = false;
+    return items_.size() - 1;
+  }
+  void status_of(size_t h) const {
+    if (!ran_) throw std::logic_error("gpu::Batch: run() has not been called");
+    const int rc = items_.at(h).status;
+    if (rc == FPX_OK) return;
+    if (rc == FPX_EDOMAIN) throw poly::domain_error("gpu::Batch: operation " + std::to_string(h));
+    if (rc == FPX_ESIZE) throw ntt_size_error("gpu::Batch: operation " + std::to_string(h));
+    if (rc == FPX_ELENGTH) throw std::length_error("gpu::Batch: operation " + std::to_string(h));
+    throw std::runtime_error("gpu::Batch: operation " + std::to_string(h) + " failed with status " +
+                             std::to_string(rc));
+  }
+  std::vector<Item> items_;
+  bool ran_ = false;
+};
+
+}  // namespace gpu
+
 // ------------------------------------------------------------------ Poly
 
 template <class M>

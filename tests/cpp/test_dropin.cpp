@@ -79,6 +79,32 @@ void suite(const char* name) {
   bool threw = false;
   try { (void)poly::inv(std::vector<M>{M(), M::from_int(1)}, 8); } catch (const poly::domain_error&) { threw = true; }
   CHECK(threw);
+  // one batch of the same operations: every result equals the single call's
+  {
+    gpu::Batch<M> batch;
+    auto x = rnd<M>(900, g), y = rnd<M>(1300, g), e0 = rnd<M>(700, g), l1 = rnd<M>(600, g);
+    x[0] = M::from_int(3);
+    e0[0] = M();
+    l1[0] = M::from_int(1);
+    const auto bad = std::vector<M>{M(), M::from_int(1)};
+    const size_t hc = batch.conv(x, y), ht = batch.conv(x, y, 500), hi = batch.inv(x, 1000);
+    const size_t he = batch.exp(e0, 800), hl = batch.log(l1, 600), hq = batch.divmod(y, x);
+    const size_t hp = batch.pow(x, 5, 700), hs = batch.sqrt(naive(x, x, 900), 900), hb = batch.inv(bad, 8);
+    batch.run();
+    CHECK(batch.get(hc) == poly::conv(x, y));
+    CHECK(batch.get(ht) == poly::conv(x, y, 500));
+    CHECK(batch.get(hi) == poly::inv(x, 1000));
+    CHECK(batch.get(he) == poly::exp(e0, 800));
+    CHECK(batch.get(hl) == poly::log(l1, 600));
+    const auto [bq, br] = poly::divmod(y, x);
+    CHECK(batch.get(hq) == bq);
+    CHECK(batch.remainder(hq) == br);
+    CHECK(batch.get(hp) == poly::pow(x, 5, 700));
+    CHECK(batch.get(hs) == poly::sqrt(naive(x, x, 900), 900));
+    bool batch_threw = false;
+    try { (void)batch.get(hb); } catch (const poly::domain_error&) { batch_threw = true; }
+    CHECK(batch_threw);
+  }
   std::printf("  %s ok\n", name);
 }
 
