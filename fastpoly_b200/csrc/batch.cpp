@@ -19,8 +19,8 @@ namespace fpx {
 namespace {
 constexpr size_t kNaiveB = 40;                                        // base.hpp:89
 const uint32_t kCrtPrimesB[3] = {167772161u, 469762049u, 754974721u};  // crt_convolution.hpp:14-18
-// Batched transforms use rows of 2^12 points: at most 2^23 points.
-constexpr int kBatchMaxLog = 23;
+// Batched transforms use rows of 2^12 points: at most 2^24 points.
+constexpr int kBatchMaxLog = 24;
 
 Tw2 shoup_pair_b(uint32_t w, uint32_t p) { return Tw2{w, (uint32_t)(((uint64_t)w << 32) / p)}; }
 size_t round64(size_t w) { return (w + 63) & ~size_t(63); }
@@ -44,7 +44,7 @@ class BatchRec {
   // One cyclic product of size 2^logN on a native prime (Engine::cyc_product semantics).
   void cyc(uint32_t p, int logN, const Engine::CycOp& op) {
     XJob j;
-    j.pt = &e_.prime_plan(p).t;
+    j.pt = &plan(p);
     j.logN = logN;
     j.x = op.x;
     j.y = op.y;
@@ -55,13 +55,12 @@ class BatchRec {
     const uint32_t N = 1u << logN;
     if (logN <= small_kernel_max_log()) {
       // 1/N, times 2^32 after a Montgomery pointwise product, times the caller's factor
-      uint64_t s = invm(N % p, p);
-      if (op.ymode != 0) s = s * ((((uint64_t)1) << 32) % p) % p;
+      uint64_t s = op.ymode != 0 ? j.pt->inv_pow2_r[logN] : j.pt->inv_pow2[logN];
       if (j.epi.scale.w) s = s * j.epi.scale.w % p;
       j.epi.scale = shoup_pair_b((uint32_t)s, p);
       need_.push_back(0);
     } else {
-      j.bt = &e_.big_plan(p, logN).t;
+      j.bt = &big(p, logN);
       if (j.epi.scale.w) j.epi.scale = shoup_pair_b(j.epi.scale.w % p, p);
       need_.push_back(op.ymode == 1 ? 2 * (size_t)N : N);
     }
@@ -184,6 +183,27 @@ class BatchRec {
   }
 
  private:
+  // plan lookups cached per recorder (a flush records thousands of products
+  // over a handful of primes and sizes)
+  const PrimeTables& plan(uint32_t p) {
+    if (p != last_p_) {
+      last_pt_ = &e_.prime_plan(p).t;
+      last_p_ = p;
+    }
+    return *last_pt_;
+  }
+  const BigTables& big(uint32_t p, int logN) {
+    const uint64_t key = ((uint64_t)p << 8) | (uint32_t)logN;
+    if (key != last_big_) {
+      last_bt_ = &e_.big_plan(p, logN).t;
+      last_big_ = key;
+    }
+    return *last_bt_;
+  }
+  uint32_t last_p_ = 0;
+  const PrimeTables* last_pt_ = nullptr;
+  uint64_t last_big_ = 0;
+  const BigTables* last_bt_ = nullptr;
   struct CBuf {
     int garner, k;
     size_t words;
@@ -341,7 +361,7 @@ void Engine::batch(fpx_job* jobs, size_t count) {
         if (j.n == 0) break;
         if (!j.out) { j.status = FPX_EINVAL; break; }
         j.out_len = j.n;
-        // log's final product has 2n - 3 terms: at most 2^23 points for n <= 2^22
+        // log's final product has 2n - 3 terms: at most 2^24 points for n <= 2^23
         const size_t lim = j.op == FPX_OP_LOG ? max_series / 2 : max_series;
         if (j.p == 2 || j.n > lim) {
           route[i] = kSingle;

@@ -362,6 +362,11 @@ const PrimePlan& Engine::prime_plan(uint32_t p) {
   plan->t.fwd = reinterpret_cast<const Tw2*>(upload(*this, plan->fwd, fwd));
   plan->t.inv = reinterpret_cast<const Tw2*>(upload(*this, plan->inv, inv));
   plan->t.q1 = (uint32_t)((((uint64_t)1) << 32) / p);
+  const uint64_t r32 = (((uint64_t)1) << 32) % p;
+  for (int k = 0; k <= 13; ++k) {
+    plan->t.inv_pow2[k] = invm((uint32_t)((((uint64_t)1) << k) % p), p);
+    plan->t.inv_pow2_r[k] = (uint32_t)(plan->t.inv_pow2[k] * r32 % p);
+  }
   auto& ref = *plan;
   primes_[p] = std::move(plan);
   return ref;
@@ -400,7 +405,7 @@ const BigPlan& Engine::big_plan(uint32_t p, int logN) {
     ci = ci * stepi % p;
   }
   plan->t.logN = logN;
-  plan->t.logC = logN >= 24 ? 13 : 12;
+  plan->t.logC = logN >= 25 ? 13 : 12;  // 2^24 = 2^12 x 2^12 keeps the fast 4096-point row pass
   plan->t.logR = logN - plan->t.logC;
   plan->t.lo_fwd = reinterpret_cast<const Tw2*>(upload(*this, plan->lo_fwd, lo_f));
   plan->t.hi_fwd = reinterpret_cast<const Tw2*>(upload(*this, plan->hi_fwd, hi_f));
@@ -445,8 +450,7 @@ void Engine::cyc_product(uint32_t p, int logN, const CycOp& op) {
     j.yspec_out = op.yspec_out;
     j.inverse = 1;
     // 1/N, times 2^32 after a Montgomery pointwise product, times the caller's factor.
-    uint64_t s = invm(N % p, p);
-    if (op.ymode != 0) s = s * ((((uint64_t)1) << 32) % p) % p;
+    uint64_t s = op.ymode != 0 ? pt.inv_pow2_r[logN] : pt.inv_pow2[logN];
     if (epi.scale.w) s = s * epi.scale.w % p;
     epi.scale = shoup_pair((uint32_t)s, p);
     j.epi = epi;

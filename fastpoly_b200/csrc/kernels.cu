@@ -286,8 +286,12 @@ __device__ __forceinline__ uint32_t redc_any(uint32_t x, uint32_t m) { return mi
 __device__ __forceinline__ void garner_body(const GarnerC& g, int primes, const uint32_t* c1, const uint32_t* c2,
                                             const uint32_t* c3, uint32_t* out, size_t n, int accumulate,
                                             const uint32_t* post_mont = nullptr, int negate = 0,
-                                            uint32_t tpinv = 0) {
-  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+                                            uint32_t tpinv = 0, size_t first = 0, size_t span = ~size_t(0)) {
+  // outputs [first, min(n, first + span)), grid-stride over the whole range when span is unbounded
+  const bool whole = span == ~size_t(0);
+  const size_t end = whole ? n : (first + span < n ? first + span : n);
+  const size_t step = whole ? (size_t)gridDim.x * blockDim.x : blockDim.x;
+  for (size_t i = (whole ? blockIdx.x * (size_t)blockDim.x : first) + threadIdx.x; i < end; i += step) {
     const uint32_t x1 = c1[i];
     uint32_t v = x1 - __umulhi(x1, g.t_q1) * g.t;
     v = redc_any(v, g.t);
@@ -363,14 +367,19 @@ __global__ void k_derivative(Fp f, uint32_t q1, uint2 r_sh, const uint32_t* a, u
 // out[i] = sum_j a[j] * b[i + off - j].
 __device__ __forceinline__ void direct_body(uint32_t p, const Fp& f, const uint32_t* a, int la, const uint32_t* b,
                                             size_t lb, size_t off, size_t cnt, uint32_t* out, int accumulate,
-                                            const uint32_t* post_mont = nullptr, int negate = 0) {
+                                            const uint32_t* post_mont = nullptr, int negate = 0,
+                                            size_t first = 0, size_t span = ~size_t(0)) {
   __shared__ uint32_t am[64];
   if (threadIdx.x < la) {
     const uint32_t v = a[threadIdx.x];
     am[threadIdx.x] = (p == 2) ? v : (uint32_t)(((uint64_t)v << 32) % p);  // Montgomery form of a[j]
   }
   __syncthreads();
-  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < cnt; i += (size_t)gridDim.x * blockDim.x) {
+  // outputs [first, min(cnt, first + span)), grid-stride over the whole range when span is unbounded
+  const bool whole = span == ~size_t(0);
+  const size_t end = whole ? cnt : (first + span < cnt ? first + span : cnt);
+  const size_t step = whole ? (size_t)gridDim.x * blockDim.x : blockDim.x;
+  for (size_t i = (whole ? blockIdx.x * (size_t)blockDim.x : first) + threadIdx.x; i < end; i += step) {
     const size_t k = i + off;
     uint64_t acc = 0;
     uint32_t bits = 0;
@@ -1305,9 +1314,19 @@ __global__ void __launch_bounds__(256, 3) k_colinv_b(const BigJobB* __restrict__
   colinv_body<LOGR, PLAIN>(j.t[0], j.bi, j.pt, j.epi);
 }
 
-__global__ void k_direct_b(const DirectJobB* __restrict__ jobs) {
-  const DirectJobB& j = jobs[blockIdx.y];
-  direct_body(j.p, j.f, j.a, j.la, j.b, j.lb, j.off, j.cnt, j.out, j.accumulate, j.post_mont, j.negate);
+// Batched direct products and Garner reconstructions: block b covers outputs
+// [map[b].first, map[b].first + kOutSpan) of job map[b].job, so blocks follow
+// each job's own length rather than the longest job's.
+constexpr size_t kOutSpan = 2048;
+struct OutBlock {
+  uint32_t job;
+  uint32_t first;
+};
+__global__ void k_direct_b(const DirectJobB* __restrict__ jobs, const OutBlock* __restrict__ map) {
+  const OutBlock m = map[blockIdx.x];
+  const DirectJobB& j = jobs[m.job];
+  direct_body(j.p, j.f, j.a, j.la, j.b, j.lb, j.off, j.cnt, j.out, j.accumulate, j.post_mont, j.negate, m.first,
+              kOutSpan);
 }
 
 // Newton seeds for many jobs (k_seed per block): blockIdx.x = job.
@@ -1325,9 +1344,11 @@ __global__ void k_seed_b(const SeedJobB* __restrict__ jobs) {
   seed_body(j.kind, j.p, j.a, j.la, j.out, j.n, j.r0);
 }
 
-__global__ void k_garner_b(const GarnerJobB* __restrict__ jobs) {
-  const GarnerJobB& j = jobs[blockIdx.y];
-  garner_body(j.g, j.primes, j.c1, j.c2, j.c3, j.out, j.n, j.accumulate, j.post_mont, j.negate, j.tpinv);
+__global__ void k_garner_b(const GarnerJobB* __restrict__ jobs, const OutBlock* __restrict__ map) {
+  const OutBlock m = map[blockIdx.x];
+  const GarnerJobB& j = jobs[m.job];
+  garner_body(j.g, j.primes, j.c1, j.c2, j.c3, j.out, j.n, j.accumulate, j.post_mont, j.negate, j.tpinv, m.first,
+              kOutSpan);
 }
 
 using BatchFn = void (*)(const BigJobB*);
@@ -1410,9 +1431,14 @@ namespace fpx {
 
 cudaError_t kernels_batch_init() { return ColsB::init(); }
 
+static size_t out_blocks(size_t n) { return n ? (n + kOutSpan - 1) / kOutSpan : 0; }
+
 size_t batch_descriptor_bytes(const BatchPlan& b) {
+  size_t blocks = 0;
+  for (const DirectJob& x : b.direct) blocks += out_blocks(x.cnt);
+  for (const GarnerJob& x : b.garner) blocks += out_blocks(x.n);
   return b.xjobs.size() * std::max(sizeof(SmallJobB), sizeof(BigJobB)) + b.direct.size() * sizeof(DirectJobB) +
-         b.garner.size() * sizeof(GarnerJobB) + 256 * 40;  // every section starts 256-byte aligned
+         b.garner.size() * sizeof(GarnerJobB) + blocks * sizeof(OutBlock) + 256 * 40;  // sections 256-byte aligned
 }
 
 cudaError_t launch_batch(const BatchPlan& b, void* host_staging, void* dev_desc, cudaStream_t s,
@@ -1526,21 +1552,37 @@ cudaError_t launch_batch(const BatchPlan& b, void* host_staging, void* dev_desc,
     std::memcpy(h + off, &j, sizeof j);
     off += sizeof j;
   }
+  // block maps of the direct and Garner launches
+  off = align256(off);
+  const size_t off_dmap = off;
+  for (size_t q = 0; q < b.direct.size(); ++q)
+    for (size_t f0 = 0; f0 < b.direct[q].cnt; f0 += kOutSpan) {
+      const OutBlock m{(uint32_t)q, (uint32_t)f0};
+      std::memcpy(h + off, &m, sizeof m);
+      off += sizeof m;
+    }
+  const size_t n_dmap = (off - off_dmap) / sizeof(OutBlock);
+  off = align256(off);
+  const size_t off_gmap = off;
+  for (size_t q = 0; q < b.garner.size(); ++q)
+    for (size_t f0 = 0; f0 < b.garner[q].n; f0 += kOutSpan) {
+      const OutBlock m{(uint32_t)q, (uint32_t)f0};
+      std::memcpy(h + off, &m, sizeof m);
+      off += sizeof m;
+    }
+  const size_t n_gmap = (off - off_gmap) / sizeof(OutBlock);
   if (off == 0) return cudaSuccess;
   cudaError_t e = cudaMemcpyAsync(d, h, off, cudaMemcpyHostToDevice, s);
   if (e != cudaSuccess) return e;
   if (staged && (e = cudaEventRecord(staged, s)) != cudaSuccess) return e;
   // grid.y / grid.z hold at most 65535 jobs per launch
   constexpr size_t kMaxY = 65535;
-  if (!b.direct.empty()) {
-    size_t maxcnt = 0;
-    for (const DirectJob& x : b.direct) maxcnt = std::max(maxcnt, x.cnt);
-    for (size_t k = 0; k < b.direct.size(); k += kMaxY) {
-      dim3 grid((unsigned)std::min<size_t>((maxcnt + 255) / 256, 1024),
-                (unsigned)std::min(kMaxY, b.direct.size() - k));
-      k_direct_b<<<grid, 256, 0, s>>>(reinterpret_cast<const DirectJobB*>(d + off_direct) + k);
-      if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    }
+  // block maps are at most 2^31 blocks; grid.x takes them in chunks
+  constexpr size_t kMaxX = size_t(1) << 30;
+  for (size_t k = 0; k < n_dmap; k += kMaxX) {
+    k_direct_b<<<(unsigned)std::min(kMaxX, n_dmap - k), 256, 0, s>>>(
+        reinterpret_cast<const DirectJobB*>(d + off_direct), reinterpret_cast<const OutBlock*>(d + off_dmap) + k);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
   }
   for (const BatchGroup& g : groups) {
     if (!g.big && g.logN == 12) {
@@ -1567,14 +1609,10 @@ cudaError_t launch_batch(const BatchPlan& b, void* host_staging, void* dev_desc,
       if (e != cudaSuccess) return e;
     }
   }
-  if (!b.garner.empty()) {
-    size_t maxn = 0;
-    for (const GarnerJob& x : b.garner) maxn = std::max(maxn, x.n);
-    for (size_t k = 0; k < b.garner.size(); k += kMaxY) {
-      dim3 grid((unsigned)std::min<size_t>((maxn + 255) / 256, 1024), (unsigned)std::min(kMaxY, b.garner.size() - k));
-      k_garner_b<<<grid, 256, 0, s>>>(reinterpret_cast<const GarnerJobB*>(d + off_garner) + k);
-      if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    }
+  for (size_t k = 0; k < n_gmap; k += kMaxX) {
+    k_garner_b<<<(unsigned)std::min(kMaxX, n_gmap - k), 256, 0, s>>>(
+        reinterpret_cast<const GarnerJobB*>(d + off_garner), reinterpret_cast<const OutBlock*>(d + off_gmap) + k);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
   }
   return cudaSuccess;
 }

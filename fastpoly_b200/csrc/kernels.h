@@ -16,6 +16,10 @@ struct PrimeTables {
   const Tw2* fwd = nullptr;   // device
   const Tw2* inv = nullptr;   // device
   uint32_t q1 = 0;            // floor(2^32 / p)
+  // host-side constants: inverse scale of a one-CTA product of 2^k points,
+  // 1/2^k and (after a Montgomery pointwise product) 2^32/2^k mod p, k <= 13
+  uint32_t inv_pow2[14] = {};
+  uint32_t inv_pow2_r[14] = {};
 };
 
 // Per-(prime, N) tables for the two-pass (four-step) decomposition.

@@ -130,7 +130,7 @@ int fpx_mod(fpx_ctx* ctx, uint32_t p, const uint32_t* a, size_t la, const uint32
  * functions, job by job.  The batch shares launches between jobs: all products
  * of a stage run as one launch set per transform size (mixed primes and CRT
  * lifts included), and the Newton loops of inv, log and exp advance in
- * lockstep.  sqrt, pow and divmod jobs, and transforms past 2^23 points, run
+ * lockstep.  sqrt, pow and divmod jobs, and transforms past 2^24 points, run
  * one after another inside the same call. */
 enum fpx_op {
   FPX_OP_CONV = 0,   /* out = conv(a, b, n)                     (convolution.hpp:145) */
