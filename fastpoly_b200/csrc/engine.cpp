@@ -381,36 +381,40 @@ const BigPlan& Engine::big_plan(uint32_t p, int logN) {
   auto plan = std::make_unique<BigPlan>();
   const uint32_t gen = primitive_root(p);
   const uint64_t N = uint64_t(1) << logN;
-  const uint32_t wN = powm(gen, (p - 1) / N, p), wNi = invm(wN, p);
+  const uint32_t wN = powm(gen, (p - 1) / N, p);
   const uint32_t invN = invm((uint32_t)(N % p), p);
   const uint32_t R = (uint32_t)((((uint64_t)1) << 32) % p);
-  const size_t nhi = std::max<size_t>(1, N >> 12);
-  std::vector<Tw2> lo_f(4096), lo_i(4096), lo_ir(4096), hi_f(nhi), hi_i(nhi);
-  uint64_t c = 1, ci = 1;
-  for (size_t y = 0; y < 4096; ++y) {
-    lo_f[y] = shoup_pair((uint32_t)c, p);
-    const uint32_t v = (uint32_t)(ci * invN % p);
+  // w_N^e = lo[e & 255] * mid[(e >> 8) & 255] * hi[e >> 16]; 1/N (and 2^32/N)
+  // ride on the inverse lo table
+  const size_t nhi = std::max<size_t>(1, N >> 16);
+  std::vector<Tw2> lo_f(256), lo_i(256), lo_ir(256), mid_f(256), mid_i(256), hi_f(nhi), hi_i(nhi);
+  auto fill = [&](std::vector<Tw2>& f, std::vector<Tw2>& fi, uint32_t step, size_t cnt) {
+    const uint32_t stepi = invm(step, p);
+    uint64_t c = 1, ci = 1;
+    for (size_t y = 0; y < cnt; ++y) {
+      f[y] = shoup_pair((uint32_t)c, p);
+      fi[y] = shoup_pair((uint32_t)ci, p);
+      c = c * step % p;
+      ci = ci * stepi % p;
+    }
+  };
+  fill(lo_f, lo_i, wN, 256);
+  fill(mid_f, mid_i, powm(wN, 256, p), 256);
+  fill(hi_f, hi_i, powm(wN, 65536, p), nhi);
+  for (size_t y = 0; y < 256; ++y) {
+    const uint32_t v = (uint32_t)((uint64_t)lo_i[y].w * invN % p);
     lo_i[y] = shoup_pair(v, p);
     lo_ir[y] = shoup_pair((uint32_t)((uint64_t)v * R % p), p);
-    c = c * wN % p;
-    ci = ci * wNi % p;
-  }
-  const uint32_t step = powm(wN, 4096, p), stepi = invm(step, p);
-  c = 1;
-  ci = 1;
-  for (size_t x = 0; x < nhi; ++x) {
-    hi_f[x] = shoup_pair((uint32_t)c, p);
-    hi_i[x] = shoup_pair((uint32_t)ci, p);
-    c = c * step % p;
-    ci = ci * stepi % p;
   }
   plan->t.logN = logN;
   plan->t.logC = logN >= 25 ? 13 : 12;  // 2^24 = 2^12 x 2^12 keeps the fast 4096-point row pass
   plan->t.logR = logN - plan->t.logC;
   plan->t.lo_fwd = reinterpret_cast<const Tw2*>(upload(*this, plan->lo_fwd, lo_f));
+  plan->t.mid_fwd = reinterpret_cast<const Tw2*>(upload(*this, plan->mid_fwd, mid_f));
   plan->t.hi_fwd = reinterpret_cast<const Tw2*>(upload(*this, plan->hi_fwd, hi_f));
   plan->t.lo_inv = reinterpret_cast<const Tw2*>(upload(*this, plan->lo_inv, lo_i));
   plan->t.lo_inv_r = reinterpret_cast<const Tw2*>(upload(*this, plan->lo_inv_r, lo_ir));
+  plan->t.mid_inv = reinterpret_cast<const Tw2*>(upload(*this, plan->mid_inv, mid_i));
   plan->t.hi_inv = reinterpret_cast<const Tw2*>(upload(*this, plan->hi_inv, hi_i));
   auto& ref = *plan;
   bigs_[key] = std::move(plan);

@@ -80,7 +80,7 @@ struct PrimePlan {
 };
 struct BigPlan {
   BigTables t;
-  Buf lo_fwd, hi_fwd, lo_inv, lo_inv_r, hi_inv;
+  Buf lo_fwd, mid_fwd, hi_fwd, lo_inv, lo_inv_r, mid_inv, hi_inv;
 };
 
 // Host-side number theory.

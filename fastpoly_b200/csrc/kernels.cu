@@ -100,7 +100,6 @@ bool host_epi_plain(const fpx::Epi& e) {
   return e.scale.w == 0 && !e.mul_mont && !e.negate && !e.sub_from && !e.accumulate;
 }
 
-__device__ __forceinline__ int brev_n(int t, int logn) { return logn ? (int)(__brev((unsigned)t) >> (32 - logn)) : 0; }
 
 // ---------------------------------------------------------------------------
 // Single-CTA transforms (N <= 2^13).
@@ -163,34 +162,17 @@ struct ColOps {
 };
 struct BigD {
   int logR, logC, logW;
-  const uint2* lo;
-  const uint2* hi;
+  const uint2* lo;   // w_N^y, y < 256
+  const uint2* mid;  // w_N^(256 y), y < 256
+  const uint2* hi;   // w_N^(65536 y), y < max(1, N / 65536)
 };
 
-__global__ void __launch_bounds__(256) k_colfwd(ColOps ops, BigD bt, Ptab pt) {
-  extern __shared__ uint32_t sm[];
-  const int tid = threadIdx.x, nt = blockDim.x;
-  const int logW = bt.logW, W = 1 << logW, logC = bt.logC;
-  const int TE = W << bt.logR;
-  const int j0 = blockIdx.x << logW;
-  const InD in = ops.in[blockIdx.y];
-  uint32_t* out = ops.out[blockIdx.y];
-  const Fp f = pt.f;
-  for (int e = tid; e < TE; e += nt) {
-    const int t = e >> logW, c = e & (W - 1);
-    sm[pad(e)] = load_in(in, (uint32_t)((t << logC) + j0 + c), f, pt.q1);
-  }
-  __syncthreads();
-  tile_dif(sm, bt.logR, logW, pt.fwd, f, tid, nt);
-  __syncthreads();
-  for (int e = tid; e < TE; e += nt) {
-    const int t = e >> logW, c = e & (W - 1);
-    const int j = j0 + c;
-    const uint32_t ex = (uint32_t)j * (uint32_t)brev_n(t, bt.logR);
-    uint32_t v = shoup(sm[pad(e)], __ldg(bt.lo + (ex & 4095u)), f.p);
-    v = shoup(v, __ldg(bt.hi + (ex >> 12)), f.p);
-    out[(t << logC) + j] = v;
-  }
+// Bailey twiddle w_N^ex from the three small tables (5 KiB for N = 2^23, L1
+// resident next to the per-prime table): three Shoup products.
+__device__ __forceinline__ uint32_t bailey_mul(uint32_t x, uint32_t ex, const BigD& bt, const Fp& f) {
+  x = shoup(x, __ldg(bt.lo + (ex & 255u)), f.p);
+  x = shoup(x, __ldg(bt.mid + ((ex >> 8) & 255u)), f.p);
+  return shoup(x, __ldg(bt.hi + (ex >> 16)), f.p);
 }
 
 // ---------------------------------------------------------------------------
@@ -236,31 +218,6 @@ __global__ void __launch_bounds__(512) k_rows(uint32_t* x, const uint32_t* y, in
   }
 }
 
-// ---------------------------------------------------------------------------
-// Pass A inverse (columns) with the output epilogue.
-// ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) k_colinv(const uint32_t* in, BigD bt, Ptab pt, EpiD epi) {
-  extern __shared__ uint32_t sm[];
-  const int tid = threadIdx.x, nt = blockDim.x;
-  const int logW = bt.logW, W = 1 << logW, logC = bt.logC;
-  const int TE = W << bt.logR;
-  const int j0 = blockIdx.x << logW;
-  const Fp f = pt.f;
-  for (int e = tid; e < TE; e += nt) {
-    const int t = e >> logW, c = e & (W - 1);
-    const int j = j0 + c;
-    const uint32_t ex = (uint32_t)j * (uint32_t)brev_n(t, bt.logR);
-    uint32_t v = shoup(__ldg(in + (t << logC) + j), __ldg(bt.lo + (ex & 4095u)), f.p);
-    sm[pad(e)] = shoup(v, __ldg(bt.hi + (ex >> 12)), f.p);
-  }
-  __syncthreads();
-  tile_dit(sm, bt.logR, logW, pt.inv, f, tid, nt);
-  __syncthreads();
-  for (int e = tid; e < TE; e += nt) {
-    const int t = e >> logW, c = e & (W - 1);
-    epi_store(epi, (uint32_t)((t << logC) + j0 + c), sm[pad(e)], f);
-  }
-}
 
 // ---------------------------------------------------------------------------
 // Elementwise kernels.
@@ -433,9 +390,7 @@ cudaError_t kernels_init() {
     if (r != cudaSuccess) e = r;
   };
   set((const void*)k_small, 2 * padded_words(1 << kSmallLog) * 4);
-  set((const void*)k_colfwd, padded_words(1 << 14) * 4);
   set((const void*)k_rows, 2 * padded_words(1 << 13) * 4);
-  set((const void*)k_colinv, padded_words(1 << 14) * 4);
   const cudaError_t r = kernels_fast_init();
   const cudaError_t r2 = kernels_batch_init();
   const cudaError_t r3 = kernels_cyc_init();
@@ -462,38 +417,6 @@ cudaError_t launch_small(const PrimeTables& pt, int logN, const SmallJob& job, c
   return cudaGetLastError();
 }
 
-// Column tile: W = 2^logW adjacent columns x R rows, at most 2^14 words (64 KiB
-// of shared memory, three CTAs per SM); 2^13 words for short columns so that
-// mid-size transforms still spread over several CTAs.
-static BigD big_dev(const BigTables& bt, const Tw2* lo, const Tw2* hi) {
-  int logW = bt.logR >= 11 ? 14 - bt.logR : 13 - bt.logR;
-  if (logW < 2) logW = 2;
-  if (logW > bt.logC) logW = bt.logC;
-  BigD d;
-  d.logR = bt.logR;
-  d.logC = bt.logC;
-  d.logW = logW;
-  d.lo = reinterpret_cast<const uint2*>(lo);
-  d.hi = reinterpret_cast<const uint2*>(hi);
-  return d;
-}
-
-static int col_tile_words(const BigD& d) { return (1 << d.logW) << d.logR; }
-
-cudaError_t launch_colfwd_generic(const PrimeTables& pt, const BigTables& bt, int nops, const InOp* in,
-                                  uint32_t* const* out, cudaStream_t s) {
-  ColOps ops{};
-  for (int i = 0; i < nops; ++i) {
-    ops.in[i] = dev_in(in[i]);
-    ops.out[i] = out[i];
-  }
-  const BigD d = big_dev(bt, bt.lo_fwd, bt.hi_fwd);
-  const size_t smem = (size_t)padded_words(col_tile_words(d)) * 4;
-  dim3 grid(1u << (d.logC - d.logW), (unsigned)nops);
-  k_colfwd<<<grid, 256, smem, s>>>(ops, d, dev_tab(pt));
-  return cudaGetLastError();
-}
-
 cudaError_t launch_rows_generic(const PrimeTables& pt, const BigTables& bt, uint32_t* x, const uint32_t* y, int ymode,
                                 uint32_t* y_spec_out, int forward, int inverse, cudaStream_t s) {
   const int C = 1 << bt.logC;
@@ -503,13 +426,6 @@ cudaError_t launch_rows_generic(const PrimeTables& pt, const BigTables& bt, uint
   return cudaGetLastError();
 }
 
-cudaError_t launch_colinv_generic(const PrimeTables& pt, const BigTables& bt, const uint32_t* in, int mont_scaled,
-                                  const Epi& epi, cudaStream_t s) {
-  const BigD d = big_dev(bt, mont_scaled ? bt.lo_inv_r : bt.lo_inv, bt.hi_inv);
-  const size_t smem = (size_t)padded_words(col_tile_words(d)) * 4;
-  k_colinv<<<1u << (d.logC - d.logW), 256, smem, s>>>(in, d, dev_tab(pt), dev_epi(epi));
-  return cudaGetLastError();
-}
 
 cudaError_t launch_pointwise(uint32_t p, uint32_t* a, const uint32_t* b, size_t n, cudaStream_t s) {
   k_pointwise<<<grid_for(n, 256), 256, 0, s>>>(make_fp(p), a, b, n);
@@ -979,6 +895,19 @@ __device__ __forceinline__ void col_tile_load(uint32_t* sm, const uint32_t* src,
   cp_async_wait_all();
 }
 
+// Every thread works on two adjacent columns c, c+1 (c even) of the tile: the
+// pair shares its twiddles, its swizzled addresses and its loop, and moves
+// through shared memory as one 64-bit access (the swizzle never touches the
+// low LOGW bits, so pairs stay adjacent and 8-byte aligned).
+__device__ __forceinline__ void lds_pair(const uint32_t* p, uint32_t& a, uint32_t& b) {
+  const uint2 v = *reinterpret_cast<const uint2*>(p);
+  a = v.x;
+  b = v.y;
+}
+__device__ __forceinline__ void sts_pair(uint32_t* p, uint32_t a, uint32_t b) {
+  *reinterpret_cast<uint2*>(p) = make_uint2(a, b);
+}
+
 // One group over the tile, shared -> registers -> shared.  REDUCE: inputs may be
 // any 32-bit value (CRT lift), reduce them on the way in (first forward group).
 template <int LOGR, int KG, bool INV, bool REDUCE, bool ZH = false>
@@ -987,11 +916,12 @@ __device__ __forceinline__ void col_group_smem(uint32_t* sm, const uint2* tw, co
   constexpr int G = ColGroups<LOGR>::size(KG);
   constexpr int T = ColGroups<LOGR>::top(KG);
   constexpr int S = T - G;
-  constexpr int NINST = C::TE >> G;
+  constexpr int LP = C::LOGW - 1;  // column pairs per row: 2^LP
+  constexpr int NINST = C::TE >> (G + 1);
 #pragma unroll 1
   for (int inst = tid; inst < NINST; inst += 256) {
-    const int c = inst & (C::W - 1);
-    const int rest = inst >> C::LOGW;
+    const int c = (inst & ((1 << LP) - 1)) << 1;
+    const int rest = inst >> LP;
     const int base = rest & ((1 << S) - 1);
     const int p0 = ((rest >> S) << T) + base;
     using A = typename C::P::template Group<S + C::LOGW, G>;
@@ -1000,12 +930,14 @@ __device__ __forceinline__ void col_group_smem(uint32_t* sm, const uint2* tw, co
     uint32_t v[2][1 << G];
 #pragma unroll
     for (int i = 0; i < (ZH ? (1 << G) / 2 : (1 << G)); ++i) {
-      const uint32_t x = sm[A::addr(ab, i)];
-      v[0][i] = REDUCE ? reduce_any(x, q1, f) : x;
+      uint32_t x0, x1;
+      lds_pair(sm + A::addr(ab, i), x0, x1);
+      v[0][i] = REDUCE ? reduce_any(x0, q1, f) : x0;
+      v[1][i] = REDUCE ? reduce_any(x1, q1, f) : x1;
     }
-    bf_group<G, T, INV, 1, false, ZH>(v, tw, base, f);
+    bf_group<G, T, INV, 2, false, ZH>(v, tw, base, f);
 #pragma unroll
-    for (int i = 0; i < (1 << G); ++i) sm[A::addr(ab, i)] = v[0][i];
+    for (int i = 0; i < (1 << G); ++i) sts_pair(sm + A::addr(ab, i), v[0][i], v[1][i]);
   }
 }
 
@@ -1031,11 +963,23 @@ __device__ __forceinline__ void col_inv_groups(uint32_t* sm, const Ptab& pt, int
   }
 }
 
+// Bailey twiddle w_N^{j * bitrev_R(t)} of column j, row t = 2^G b + i (i < 2^G):
+// exponent eb + js * bitrev_G(i).
+struct BaileyCol {
+  uint32_t eb, js;
+  __device__ __forceinline__ BaileyCol(uint32_t j, int b, int logr, int g)
+      : eb(j * brev_c(b, logr - g)), js(j << (logr - g)) {}
+  __device__ __forceinline__ uint32_t apply(uint32_t x, int i, int g, const BigD& bt, const Fp& f) const {
+    return bailey_mul(x, eb + js * brev_c(i, g), bt, f);
+  }
+};
+
 template <int LOGR>
 __device__ __forceinline__ void colfwd_body(const InD& in, uint32_t* __restrict__ out, const BigD& bt, const Ptab& pt) {
   using C = ColCfg<LOGR>;
   constexpr int K = ColGroups<LOGR>::K;
   constexpr int G = C::GL;
+  constexpr int LP = C::LOGW - 1;
   extern __shared__ uint32_t sm[];
   const int tid = threadIdx.x, logC = bt.logC;
   const int j0 = blockIdx.x << C::LOGW;
@@ -1052,13 +996,13 @@ __device__ __forceinline__ void colfwd_body(const InD& in, uint32_t* __restrict_
     __syncthreads();
     col_fwd_groups<LOGR, 0>(sm, pt, in.reduce != 0, tid);
   }
-  // last group: shared -> registers -> Bailey twiddle -> global
-  constexpr int NINST = C::TE >> G;
+  // last group: shared -> registers -> Bailey twiddle -> global (64-bit stores)
+  constexpr int NINST = C::TE >> (G + 1);
   const bool reduce_here = K == 1 && in.reduce;
 #pragma unroll 1
   for (int inst = tid; inst < NINST; inst += 256) {
-    const int c = inst & (C::W - 1);
-    const int b = inst >> C::LOGW;
+    const int c = (inst & ((1 << LP) - 1)) << 1;
+    const int b = inst >> LP;
     const int p0 = b << G;
     using A = typename C::P::template Group<C::LOGW, G>;
     int ab[A::P];
@@ -1066,19 +1010,18 @@ __device__ __forceinline__ void colfwd_body(const InD& in, uint32_t* __restrict_
     uint32_t v[2][1 << G];
 #pragma unroll
     for (int i = 0; i < (1 << G); ++i) {
-      const uint32_t x = sm[A::addr(ab, i)];
-      v[0][i] = reduce_here ? reduce_any(x, pt.q1, f) : x;
+      uint32_t x0, x1;
+      lds_pair(sm + A::addr(ab, i), x0, x1);
+      v[0][i] = reduce_here ? reduce_any(x0, pt.q1, f) : x0;
+      v[1][i] = reduce_here ? reduce_any(x1, pt.q1, f) : x1;
     }
-    bf_group<G, G, false, 1, true>(v, pt.fwd, 0, f);
+    bf_group<G, G, false, 2, true>(v, pt.fwd, 0, f);
     const uint32_t j = j0 + c;
-    const uint32_t eb = j * brev_c(b, LOGR - G);
-    const uint32_t js = j << (LOGR - G);
+    const BaileyCol w0(j, b, LOGR, G), w1(j + 1, b, LOGR, G);
 #pragma unroll
-    for (int i = 0; i < (1 << G); ++i) {
-      const uint32_t ex = eb + js * brev_c(i, G);
-      uint32_t w = shoup(v[0][i], __ldg(bt.lo + (ex & 4095u)), f.p);
-      out[((p0 + i) << logC) + j] = shoup(w, __ldg(bt.hi + (ex >> 12)), f.p);
-    }
+    for (int i = 0; i < (1 << G); ++i)
+      *reinterpret_cast<uint2*>(out + ((size_t)(p0 + i) << logC) + j) =
+          make_uint2(w0.apply(v[0][i], i, G, bt, f), w1.apply(v[1][i], i, G, bt, f));
   }
 }
 
@@ -1094,6 +1037,7 @@ __device__ __forceinline__ void colinv_body(const uint32_t* __restrict__ in, con
                                             const EpiD& epi) {
   using C = ColCfg<LOGR>;
   constexpr int K = ColGroups<LOGR>::K;
+  constexpr int LP = C::LOGW - 1;
   extern __shared__ uint32_t sm[];
   const int tid = threadIdx.x, logC = bt.logC;
   const int j0 = blockIdx.x << C::LOGW;
@@ -1103,32 +1047,36 @@ __device__ __forceinline__ void colinv_body(const uint32_t* __restrict__ in, con
   // first: the smallest blocks (Bailey twiddle on the way in), in place
   {
     constexpr int G = C::GL;
-    constexpr int NINST = C::TE >> G;
+    constexpr int NINST = C::TE >> (G + 1);
 #pragma unroll 1
     for (int inst = tid; inst < NINST; inst += 256) {
-      const int c = inst & (C::W - 1);
-      const int b = inst >> C::LOGW;
+      const int c = (inst & ((1 << LP) - 1)) << 1;
+      const int b = inst >> LP;
       const int p0 = b << G;
       const uint32_t j = j0 + c;
-      const uint32_t eb = j * brev_c(b, LOGR - G);
-      const uint32_t js = j << (LOGR - G);
+      const BaileyCol w0(j, b, LOGR, G), w1(j + 1, b, LOGR, G);
       using A = typename C::P::template Group<C::LOGW, G>;
       int ab[A::P];
       A::bases((p0 << C::LOGW) + c, ab);
       uint32_t v[2][1 << G];
 #pragma unroll
       for (int i = 0; i < (1 << G); ++i) {
-        const uint32_t ex = eb + js * brev_c(i, G);
-        uint32_t w = shoup(sm[A::addr(ab, i)], __ldg(bt.lo + (ex & 4095u)), f.p);
-        v[0][i] = shoup(w, __ldg(bt.hi + (ex >> 12)), f.p);
+        uint32_t x0, x1;
+        lds_pair(sm + A::addr(ab, i), x0, x1);
+        v[0][i] = w0.apply(x0, i, G, bt, f);
+        v[1][i] = w1.apply(x1, i, G, bt, f);
       }
-      bf_group<G, G, true, 1, true>(v, pt.inv, 0, f);
+      bf_group<G, G, true, 2, true>(v, pt.inv, 0, f);
       if constexpr (K == 1) {
 #pragma unroll
-        for (int i = 0; i < (1 << G); ++i) epi_store_t<PLAIN>(epi, (uint32_t)(((p0 + i) << logC) + j), v[0][i], f);
+        for (int i = 0; i < (1 << G); ++i) {
+          const uint32_t gi = (uint32_t)(((p0 + i) << logC) + j);
+          epi_store_t<PLAIN>(epi, gi, v[0][i], f);
+          epi_store_t<PLAIN>(epi, gi + 1, v[1][i], f);
+        }
       } else {
 #pragma unroll
-        for (int i = 0; i < (1 << G); ++i) sm[A::addr(ab, i)] = v[0][i];
+        for (int i = 0; i < (1 << G); ++i) sts_pair(sm + A::addr(ab, i), v[0][i], v[1][i]);
       }
     }
   }
@@ -1138,21 +1086,24 @@ __device__ __forceinline__ void colinv_body(const uint32_t* __restrict__ in, con
     // last: the full column blocks, shared -> registers -> epilogue (global)
     constexpr int G = ColGroups<LOGR>::size(0);
     constexpr int S = LOGR - G;
-    constexpr int NINST = C::TE >> G;
+    constexpr int NINST = C::TE >> (G + 1);
 #pragma unroll 1
     for (int inst = tid; inst < NINST; inst += 256) {
-      const int c = inst & (C::W - 1);
-      const int base = inst >> C::LOGW;
+      const int c = (inst & ((1 << LP) - 1)) << 1;
+      const int base = inst >> LP;
       using A = typename C::P::template Group<S + C::LOGW, G>;
       int ab[A::P];
       A::bases((base << C::LOGW) + c, ab);
       uint32_t v[2][1 << G];
 #pragma unroll
-      for (int i = 0; i < (1 << G); ++i) v[0][i] = sm[A::addr(ab, i)];
-      bf_group<G, LOGR, true, 1>(v, pt.inv, base, f);
+      for (int i = 0; i < (1 << G); ++i) lds_pair(sm + A::addr(ab, i), v[0][i], v[1][i]);
+      bf_group<G, LOGR, true, 2>(v, pt.inv, base, f);
 #pragma unroll
-      for (int i = 0; i < (1 << G); ++i)
-        epi_store_t<PLAIN>(epi, (uint32_t)(((base + (i << S)) << logC) + j0 + c), v[0][i], f);
+      for (int i = 0; i < (1 << G); ++i) {
+        const uint32_t gi = (uint32_t)(((base + (i << S)) << logC) + j0 + c);
+        epi_store_t<PLAIN>(epi, gi, v[0][i], f);
+        epi_store_t<PLAIN>(epi, gi + 1, v[1][i], f);
+      }
     }
   }
 }
@@ -1221,7 +1172,7 @@ cudaError_t launch_colfwd(const PrimeTables& pt, const BigTables& bt, int nops, 
     ops.out[i] = out[i];
   }
   BigD d{bt.logR, bt.logC, Cols::logw(bt.logR), reinterpret_cast<const uint2*>(bt.lo_fwd),
-         reinterpret_cast<const uint2*>(bt.hi_fwd)};
+         reinterpret_cast<const uint2*>(bt.mid_fwd), reinterpret_cast<const uint2*>(bt.hi_fwd)};
   ColFwdFn fn = Cols::fwd(bt.logR);
   if (!fn || d.logW > bt.logC) return cudaErrorInvalidValue;
   dim3 grid(1u << (bt.logC - d.logW), (unsigned)nops);
@@ -1233,7 +1184,7 @@ cudaError_t launch_colinv(const PrimeTables& pt, const BigTables& bt, const uint
                                const Epi& epi, cudaStream_t s) {
   BigD d{bt.logR, bt.logC, Cols::logw(bt.logR),
          reinterpret_cast<const uint2*>(mont_scaled ? bt.lo_inv_r : bt.lo_inv),
-         reinterpret_cast<const uint2*>(bt.hi_inv)};
+         reinterpret_cast<const uint2*>(bt.mid_inv), reinterpret_cast<const uint2*>(bt.hi_inv)};
   ColInvFn fn = Cols::inv(bt.logR, host_epi_plain(epi));
   if (!fn || d.logW > bt.logC) return cudaErrorInvalidValue;
   fn<<<1u << (bt.logC - d.logW), 256, Cols::words(bt.logR) * 4, s>>>(in, d, dev_tab(pt), dev_epi(epi));
@@ -1489,10 +1440,10 @@ cudaError_t launch_batch(const BatchPlan& b, void* host_staging, void* dev_desc,
         BigJobB j{};
         j.pt = pt;
         j.bf = BigD{bt.logR, bt.logC, Cols::logw(bt.logR), reinterpret_cast<const uint2*>(bt.lo_fwd),
-                    reinterpret_cast<const uint2*>(bt.hi_fwd)};
+                    reinterpret_cast<const uint2*>(bt.mid_fwd), reinterpret_cast<const uint2*>(bt.hi_fwd)};
         j.bi = BigD{bt.logR, bt.logC, Cols::logw(bt.logR),
                     reinterpret_cast<const uint2*>(x.ymode != 0 ? bt.lo_inv_r : bt.lo_inv),
-                    reinterpret_cast<const uint2*>(bt.hi_inv)};
+                    reinterpret_cast<const uint2*>(bt.mid_inv), reinterpret_cast<const uint2*>(bt.hi_inv)};
         j.in[0] = dev_in(x.x);
         j.in[1] = dev_in(x.y);
         j.t[0] = x.t1;

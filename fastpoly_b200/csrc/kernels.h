@@ -23,13 +23,17 @@ struct PrimeTables {
 };
 
 // Per-(prime, N) tables for the two-pass (four-step) decomposition.
+// The Bailey twiddle w_N^e (e < N) is lo[e & 255] * mid[(e >> 8) & 255] *
+// hi[e >> 16]: three small tables instead of one of N entries.
 struct BigTables {
   int logN = 0, logR = 0, logC = 0;
-  const Tw2* lo_fwd = nullptr;     // w_N^y, y < 4096
-  const Tw2* hi_fwd = nullptr;     // w_N^(4096 x), x < N/4096
+  const Tw2* lo_fwd = nullptr;     // w_N^y, y < 256
+  const Tw2* mid_fwd = nullptr;    // w_N^(256 y), y < 256
+  const Tw2* hi_fwd = nullptr;     // w_N^(65536 y), y < max(1, N / 65536)
   const Tw2* lo_inv = nullptr;     // w_N^-y / N
   const Tw2* lo_inv_r = nullptr;   // w_N^-y * 2^32 / N  (after a Montgomery pointwise)
-  const Tw2* hi_inv = nullptr;     // w_N^-(4096 x)
+  const Tw2* mid_inv = nullptr;    // w_N^-(256 y)
+  const Tw2* hi_inv = nullptr;     // w_N^-(65536 y)
 };
 
 // A forward-transform input: values at ptr[0, count), zero beyond.

@@ -32,18 +32,21 @@ namespace {
 constexpr int kMaxLog = 20;                       // largest transform: 2^20 points
 constexpr size_t kMaxN = size_t(1) << kMaxLog;
 constexpr size_t kSmallWords = size_t(2) << 13;   // 2^13 (value, quotient) pairs
-constexpr size_t kLoWords = 2 * 4096;
-constexpr size_t kHiWords = 2 * (kMaxN >> 12);
+constexpr size_t kLoWords = 2 * 256;                // Bailey lo and mid tables: 256 pairs each
+constexpr size_t kHiWords = 2 * ((kMaxN >> 16) > 0 ? (kMaxN >> 16) : 1);
 // Layout in 32-bit words: two transform buffers, forward and inverse per-prime
-// tables, forward Bailey tables, inverse Bailey tables (scaled by 2^32 / N).
+// tables, forward Bailey tables (lo, mid, hi), inverse Bailey tables (lo scaled
+// by 2^32 / N, mid, hi).
 constexpr size_t kOffT1 = 0;
 constexpr size_t kOffT2 = kMaxN;
 constexpr size_t kOffFwd = 2 * kMaxN;
 constexpr size_t kOffInv = kOffFwd + kSmallWords;
 constexpr size_t kOffLoF = kOffInv + kSmallWords;
-constexpr size_t kOffHiF = kOffLoF + kLoWords;
+constexpr size_t kOffMidF = kOffLoF + kLoWords;
+constexpr size_t kOffHiF = kOffMidF + kLoWords;
 constexpr size_t kOffLoI = kOffHiF + kHiWords;
-constexpr size_t kOffHiI = kOffLoI + kLoWords;
+constexpr size_t kOffMidI = kOffLoI + kLoWords;
+constexpr size_t kOffHiI = kOffMidI + kLoWords;
 constexpr size_t kWords = kOffHiI + kHiWords;
 
 static __device__ __align__(256) uint32_t g_noalloc_scratch[kWords];
@@ -53,7 +56,7 @@ struct Roots {
   uint32_t w[14], wi[14];  // w[lg] = primitive 2^lg-th root of unity and its inverse (lg <= 13)
   uint32_t wN, wNi;        // primitive N-th root and inverse (two-pass sizes)
   uint32_t inv_scale;      // 2^32 / N mod p
-  uint32_t nhi;            // N / 4096 (0 for one-CTA sizes)
+  uint32_t nhi;            // max(1, N / 65536) (0 for one-CTA sizes)
 };
 
 __device__ uint32_t mulm(uint32_t a, uint32_t b, uint32_t p) { return (uint32_t)((uint64_t)a * b % p); }
@@ -72,7 +75,7 @@ __device__ void put(uint32_t* t, size_t i, uint32_t w, uint32_t p) {
 __global__ void k_noalloc_tables(Roots r) {
   uint32_t* s = g_noalloc_scratch;
   const uint32_t p = r.p;
-  const size_t total = (size_t(1) << 13) + 4096 + r.nhi;
+  const size_t total = (size_t(1) << 13) + 512 + r.nhi;
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
     if (i < (size_t(1) << 13)) {
       if (i == 0) {
@@ -85,15 +88,20 @@ __global__ void k_noalloc_tables(Roots r) {
       const uint32_t k = (uint32_t)i - h;
       put(s + kOffFwd, i, powm_dev(r.w[lg], k, p), p);
       put(s + kOffInv, i, powm_dev(r.wi[lg], k, p), p);
-    } else if (i < (size_t(1) << 13) + 4096) {
+    } else if (i < (size_t(1) << 13) + 512) {
       if (!r.nhi) continue;
       const uint32_t y = (uint32_t)(i - (size_t(1) << 13));
-      put(s + kOffLoF, y, powm_dev(r.wN, y, p), p);
-      put(s + kOffLoI, y, mulm(powm_dev(r.wNi, y, p), r.inv_scale, p), p);
-    } else {
-      const uint32_t x = (uint32_t)(i - (size_t(1) << 13) - 4096);
-      put(s + kOffHiF, x, powm_dev(r.wN, 4096u * x, p), p);
-      put(s + kOffHiI, x, powm_dev(r.wNi, 4096u * x, p), p);
+      if (y < 256) {  // w_N^y, inverse scaled by 2^32 / N
+        put(s + kOffLoF, y, powm_dev(r.wN, y, p), p);
+        put(s + kOffLoI, y, mulm(powm_dev(r.wNi, y, p), r.inv_scale, p), p);
+      } else {        // w_N^(256 y)
+        put(s + kOffMidF, y - 256, powm_dev(r.wN, 256u * (y - 256), p), p);
+        put(s + kOffMidI, y - 256, powm_dev(r.wNi, 256u * (y - 256), p), p);
+      }
+    } else {  // w_N^(65536 x)
+      const uint32_t x = (uint32_t)(i - (size_t(1) << 13) - 512);
+      put(s + kOffHiF, x, powm_dev(r.wN, 65536u * x, p), p);
+      put(s + kOffHiI, x, powm_dev(r.wNi, 65536u * x, p), p);
     }
   }
 }
@@ -165,7 +173,7 @@ extern "C" int fpx_conv_noalloc(uint32_t p, const uint32_t* d_a, size_t la, cons
     r.wN = fpx::powm(g, (p - 1) >> logN, p);
     r.wNi = fpx::invm(r.wN, p);
     r.inv_scale = scale;
-    r.nhi = N >> 12;
+    r.nhi = (N >> 16) > 0 ? (N >> 16) : 1;
   }
   k_noalloc_tables<<<64, 256, 0, s>>>(r);
   if (cudaGetLastError() != cudaSuccess) return FPX_ECUDA;
@@ -195,8 +203,10 @@ extern "C" int fpx_conv_noalloc(uint32_t p, const uint32_t* d_a, size_t la, cons
     bt.logC = 12;
     bt.logR = logN - 12;
     bt.lo_fwd = reinterpret_cast<const fpx::Tw2*>(base + kOffLoF);
+    bt.mid_fwd = reinterpret_cast<const fpx::Tw2*>(base + kOffMidF);
     bt.hi_fwd = reinterpret_cast<const fpx::Tw2*>(base + kOffHiF);
     bt.lo_inv_r = reinterpret_cast<const fpx::Tw2*>(base + kOffLoI);
+    bt.mid_inv = reinterpret_cast<const fpx::Tw2*>(base + kOffMidI);
     bt.hi_inv = reinterpret_cast<const fpx::Tw2*>(base + kOffHiI);
     uint32_t* t1 = base + kOffT1;
     uint32_t* t2 = base + kOffT2;
