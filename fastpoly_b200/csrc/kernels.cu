@@ -96,6 +96,26 @@ __device__ __forceinline__ void epi_store_t(const EpiD& e, uint32_t gi, uint32_t
     epi_store(e, gi, x, f);
   }
 }
+// Two adjacent outputs gi, gi + 1 of the plain epilogue: one 64-bit store when
+// both fall in the window and the destination is 8-byte aligned.
+template <bool PLAIN>
+__device__ __forceinline__ void epi_store_pair(const EpiD& e, uint32_t gi, uint32_t x0, uint32_t x1, const Fp& f) {
+  if constexpr (PLAIN) {
+    if (gi >= e.lo && gi + 1 < e.hi) {
+      uint32_t* o = e.out + (gi - e.lo);
+      const uint32_t y0 = red(red(x0, f.p2), f.p), y1 = red(red(x1, f.p2), f.p);
+      if (((uintptr_t)o & 7u) == 0) {
+        *reinterpret_cast<uint2*>(o) = make_uint2(y0, y1);
+      } else {
+        o[0] = y0;
+        o[1] = y1;
+      }
+      return;
+    }
+  }
+  epi_store_t<PLAIN>(e, gi, x0, f);
+  epi_store_t<PLAIN>(e, gi + 1, x1, f);
+}
 bool host_epi_plain(const fpx::Epi& e) {
   return e.scale.w == 0 && !e.mul_mont && !e.negate && !e.sub_from && !e.accumulate;
 }
@@ -1069,11 +1089,8 @@ __device__ __forceinline__ void colinv_body(const uint32_t* __restrict__ in, con
       bf_group<G, G, true, 2, true>(v, pt.inv, 0, f);
       if constexpr (K == 1) {
 #pragma unroll
-        for (int i = 0; i < (1 << G); ++i) {
-          const uint32_t gi = (uint32_t)(((p0 + i) << logC) + j);
-          epi_store_t<PLAIN>(epi, gi, v[0][i], f);
-          epi_store_t<PLAIN>(epi, gi + 1, v[1][i], f);
-        }
+        for (int i = 0; i < (1 << G); ++i)
+          epi_store_pair<PLAIN>(epi, (uint32_t)(((p0 + i) << logC) + j), v[0][i], v[1][i], f);
       } else {
 #pragma unroll
         for (int i = 0; i < (1 << G); ++i) sts_pair(sm + A::addr(ab, i), v[0][i], v[1][i]);
@@ -1099,11 +1116,8 @@ __device__ __forceinline__ void colinv_body(const uint32_t* __restrict__ in, con
       for (int i = 0; i < (1 << G); ++i) lds_pair(sm + A::addr(ab, i), v[0][i], v[1][i]);
       bf_group<G, LOGR, true, 2>(v, pt.inv, base, f);
 #pragma unroll
-      for (int i = 0; i < (1 << G); ++i) {
-        const uint32_t gi = (uint32_t)(((base + (i << S)) << logC) + j0 + c);
-        epi_store_t<PLAIN>(epi, gi, v[0][i], f);
-        epi_store_t<PLAIN>(epi, gi + 1, v[1][i], f);
-      }
+      for (int i = 0; i < (1 << G); ++i)
+        epi_store_pair<PLAIN>(epi, (uint32_t)(((base + (i << S)) << logC) + j0 + c), v[0][i], v[1][i], f);
     }
   }
 }
