@@ -18,6 +18,15 @@ seeded uniform residues.  Metric: output Mcoeff/s.
 `cpu_baseline` the reference library (compiled from its own headers,
          oracle/_ref) on this host's cores, bounded sample, rank 0 at N = 1.
 Multi-GPU: one process per GPU (torchrun), independent replicas ("weak").
+
+Other workloads, one JSON line each (not the default):
+  --workload batch   4096 convs + 512 inv/exp of mixed sizes and moduli in one
+                     fpx_batch_submit (polys/s), beside the per-call path and
+                     the reference on all host cores
+  --workload serve   the request loop: burst and closed-loop saturation req/s,
+                     then Poisson arrivals at 50 / 80 / 100 % of saturation
+                     with p50 / p99 latency
+  --workload ops     single operations of the reference's configs 1-3
 """
 from __future__ import annotations
 
@@ -583,7 +592,7 @@ def _ref_call(ref, spec):
         return 0.0
 
 
-def cpu_mix_sample(specs, budget_s: float = 20.0, threads: int | None = None):
+def cpu_mix_sample(specs, budget_s: float = 20.0, threads: int | None = None, unit: str = "polys/s"):
     """The reference on this host's cores: one worker thread per core pulling jobs
     of the mix (the library is thread-safe across calls), until the job list or
     the time budget runs out; polys/s over the jobs finished."""
@@ -606,7 +615,7 @@ def cpu_mix_sample(specs, budget_s: float = 20.0, threads: int | None = None):
     with ThreadPoolExecutor(threads) as ex:
         list(ex.map(work, specs))
     el = time.perf_counter() - t0
-    return {"value": round(done[0] / el, 1), "unit": "polys/s", "cores": threads, "kind": "reference",
+    return {"value": round(done[0] / el, 1), "unit": unit, "cores": threads, "kind": "reference",
             "sample": f"{done[0]} of {len(specs)} jobs of the mix on {threads} threads in {el:.1f} s ({ref.backend})"}
 
 
@@ -645,17 +654,29 @@ def run_serve_fpx(args):
         # warm-up: plans, pools and pinned buffers of every worker, on the same mix
         for t in [srv.submit(s) for s in specs]:
             srv.poll(t)
-        # saturation: everything offered at once
+        # burst: everything offered at once (largest micro-batches)
         t0 = time.perf_counter()
         tickets = [srv.submit(s) for s in specs]
-        lat = []
         fails = 0
         for t in tickets:
-            r, l = srv.poll(t)
+            r, _ = srv.poll(t)
             fails += isinstance(r, Exception)
-            lat.append(l)
-        sat_s = time.perf_counter() - t0
-        sat_rate = count / sat_s
+        burst_rate = count / (time.perf_counter() - t0)
+        # saturation: a closed loop of `clients` callers, each submitting its next
+        # request when the previous one completes (the steady state the open-loop
+        # loads below are fractions of)
+        def closed_loop(clients):
+            def client(k):
+                for i in range(k, count, clients):
+                    srv.poll(srv.submit(specs[i]))
+            th = [threading.Thread(target=client, args=(k,)) for k in range(clients)]
+            t0 = time.perf_counter()
+            for t in th:
+                t.start()
+            for t in th:
+                t.join()
+            return count / (time.perf_counter() - t0)
+        sat_rate = closed_loop(args.clients)
         loads = {}
         for frac in (0.5, 0.8, 1.0):
             rate = frac * sat_rate
@@ -690,18 +711,22 @@ def run_serve_fpx(args):
     finally:
         srv.stop()
     in_bytes = 4 * sum(len(s[2]) + (len(s[3]) if s[0] in ("conv", "divmod") else 0) for s in specs)
+    out_bytes = 4 * sum(len(s[2]) + len(s[3]) - 1 if s[0] == "conv" else
+                        (len(s[2]) + len(s[3]) if s[0] == "divmod" else s[-1]) for s in specs)
     line = {"metric": "served requests/s at saturation (mixed ops, sizes 2^8..2^%d)" % args.serve_max_log,
             "value": round(sat_rate, 2), "unit": "req/s", "n_gpus": 1, "steps": count, "warmup": count,
             "ms_per_step": round(1e3 / sat_rate, 3), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "u32", "data": "synthetic",
             "config": {"workload": "conv 40 / inv 20 / exp 15 / sqrt 10 / divmod 10 / pow 5 %, sizes log-uniform "
                                    f"2^8..2^{args.serve_max_log}, moduli 998244353 / 167772161 / 1e9+7 / 2^31-1",
-                       "requests": count, "workers": args.workers, "failed": int(fails)},
+                       "requests": count, "workers": args.workers, "failed": int(fails),
+                       "saturation": f"closed loop of {args.clients} callers"},
             "latency": loads, "server": st,
+            "burst_req_s": round(burst_rate, 2),
             "e2e": {"value": round(sat_rate, 2), "unit": "req/s", "h2d_bytes_per_step": in_bytes // count,
-                    "d2h_bytes_per_step": None, "api": "fpx_serve_submit / fpx_serve_poll (host buffers)"}}
+                    "d2h_bytes_per_step": out_bytes // count, "api": "fpx_serve_submit / fpx_serve_poll (host buffers)"}}
     if not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_mix_sample(specs, budget_s=30.0)
+        line["cpu_baseline"] = cpu_mix_sample(specs, budget_s=30.0, unit="req/s")
     print(json.dumps(line))
     return 0
 
@@ -819,9 +844,10 @@ def main():
     ap.add_argument("--workload", default="conv", choices=["conv", "batch", "serve", "ops"],
                     help="conv: the headline 2^23 conv (default); batch: mixed batch; serve: request loop; "
                          "ops: single operations of configs 1-3")
-    ap.add_argument("--requests", type=int, default=300, help="serve: requests per load level")
+    ap.add_argument("--requests", type=int, default=600, help="serve: requests per load level")
     ap.add_argument("--serve-max-log", type=int, default=22, help="serve: largest size 2^k")
     ap.add_argument("--workers", type=int, default=2, help="serve: micro-batches in flight")
+    ap.add_argument("--clients", type=int, default=32, help="serve: callers of the closed-loop saturation run")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
@@ -834,7 +860,7 @@ def main():
             rank, _, world = env_rank()
             if rank == 0:
                 specs = serve_mix(args.requests, max_log=args.serve_max_log)
-                b = cpu_mix_sample(specs, budget_s=60.0)
+                b = cpu_mix_sample(specs, budget_s=60.0, unit="req/s")
                 print(json.dumps({"impl": "reference", "metric": "served requests/s at saturation", "value": b["value"],
                                   "unit": "req/s", "n_gpus": world, "higher_is_better": True, "cpu_baseline": b,
                                   "e2e": {"value": b["value"], "unit": "req/s", "h2d_bytes_per_step": 0,
