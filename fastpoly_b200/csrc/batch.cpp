@@ -278,6 +278,13 @@ void Engine::convert_repr(const std::vector<ReprSeg>& segs) {
   launches_ += (segs.size() + 65534) / 65535;
 }
 
+void Engine::window_product(uint32_t p, const uint32_t* a, size_t la, const uint32_t* b, size_t lb, size_t off,
+                            size_t cnt, uint32_t* out, int cyc_log, const uint32_t* post_mont, bool negate) {
+  BatchRec rec(*this);
+  rec.product(p, a, la, b, lb, off, cnt, out, cyc_log, post_mont, negate);
+  rec.flush();
+}
+
 // ------------------------------------------------- lockstep inverse extension
 
 // Five transforms at N = 2k for a native prime (as Engine::extend_inverse):

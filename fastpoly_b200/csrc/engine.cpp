@@ -516,6 +516,12 @@ void Engine::product(uint32_t p, const uint32_t* a, size_t la, const uint32_t* b
     cyc_product(p, logN, op);
     return;
   }
+  if (!accumulate && logN <= 24) {
+    // one block pair: the auxiliary primes' transforms share one launch set and
+    // the Garner epilogue applies post_mont
+    window_product(p, a, la, b, lb, 0, outn, out, 0, post_mont, false);
+    return;
+  }
   crt_product(p, a, la, b, lb, outn, out, accumulate);
   if (post_mont) kcheck(launch_mul_mont_tab(p, out, post_mont, out, outn, stream_), "post scale");
 }
@@ -629,6 +635,13 @@ void Engine::extend_inverse(uint32_t p, const uint32_t* a, size_t la, uint32_t* 
   }
   // crt_middle_product + conv_limbs (inverse.hpp:35-42).
   Buf e(&pool_, hlen);
+  if (logN <= 24) {
+    // the middle product is free of wraparound at N = 2k: CRT transforms of
+    // 2k points instead of the full product's 4k, negation in the Garner epilogue
+    window_product(p, a, aw, c, k, k, hlen, e.get(), logN, nullptr, true);
+    window_product(p, e.get(), hlen, c, k, 0, hlen, c + k, logN, nullptr, false);
+    return;
+  }
   mul_window(p, a, aw, c, k, k, hlen, e.get());
   kcheck(launch_scale(p, e.get(), e.get(), hlen, p - 1, stream_), "negate");
   product(p, e.get(), hlen, c, k, hlen, c + k);
@@ -735,7 +748,8 @@ void Engine::exp_into(uint32_t p, const uint32_t* a, size_t la, size_t n, uint32
       cyc_product(p, logN, op3);
     } else {
       Buf t1(&pool_, hlen), t2(&pool_, hlen);
-      mul_window(p, ap.get(), lx, out, m, m - 1, hlen, t1.get());
+      if (logN <= 24) window_product(p, ap.get(), lx, out, m, m - 1, hlen, t1.get(), logN, nullptr, false);
+      else mul_window(p, ap.get(), lx, out, m, m - 1, hlen, t1.get());
       product(p, t1.get(), hlen, c.get(), csize, hlen, t2.get(), tab + m);
       product(p, t2.get(), hlen, out, m, hlen, out + m);
     }

@@ -159,6 +159,11 @@ class Engine {
   void crt_product(uint32_t p, const uint32_t* a, size_t la, const uint32_t* b, size_t lb, size_t outn,
                    uint32_t* out, bool accumulate);
   // Exact coefficients [off, off+cnt) of a*b.
+  // The same window through the batch recorder (batch.cpp): one launch set,
+  // 3-prime CRT with batched Garner for non-native primes; cyc_log > 0 is a
+  // cyclic size that leaves the window free of wraparound (<= 2^24 points).
+  void window_product(uint32_t p, const uint32_t* a, size_t la, const uint32_t* b, size_t lb, size_t off,
+                      size_t cnt, uint32_t* out, int cyc_log, const uint32_t* post_mont, bool negate);
   void mul_window(uint32_t p, const uint32_t* a, size_t la, const uint32_t* b, size_t lb, size_t off, size_t cnt,
                   uint32_t* out);
   // c[0,k) -> c[0,wanted) for the inverse of a (inverse.hpp:18-65).
