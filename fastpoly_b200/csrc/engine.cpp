@@ -516,9 +516,10 @@ void Engine::product(uint32_t p, const uint32_t* a, size_t la, const uint32_t* b
     cyc_product(p, logN, op);
     return;
   }
-  if (!accumulate && logN <= 24) {
-    // one block pair: the auxiliary primes' transforms share one launch set and
-    // the Garner epilogue applies post_mont
+  if (!accumulate && logN <= 20) {
+    // one block pair of at most 2^20 points: the auxiliary primes' transforms
+    // share one launch set and the Garner epilogue applies post_mont (larger
+    // products measured 4 % faster on separate per-prime launches)
     window_product(p, a, la, b, lb, 0, outn, out, 0, post_mont, false);
     return;
   }
