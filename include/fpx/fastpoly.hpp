@@ -21,9 +21,12 @@
 
 #include <algorithm>
 #include <array>
+#include <bit>
 #include <cstdint>
 #include <cstdlib>
+#include <cstring>
 #include <istream>
+#include <map>
 #include <memory>
 #include <mutex>
 #include <ostream>
@@ -238,6 +241,33 @@ uint32_t* limbs(std::vector<M>& v) {
 
 }  // namespace gpu
 
+// ------------------------------------------------------- scratch memory
+
+/// The reference's scratch statistics (memory.hpp:21-26), here of the GPU
+/// context's device pool (one per process rather than per thread).
+struct ScratchMemoryStats {
+  size_t cached_bytes = 0;
+  size_t cached_blocks = 0;
+  size_t system_allocations = 0;
+  size_t cache_hits = 0;
+};
+inline ScratchMemoryStats scratch_memory_stats() noexcept {
+  fpx_pool_stats_t st{};
+  try {
+    if (fpx_pool_stats(gpu::context(), &st) != FPX_OK) return {};
+  } catch (...) {
+    return {};
+  }
+  return ScratchMemoryStats{st.cached_bytes, st.cached_blocks, st.system_allocations, st.cache_hits};
+}
+/// Frees the idle cached blocks (memory.hpp:252-254); live buffers and plans stay.
+inline void release_scratch_memory() noexcept {
+  try {
+    (void)fpx_release_pool(gpu::context());
+  } catch (...) {
+  }
+}
+
 // ---------------------------------------------------------------- NttPlan
 
 /// GPU transform of one size (the reference's NttPlan<M>, ntt.hpp:86-194):
@@ -251,9 +281,38 @@ class NttPlan {
     check_size(n);
     return std::shared_ptr<const NttPlan>(new NttPlan(n));
   }
+  /// One plan per size for the life of the process (ntt.hpp:135).
+  static const NttPlan& get_ref(uint32_t n) {
+    check_size(n);
+    static std::mutex mu;
+    static std::map<uint32_t, std::unique_ptr<NttPlan>> plans;
+    std::lock_guard<std::mutex> g(mu);
+    auto& slot = plans[n];
+    if (!slot) slot.reset(new NttPlan(n));
+    return *slot;
+  }
   uint32_t size() const { return n_; }
+  int log_size() const { return std::countr_zero(n_); }
   void forward(uint32_t* a) const { gpu::check(fpx_ntt_forward(gpu::context(), M::mod, a, n_, FPX_REPR_MONTGOMERY), "ntt"); }
   void inverse(uint32_t* a) const { gpu::check(fpx_ntt_inverse(gpu::context(), M::mod, a, n_, FPX_REPR_MONTGOMERY), "ntt"); }
+  /// The reference's lazy forward (ntt.hpp:145-148): same permutation and residues
+  /// as forward(); the GPU returns them reduced, a valid lazy representative.
+  void forward_lazy(uint32_t* a) const { forward(a); }
+  /// Forward transform of a live prefix a[0, count), [count, n) taken as zero
+  /// (ntt.hpp:150-175): those limbs are overwritten with zeros first.
+  void forward_prefix(uint32_t* a, size_t count) const {
+    if (count > n_) throw ntt_size_error("NTT input prefix exceeds plan size");
+    std::memset(a + count, 0, (n_ - count) * sizeof(uint32_t));
+    forward(a);
+  }
+  /// Inverse whose caller needs only [0, count) (ntt.hpp:181-188); every output
+  /// is produced, the rest is valid too.
+  void inverse_prefix(uint32_t* a, size_t count) const {
+    if (count > n_) throw ntt_size_error("NTT output prefix exceeds plan size");
+    inverse(a);
+  }
+  /// Inverse whose caller needs only the high half [n/2, n) (ntt.hpp:190-191).
+  void inverse_highhalf(uint32_t* a) const { inverse(a); }
 
  private:
   explicit NttPlan(uint32_t n) : n_(n) {}

@@ -145,6 +145,36 @@ int main() {
     bool threw = false;
     try { (void)NttPlan<M>::get(1u << 24); } catch (const ntt_size_error&) { threw = true; }
     CHECK(threw);
+    // window contracts (tests/test_ntt.cpp:289-336): a prefix forward equals the
+    // zero-padded forward, the prefix / high-half inverses give back the window
+    std::mt19937_64 g(11);
+    const uint32_t m = 1024;
+    const auto& big = NttPlan<M>::get_ref(m);
+    CHECK(&big == &NttPlan<M>::get_ref(m) && big.log_size() == 10);
+    std::vector<uint32_t> x(m), padded(m, 0);
+    for (uint32_t i = 0; i < 300; ++i) x[i] = padded[i] = M::from_int(g() % M::mod).raw_val();
+    const auto orig = padded;
+    for (uint32_t i = 300; i < m; ++i) x[i] = 12345;  // garbage past the prefix
+    big.forward_prefix(x.data(), 300);
+    big.forward_lazy(padded.data());
+    CHECK(x == padded);
+    auto lo = x, hi = x;
+    big.inverse_prefix(lo.data(), 300);
+    big.inverse_highhalf(hi.data());
+    bool lo_ok = true, hi_ok = true;
+    for (uint32_t i = 0; i < 300; ++i) lo_ok = lo_ok && lo[i] == orig[i];
+    CHECK(lo_ok);
+    for (uint32_t i = m / 2; i < m; ++i) hi_ok = hi_ok && hi[i] == orig[i];
+    CHECK(hi_ok);
+    threw = false;
+    try { big.forward_prefix(x.data(), m + 1); } catch (const ntt_size_error&) { threw = true; }
+    CHECK(threw);
+  }
+  {  // scratch statistics of the device pool (memory.hpp:21-26, 252-258)
+    const auto st = scratch_memory_stats();
+    CHECK(st.system_allocations > 0);
+    release_scratch_memory();
+    CHECK(scratch_memory_stats().cached_bytes == 0);
   }
   std::printf(failures ? "FAILED (%d)\n" : "all drop-in checks passed\n", failures);
   return failures ? 1 : 0;
