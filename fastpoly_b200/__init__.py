@@ -102,6 +102,9 @@ def load_library(path: str = LIB_PATH):
     L.fpx_serve_stop.argtypes = [vp]
     L.fpx_serve_plan_bytes.argtypes = [vp]
     L.fpx_serve_plan_bytes.restype = sz
+    L.fpx_col_shape_candidates.argtypes = [vp, i32, i32, vp, i32, C.POINTER(i32)]
+    L.fpx_col_shape_get.argtypes = [vp, i32, i32, vp]
+    L.fpx_col_shape_set.argtypes = [vp, i32, i32, vp]
     _lib = L
     return L
 
@@ -109,6 +112,17 @@ def load_library(path: str = LIB_PATH):
 OP_CONV, OP_INV, OP_LOG, OP_EXP, OP_SQRT, OP_POW, OP_DIVMOD = range(7)
 _OPS = {"conv": OP_CONV, "inv": OP_INV, "log": OP_LOG, "exp": OP_EXP, "sqrt": OP_SQRT, "pow": OP_POW,
         "divmod": OP_DIVMOD}
+
+
+class ColShape(C.Structure):
+    """struct fpx_col_shape (include/fpx_b200.h): tile shape of a column pass."""
+    _fields_ = [("lw1", C.c_int), ("lw2", C.c_int), ("split", C.c_int)]
+
+    def astuple(self):
+        return (self.lw1, self.lw2, self.split)
+
+
+COL_FWD1, COL_FWD2, COL_INV = 0, 1, 2
 
 
 class Job(C.Structure):
@@ -314,6 +328,25 @@ class Context:
 
     def release_pool(self):
         self._check(self._L.fpx_release_pool(self._h), "release_pool")
+
+    # -- column-pass tile shapes (the tuner's choice per transform size) ----------
+    def col_shape_candidates(self, log_n: int, kind: int) -> list:
+        """Compiled (lw1, lw2, split) shapes of one column pass, the default first."""
+        arr = (ColShape * 8)()
+        cnt = C.c_int(0)
+        self._check(self._L.fpx_col_shape_candidates(self._h, log_n, kind, arr, 8, C.byref(cnt)),
+                    "col_shape_candidates")
+        return [arr[i].astuple() for i in range(min(cnt.value, 8))]
+
+    def col_shape(self, log_n: int, kind: int) -> tuple:
+        """The shape in use (tuned on first use of the size)."""
+        sh = ColShape()
+        self._check(self._L.fpx_col_shape_get(self._h, log_n, kind, C.byref(sh)), "col_shape_get")
+        return sh.astuple()
+
+    def set_col_shape(self, log_n: int, kind: int, shape) -> None:
+        sh = ColShape(*shape)
+        self._check(self._L.fpx_col_shape_set(self._h, log_n, kind, C.byref(sh)), "col_shape_set")
 
     # -- transforms (NttPlan<M>::forward / inverse) ------------------------------
     def ntt_forward(self, p: int, x, repr: int = CANONICAL) -> np.ndarray:

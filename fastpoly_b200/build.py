@@ -25,7 +25,7 @@ NVCC = os.path.join(CUDA_HOME, "bin", "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 CU_SOURCES = ["kernels.cu", "noalloc.cu", "peaks.cu"]
-CPP_SOURCES = ["engine.cpp", "batch.cpp", "serve.cpp", "api.cpp"]
+CPP_SOURCES = ["engine.cpp", "batch.cpp", "serve.cpp", "tune.cpp", "api.cpp"]
 HEADERS = ["field.cuh", "ntt_core.cuh", "ntt_fast.cuh", "kernels.h", "engine.h"]
 
 
@@ -67,8 +67,12 @@ def build(force: bool = False, verbose: bool = False) -> str:
               "-I" + os.path.join(CUDA_HOME, "include"), "-c", os.path.join(CSRC, s), "-o", o], verbose)
         objs.append(o)
     tmp = LIB + ".tmp"
+    # --exclude-libs: symbols of static archives (the CUDA runtime, and the C++
+    # runtime where the toolchain links it statically) stay private, so a host
+    # process holding its own copies (Python with libstdc++.so) cannot interpose
+    # them half-way.
     _run([cxx, "-shared", "-o", tmp, *objs, "-L" + os.path.join(CUDA_HOME, "lib64"), "-lcudart_static", "-ldl",
-          "-lrt", "-pthread"], verbose)
+          "-lrt", "-pthread", "-Wl,--exclude-libs,ALL"], verbose)
     os.replace(tmp, LIB)
     return LIB
 

@@ -154,6 +154,39 @@ int fpx_release_pool(fpx_ctx* ctx) {
   });
 }
 
+int fpx_col_shape_candidates(fpx_ctx* ctx, int log_n, int kind, fpx_col_shape* out, int max, int* count) {
+  if (!out || !count || max < 0) return FPX_EINVAL;
+  return guarded(ctx, [&](fpx::Engine& e) {
+    fpx::ColShape c[8];
+    const int n = e.col_shape_candidates(log_n, kind, c, 8);
+    *count = n;
+    for (int i = 0; i < n && i < max; ++i) out[i] = fpx_col_shape{c[i].lw1, c[i].lw2, c[i].split};
+  });
+}
+
+int fpx_col_shape_get(fpx_ctx* ctx, int log_n, int kind, fpx_col_shape* out) {
+  if (!out) return FPX_EINVAL;
+  return guarded(ctx, [&](fpx::Engine& e) {
+    fpx::ColShape s = e.col_shape(log_n, kind);
+    if (s.lw1 == 0) {  // the default shape, spelled out
+      fpx::ColShape c[8];
+      if (e.col_shape_candidates(log_n, kind, c, 8) > 0) s = c[0];
+    }
+    *out = fpx_col_shape{s.lw1, s.lw2, s.split};
+  });
+}
+
+int fpx_col_shape_set(fpx_ctx* ctx, int log_n, int kind, const fpx_col_shape* shape) {
+  if (!shape) return FPX_EINVAL;
+  return guarded(ctx, [&](fpx::Engine& e) {
+    fpx::ColShape s;
+    s.lw1 = shape->lw1;
+    s.lw2 = shape->lw2;
+    s.split = shape->split;
+    e.set_col_shape(log_n, kind, s);
+  });
+}
+
 int fpx_profile(fpx_ctx* ctx, int enable) {
   return guarded(ctx, [&](fpx::Engine& e) { e.profile(enable != 0); });
 }

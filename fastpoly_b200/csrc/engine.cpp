@@ -337,6 +337,10 @@ static uint32_t* upload(Engine& eng, Buf& dst, const std::vector<Tw2>& v) {
 // into one table indexed by block length): tw[h + k] = w_{2h}^k.
 const PrimePlan& Engine::prime_plan(uint32_t p) {
   std::lock_guard<std::mutex> g(plan_mu_);
+  return prime_plan_locked(p);
+}
+
+const PrimePlan& Engine::prime_plan_locked(uint32_t p) {
   auto it = primes_.find(p);
   if (it != primes_.end()) return *it->second;
   auto plan = std::make_unique<PrimePlan>();
@@ -416,6 +420,7 @@ const BigPlan& Engine::big_plan(uint32_t p, int logN) {
   plan->t.lo_inv_r = reinterpret_cast<const Tw2*>(upload(*this, plan->lo_inv_r, lo_ir));
   plan->t.mid_inv = reinterpret_cast<const Tw2*>(upload(*this, plan->mid_inv, mid_i));
   plan->t.hi_inv = reinterpret_cast<const Tw2*>(upload(*this, plan->hi_inv, hi_i));
+  plan->t.shapes = tuned_shapes_locked(p, plan->t);
   auto& ref = *plan;
   bigs_[key] = std::move(plan);
   return ref;

@@ -127,6 +127,14 @@ class Engine {
   void check(cudaError_t e, const char* what);
   void sync();
 
+  // Column-pass tile shapes of N = 2^logN transforms on this device (kind 0:
+  // forward pass of one operand, 1: of two or three, 2: inverse pass), chosen
+  // by timing the compiled candidates once per process, device and size
+  // (tune.cpp).  Every shape computes the same values.
+  ColShape col_shape(int logN, int kind);
+  int col_shape_candidates(int logN, int kind, ColShape* out, int max);
+  void set_col_shape(int logN, int kind, const ColShape& sh);  // throws Error(FPX_EINVAL) if not compiled
+
   // Per-kernel timing (CUDA events on the launching stream) and launch count.
   void profile(bool on);
   std::string profile_report();  // {"kernel": [launches, total_ms], ...}
@@ -136,7 +144,11 @@ class Engine {
   friend class BatchRec;
   // ---- plans
   const PrimePlan& prime_plan(uint32_t p);
+  const PrimePlan& prime_plan_locked(uint32_t p);  // plan_mu_ held
   const BigPlan& big_plan(uint32_t p, int logN);
+  // The shapes big plans of N = bt's size point to; tunes them on first use
+  // (plan_mu_ held, tables of bt uploaded).
+  const ColShapes* tuned_shapes_locked(uint32_t p, const BigTables& bt);
   const uint32_t* inv_table(uint32_t p, size_t n);  // Montgomery form 1/i, i <= n
 
   bool native(uint32_t p, int logN) const;  // GPU NTT usable for (p, 2^logN)

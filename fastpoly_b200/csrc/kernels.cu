@@ -870,9 +870,13 @@ __global__ void __launch_bounds__(256, 3) k_rows12(uint32_t* __restrict__ x, con
   rows12_body(x, y, ymode, y_spec_out, forward, inverse, pt, blockIdx.x);
 }
 
-template <int LOGR>
+// Default tile width: 2^LOGW columns with R * W = 2^13 words (32 KiB) up to
+// R = 2^10 and 2^14 words (64 KiB) above, so that three CTAs fit on an SM.
+__host__ __device__ constexpr int col_logw(int logr) { return logr >= 11 ? 14 - logr : 13 - logr; }
+
+template <int LOGR, int LW = col_logw(LOGR)>
 struct ColCfg {
-  static constexpr int LOGW = LOGR >= 11 ? 14 - LOGR : 13 - LOGR;
+  static constexpr int LOGW = LW;
   static constexpr int W = 1 << LOGW;
   static constexpr int TE = 1 << (LOGR + LOGW);
   static constexpr int K = ColGroups<LOGR>::K;
@@ -884,18 +888,18 @@ struct ColCfg {
 // Loads the W x R column tile (rows t, columns j0..j0+W) into shared memory
 // with cp.async: all copies in flight at once, no register staging, zero
 // beyond `count`.  16-byte copies when the source is 16-byte aligned.
-template <int LOGR, bool HALF = false>
+template <int LOGR, int LOGW, bool HALF = false>
 __device__ __forceinline__ void col_tile_load(uint32_t* sm, const uint32_t* src, uint32_t count, int j0, int logC,
                                               int tid) {
   // HALF: only rows t < R/2 (the rest are known zeros, never read as such)
-  using C = ColCfg<LOGR>;
+  using C = ColCfg<LOGR, LOGW>;
   constexpr int TL = HALF ? C::TE / 2 : C::TE;
   if (src == nullptr || count == 0) {
     for (int e = tid; e < C::SMEM_WORDS; e += 256) sm[e] = 0u;
     return;
   }
-  if (((uintptr_t)src & 15u) == 0) {
-    constexpr int CPR = C::W / 4;  // 16-byte chunks per row segment
+  if (C::W >= 4 && ((uintptr_t)src & 15u) == 0) {
+    constexpr int CPR = C::W >= 4 ? C::W / 4 : 1;  // 16-byte chunks per row segment
 #pragma unroll 4
     for (int q = tid; q < TL / 4; q += 256) {
       const int t = q / CPR, cc = (q % CPR) * 4;
@@ -930,9 +934,9 @@ __device__ __forceinline__ void sts_pair(uint32_t* p, uint32_t a, uint32_t b) {
 
 // One group over the tile, shared -> registers -> shared.  REDUCE: inputs may be
 // any 32-bit value (CRT lift), reduce them on the way in (first forward group).
-template <int LOGR, int KG, bool INV, bool REDUCE, bool ZH = false>
+template <int LOGR, int LOGW, int KG, bool INV, bool REDUCE, bool ZH = false>
 __device__ __forceinline__ void col_group_smem(uint32_t* sm, const uint2* tw, const Fp& f, uint32_t q1, int tid) {
-  using C = ColCfg<LOGR>;
+  using C = ColCfg<LOGR, LOGW>;
   constexpr int G = ColGroups<LOGR>::size(KG);
   constexpr int T = ColGroups<LOGR>::top(KG);
   constexpr int S = T - G;
@@ -962,24 +966,24 @@ __device__ __forceinline__ void col_group_smem(uint32_t* sm, const uint2* tw, co
 }
 
 // Forward groups 0 .. K-2 (the last group is the caller's).
-template <int LOGR, int KG, bool ZH = false>
+template <int LOGR, int LOGW, int KG, bool ZH = false>
 __device__ __forceinline__ void col_fwd_groups(uint32_t* sm, const Ptab& pt, bool reduce, int tid) {
   if constexpr (KG < ColGroups<LOGR>::K - 1) {
     constexpr bool Z = ZH && KG == 0;
-    if (KG == 0 && reduce) col_group_smem<LOGR, KG, false, true, Z>(sm, pt.fwd, pt.f, pt.q1, tid);
-    else col_group_smem<LOGR, KG, false, false, Z>(sm, pt.fwd, pt.f, pt.q1, tid);
+    if (KG == 0 && reduce) col_group_smem<LOGR, LOGW, KG, false, true, Z>(sm, pt.fwd, pt.f, pt.q1, tid);
+    else col_group_smem<LOGR, LOGW, KG, false, false, Z>(sm, pt.fwd, pt.f, pt.q1, tid);
     __syncthreads();
-    col_fwd_groups<LOGR, KG + 1>(sm, pt, reduce, tid);
+    col_fwd_groups<LOGR, LOGW, KG + 1>(sm, pt, reduce, tid);
   }
 }
 
 // Inverse groups K-2 .. 1 (the first, smallest group and the last, group 0, are the caller's).
-template <int LOGR, int KG>
+template <int LOGR, int LOGW, int KG>
 __device__ __forceinline__ void col_inv_groups(uint32_t* sm, const Ptab& pt, int tid) {
   if constexpr (KG >= 1) {
-    col_group_smem<LOGR, KG, true, false>(sm, pt.inv, pt.f, pt.q1, tid);
+    col_group_smem<LOGR, LOGW, KG, true, false>(sm, pt.inv, pt.f, pt.q1, tid);
     __syncthreads();
-    col_inv_groups<LOGR, KG - 1>(sm, pt, tid);
+    col_inv_groups<LOGR, LOGW, KG - 1>(sm, pt, tid);
   }
 }
 
@@ -994,27 +998,27 @@ struct BaileyCol {
   }
 };
 
-template <int LOGR>
-__device__ __forceinline__ void colfwd_body(const InD& in, uint32_t* __restrict__ out, const BigD& bt, const Ptab& pt) {
-  using C = ColCfg<LOGR>;
+template <int LOGR, int LOGW>
+__device__ __forceinline__ void colfwd_body(const InD& in, uint32_t* __restrict__ out, const BigD& bt, const Ptab& pt,
+                                            int j0) {
+  using C = ColCfg<LOGR, LOGW>;
   constexpr int K = ColGroups<LOGR>::K;
   constexpr int G = C::GL;
   constexpr int LP = C::LOGW - 1;
   extern __shared__ uint32_t sm[];
   const int tid = threadIdx.x, logC = bt.logC;
-  const int j0 = blockIdx.x << C::LOGW;
   const Fp f = pt.f;
   // zero-padded input (count <= N/2, every conv operand): the lower half of
   // each column is never loaded and the first level needs no additions
   const bool half = K > 1 && in.ptr != nullptr && in.count != 0 && in.count <= (1u << (LOGR - 1 + logC));
   if (half) {
-    col_tile_load<LOGR, true>(sm, in.ptr, in.count, j0, logC, tid);
+    col_tile_load<LOGR, LOGW, true>(sm, in.ptr, in.count, j0, logC, tid);
     __syncthreads();
-    col_fwd_groups<LOGR, 0, true>(sm, pt, in.reduce != 0, tid);
+    col_fwd_groups<LOGR, LOGW, 0, true>(sm, pt, in.reduce != 0, tid);
   } else {
-    col_tile_load<LOGR>(sm, in.ptr, in.count, j0, logC, tid);
+    col_tile_load<LOGR, LOGW>(sm, in.ptr, in.count, j0, logC, tid);
     __syncthreads();
-    col_fwd_groups<LOGR, 0>(sm, pt, in.reduce != 0, tid);
+    col_fwd_groups<LOGR, LOGW, 0>(sm, pt, in.reduce != 0, tid);
   }
   // last group: shared -> registers -> Bailey twiddle -> global (64-bit stores)
   constexpr int NINST = C::TE >> (G + 1);
@@ -1045,24 +1049,53 @@ __device__ __forceinline__ void colfwd_body(const InD& in, uint32_t* __restrict_
   }
 }
 
-template <int LOGR>
-__global__ void __launch_bounds__(256, 3) k_colfwd_t(ColOps ops, BigD bt, Ptab pt) {
-  const InD in = blockIdx.y == 0 ? ops.in[0] : (blockIdx.y == 1 ? ops.in[1] : ops.in[2]);
-  uint32_t* out = blockIdx.y == 0 ? ops.out[0] : (blockIdx.y == 1 ? ops.out[1] : ops.out[2]);
-  colfwd_body<LOGR>(in, out, bt, pt);
+// Tiles of a column pass.  The first `nbig` tiles of every operand are 2^LW1
+// columns wide, the remaining `nsmall` are 2^LW2 wide; blocks run through the
+// wide tiles of all operands first (operand-major), then the narrow ones.  With
+// the wide tiles filling whole waves of resident CTAs, the grid ends on narrow
+// tiles instead of a partial wave of wide ones (148 SMs never divide a power of
+// two).  LW1 == LW2: every tile is wide (nsmall = 0).
+struct ColSplit {
+  int nbig, nsmall, nops;
+};
+__device__ __forceinline__ bool col_tile_of(const ColSplit& sp, int lw1, int lw2, int& op, int& j0) {
+  int b = (int)blockIdx.x;
+  const int nb = sp.nbig * sp.nops;
+  if (b < nb) {
+    op = b / sp.nbig;
+    j0 = (b - op * sp.nbig) << lw1;
+    return true;
+  }
+  b -= nb;
+  op = b / sp.nsmall;
+  j0 = (sp.nbig << lw1) + ((b - op * sp.nsmall) << lw2);
+  return false;
 }
 
-template <int LOGR, bool PLAIN>
+template <int LOGR, int LW1, int LW2>
+__global__ void __launch_bounds__(256, 3) k_colfwd_t(ColOps ops, BigD bt, Ptab pt, ColSplit sp) {
+  int op, j0;
+  const bool wide = col_tile_of(sp, LW1, LW2, op, j0);
+  const InD in = op == 0 ? ops.in[0] : (op == 1 ? ops.in[1] : ops.in[2]);
+  uint32_t* out = op == 0 ? ops.out[0] : (op == 1 ? ops.out[1] : ops.out[2]);
+  if constexpr (LW1 == LW2) {
+    colfwd_body<LOGR, LW1>(in, out, bt, pt, j0);
+  } else {
+    if (wide) colfwd_body<LOGR, LW1>(in, out, bt, pt, j0);
+    else colfwd_body<LOGR, LW2>(in, out, bt, pt, j0);
+  }
+}
+
+template <int LOGR, int LOGW, bool PLAIN>
 __device__ __forceinline__ void colinv_body(const uint32_t* __restrict__ in, const BigD& bt, const Ptab& pt,
-                                            const EpiD& epi) {
-  using C = ColCfg<LOGR>;
+                                            const EpiD& epi, int j0) {
+  using C = ColCfg<LOGR, LOGW>;
   constexpr int K = ColGroups<LOGR>::K;
   constexpr int LP = C::LOGW - 1;
   extern __shared__ uint32_t sm[];
   const int tid = threadIdx.x, logC = bt.logC;
-  const int j0 = blockIdx.x << C::LOGW;
   const Fp f = pt.f;
-  col_tile_load<LOGR>(sm, in, 0xffffffffu, j0, logC, tid);
+  col_tile_load<LOGR, LOGW>(sm, in, 0xffffffffu, j0, logC, tid);
   __syncthreads();
   // first: the smallest blocks (Bailey twiddle on the way in), in place
   {
@@ -1099,7 +1132,7 @@ __device__ __forceinline__ void colinv_body(const uint32_t* __restrict__ in, con
   }
   if constexpr (K > 1) {
     __syncthreads();
-    col_inv_groups<LOGR, K - 2>(sm, pt, tid);
+    col_inv_groups<LOGR, LOGW, K - 2>(sm, pt, tid);
     // last: the full column blocks, shared -> registers -> epilogue (global)
     constexpr int G = ColGroups<LOGR>::size(0);
     constexpr int S = LOGR - G;
@@ -1122,37 +1155,41 @@ __device__ __forceinline__ void colinv_body(const uint32_t* __restrict__ in, con
   }
 }
 
-template <int LOGR, bool PLAIN>
-__global__ void __launch_bounds__(256, 3) k_colinv_t(const uint32_t* __restrict__ in, BigD bt, Ptab pt, EpiD epi) {
-  colinv_body<LOGR, PLAIN>(in, bt, pt, epi);
+template <int LOGR, bool PLAIN, int LW1, int LW2>
+__global__ void __launch_bounds__(256, 3) k_colinv_t(const uint32_t* __restrict__ in, BigD bt, Ptab pt, EpiD epi,
+                                                     ColSplit sp) {
+  int op, j0;
+  const bool wide = col_tile_of(sp, LW1, LW2, op, j0);
+  if constexpr (LW1 == LW2) {
+    colinv_body<LOGR, LW1, PLAIN>(in, bt, pt, epi, j0);
+  } else {
+    if (wide) colinv_body<LOGR, LW1, PLAIN>(in, bt, pt, epi, j0);
+    else colinv_body<LOGR, LW2, PLAIN>(in, bt, pt, epi, j0);
+  }
 }
 
-template <int LOGR>
-int col_smem_bytes() { return ColCfg<LOGR>::SMEM_WORDS * 4; }
+using ColFwdFn = void (*)(ColOps, BigD, Ptab, ColSplit);
+using ColInvFn = void (*)(const uint32_t*, BigD, Ptab, EpiD, ColSplit);
 
-using ColFwdFn = void (*)(ColOps, BigD, Ptab);
-using ColInvFn = void (*)(const uint32_t*, BigD, Ptab, EpiD);
+// One compiled column-pass shape: R = 2^LOGR points per column, wide tiles of
+// 2^LW1 columns, narrow tiles of 2^LW2 (LW1 == LW2: a single width).
+template <int LOGR, int LW1, int LW2>
+struct ColK {};
 
-template <int... L>
-struct ColTable {
-  static ColFwdFn fwd(int logR) {
+template <class... K>
+struct ColTable;
+template <int... R, int... A, int... B>
+struct ColTable<ColK<R, A, B>...> {
+  static ColFwdFn fwd(int logR, int lw1, int lw2) {
     ColFwdFn r = nullptr;
-    ((logR == L ? (r = k_colfwd_t<L>, 0) : 0), ...);
+    ((logR == R && lw1 == A && lw2 == B ? (r = k_colfwd_t<R, A, B>, 0) : 0), ...);
     return r;
   }
-  static ColInvFn inv(int logR, bool plain) {
+  static ColInvFn inv(int logR, int lw1, int lw2, bool plain) {
     ColInvFn r = nullptr;
-    ((logR == L ? (r = plain ? k_colinv_t<L, true> : k_colinv_t<L, false>, 0) : 0), ...);
-    return r;
-  }
-  static int words(int logR) {
-    int r = 0;
-    ((logR == L ? (r = ColCfg<L>::SMEM_WORDS, 0) : 0), ...);
-    return r;
-  }
-  static int logw(int logR) {
-    int r = 0;
-    ((logR == L ? (r = ColCfg<L>::LOGW, 0) : 0), ...);
+    ((logR == R && lw1 == A && lw2 == B ? (r = plain ? k_colinv_t<R, true, A, B> : k_colinv_t<R, false, A, B>, 0)
+                                        : 0),
+     ...);
     return r;
   }
   static cudaError_t init() {
@@ -1161,13 +1198,23 @@ struct ColTable {
       const cudaError_t r = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
       if (r != cudaSuccess) e = r;
     };
-    (set((const void*)k_colfwd_t<L>, ColCfg<L>::SMEM_WORDS * 4), ...);
-    (set((const void*)k_colinv_t<L, true>, ColCfg<L>::SMEM_WORDS * 4), ...);
-    (set((const void*)k_colinv_t<L, false>, ColCfg<L>::SMEM_WORDS * 4), ...);
+    (set((const void*)k_colfwd_t<R, A, B>, ColCfg<R, A>::SMEM_WORDS * 4), ...);
+    (set((const void*)k_colinv_t<R, true, A, B>, ColCfg<R, A>::SMEM_WORDS * 4), ...);
+    (set((const void*)k_colinv_t<R, false, A, B>, ColCfg<R, A>::SMEM_WORDS * 4), ...);
     return e;
   }
 };
-using Cols = ColTable<2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12>;
+template <int L>
+using ColD = ColK<L, col_logw(L), col_logw(L)>;
+// Default widths for every R; for R = 2^9 .. 2^12 (transforms of 2^21 .. 2^24
+// points, whose grids span several waves) also half-width tiles and the split
+// grids the tuner chooses from.  Narrow tiles keep 2^LW >= 4 columns below
+// R = 2^12: at two columns the swizzle leaves 4-way bank conflicts there.
+using Cols = ColTable<ColD<2>, ColD<3>, ColD<4>, ColD<5>, ColD<6>, ColD<7>, ColD<8>,
+                      ColD<9>, ColK<9, 3, 3>, ColK<9, 4, 3>, ColK<9, 4, 2>,
+                      ColD<10>, ColK<10, 2, 2>, ColK<10, 3, 2>,
+                      ColD<11>, ColK<11, 2, 2>, ColK<11, 3, 2>,
+                      ColD<12>, ColK<12, 1, 1>, ColK<12, 2, 1>>;
 
 }  // namespace
 
@@ -1175,8 +1222,53 @@ namespace fpx {
 
 cudaError_t kernels_fast_init() { return Cols::init(); }
 
+int col_shape_candidates(int logR, bool inverse, ColShape* out, int max) {
+  const int d = col_logw(logR);
+  int n = 0;
+  auto add = [&](int lw1, int lw2) {
+    if (n >= max) return;
+    ColShape sh;
+    sh.lw1 = lw1;
+    sh.lw2 = lw2;
+    sh.split = lw2 != lw1;
+    if (sh.split) {
+      const void* fn = inverse ? (const void*)Cols::inv(logR, lw1, lw2, true) : (const void*)Cols::fwd(logR, lw1, lw2);
+      int dev = 0, sms = 0, per_sm = 0;
+      if (cudaGetDevice(&dev) != cudaSuccess ||
+          cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+          cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, 256, (size_t(4) << (logR + lw1))) !=
+              cudaSuccess) {
+        cudaGetLastError();
+        return;
+      }
+      sh.slots = sms * per_sm;
+    }
+    out[n++] = sh;
+  };
+  add(d, d);
+  for (int a = d; a >= 1; --a)
+    for (int b = a; b >= 1; --b)
+      if ((a != d || b != d) && Cols::fwd(logR, a, b)) add(a, b);
+  return n;
+}
 
-
+namespace {
+// Tiles per operand of one column pass with shape `sh` (see ColSplit).
+ColSplit col_split(const BigTables& bt, const ColShape& sh, int nops, int& lw1, int& lw2) {
+  lw1 = sh.lw1 ? sh.lw1 : col_logw(bt.logR);
+  lw2 = sh.lw1 && sh.split ? sh.lw2 : lw1;
+  const int tiles = 1 << (bt.logC - lw1);
+  ColSplit sp{tiles, 0, nops};
+  if (lw2 < lw1 && sh.slots > 0) {
+    const int nbig = (nops * tiles / sh.slots) * sh.slots / nops;  // whole waves of wide tiles
+    if (nbig > 0 && nbig < tiles) {
+      sp.nbig = nbig;
+      sp.nsmall = (tiles - nbig) << (lw1 - lw2);
+    }
+  }
+  return sp;
+}
+}  // namespace
 
 cudaError_t launch_colfwd(const PrimeTables& pt, const BigTables& bt, int nops, const InOp* in,
                                uint32_t* const* out, cudaStream_t s) {
@@ -1185,23 +1277,28 @@ cudaError_t launch_colfwd(const PrimeTables& pt, const BigTables& bt, int nops, 
     ops.in[i] = dev_in(in[i]);
     ops.out[i] = out[i];
   }
-  BigD d{bt.logR, bt.logC, Cols::logw(bt.logR), reinterpret_cast<const uint2*>(bt.lo_fwd),
+  const ColShape sh = bt.shapes ? (nops == 1 ? bt.shapes->fwd1 : bt.shapes->fwd2) : ColShape{};
+  int lw1, lw2;
+  const ColSplit sp = col_split(bt, sh, nops, lw1, lw2);
+  ColFwdFn fn = Cols::fwd(bt.logR, lw1, lw2);
+  if (!fn || lw1 > bt.logC || nops < 1 || nops > 3) return cudaErrorInvalidValue;
+  BigD d{bt.logR, bt.logC, lw1, reinterpret_cast<const uint2*>(bt.lo_fwd),
          reinterpret_cast<const uint2*>(bt.mid_fwd), reinterpret_cast<const uint2*>(bt.hi_fwd)};
-  ColFwdFn fn = Cols::fwd(bt.logR);
-  if (!fn || d.logW > bt.logC) return cudaErrorInvalidValue;
-  dim3 grid(1u << (bt.logC - d.logW), (unsigned)nops);
-  fn<<<grid, 256, Cols::words(bt.logR) * 4, s>>>(ops, d, dev_tab(pt));
+  fn<<<(unsigned)(nops * (sp.nbig + sp.nsmall)), 256, size_t(4) << (bt.logR + lw1), s>>>(ops, d, dev_tab(pt), sp);
   return cudaGetLastError();
 }
 
 cudaError_t launch_colinv(const PrimeTables& pt, const BigTables& bt, const uint32_t* in, int mont_scaled,
                                const Epi& epi, cudaStream_t s) {
-  BigD d{bt.logR, bt.logC, Cols::logw(bt.logR),
-         reinterpret_cast<const uint2*>(mont_scaled ? bt.lo_inv_r : bt.lo_inv),
+  const ColShape sh = bt.shapes ? bt.shapes->inv : ColShape{};
+  int lw1, lw2;
+  const ColSplit sp = col_split(bt, sh, 1, lw1, lw2);
+  ColInvFn fn = Cols::inv(bt.logR, lw1, lw2, host_epi_plain(epi));
+  if (!fn || lw1 > bt.logC) return cudaErrorInvalidValue;
+  BigD d{bt.logR, bt.logC, lw1, reinterpret_cast<const uint2*>(mont_scaled ? bt.lo_inv_r : bt.lo_inv),
          reinterpret_cast<const uint2*>(bt.mid_inv), reinterpret_cast<const uint2*>(bt.hi_inv)};
-  ColInvFn fn = Cols::inv(bt.logR, host_epi_plain(epi));
-  if (!fn || d.logW > bt.logC) return cudaErrorInvalidValue;
-  fn<<<1u << (bt.logC - d.logW), 256, Cols::words(bt.logR) * 4, s>>>(in, d, dev_tab(pt), dev_epi(epi));
+  fn<<<(unsigned)(sp.nbig + sp.nsmall), 256, size_t(4) << (bt.logR + lw1), s>>>(in, d, dev_tab(pt), dev_epi(epi),
+                                                                                 sp);
   return cudaGetLastError();
 }
 
@@ -1265,7 +1362,7 @@ template <int LOGR>
 __global__ void __launch_bounds__(256, 3) k_colfwd_b(const BigJobB* __restrict__ jobs) {
   const BigJobB& j = jobs[blockIdx.z];
   if ((int)blockIdx.y >= j.nops) return;
-  colfwd_body<LOGR>(j.in[blockIdx.y], j.t[blockIdx.y], j.bf, j.pt);
+  colfwd_body<LOGR, col_logw(LOGR)>(j.in[blockIdx.y], j.t[blockIdx.y], j.bf, j.pt, blockIdx.x << col_logw(LOGR));
 }
 
 __global__ void __launch_bounds__(256, 3) k_rows12_b(const BigJobB* __restrict__ jobs) {
@@ -1276,7 +1373,7 @@ __global__ void __launch_bounds__(256, 3) k_rows12_b(const BigJobB* __restrict__
 template <int LOGR, bool PLAIN>
 __global__ void __launch_bounds__(256, 3) k_colinv_b(const BigJobB* __restrict__ jobs) {
   const BigJobB& j = jobs[blockIdx.y];
-  colinv_body<LOGR, PLAIN>(j.t[0], j.bi, j.pt, j.epi);
+  colinv_body<LOGR, col_logw(LOGR), PLAIN>(j.t[0], j.bi, j.pt, j.epi, blockIdx.x << col_logw(LOGR));
 }
 
 // Batched direct products and Garner reconstructions: block b covers outputs
@@ -1453,9 +1550,9 @@ cudaError_t launch_batch(const BatchPlan& b, void* host_staging, void* dev_desc,
         const BigTables& bt = *x.bt;
         BigJobB j{};
         j.pt = pt;
-        j.bf = BigD{bt.logR, bt.logC, Cols::logw(bt.logR), reinterpret_cast<const uint2*>(bt.lo_fwd),
+        j.bf = BigD{bt.logR, bt.logC, col_logw(bt.logR), reinterpret_cast<const uint2*>(bt.lo_fwd),
                     reinterpret_cast<const uint2*>(bt.mid_fwd), reinterpret_cast<const uint2*>(bt.hi_fwd)};
-        j.bi = BigD{bt.logR, bt.logC, Cols::logw(bt.logR),
+        j.bi = BigD{bt.logR, bt.logC, col_logw(bt.logR),
                     reinterpret_cast<const uint2*>(x.ymode != 0 ? bt.lo_inv_r : bt.lo_inv),
                     reinterpret_cast<const uint2*>(bt.mid_inv), reinterpret_cast<const uint2*>(bt.hi_inv)};
         j.in[0] = dev_in(x.x);
@@ -1561,8 +1658,8 @@ cudaError_t launch_batch(const BatchPlan& b, void* host_staging, void* dev_desc,
       continue;
     }
     const int logC = 12, logR = g.logN - logC;
-    const int logW = Cols::logw(logR);
-    const int smem = Cols::words(logR) * 4;
+    const int logW = col_logw(logR);
+    const int smem = 4 << (logR + logW);
     for (size_t k = 0; k < (size_t)g.count; k += kMaxY) {
       const BigJobB* jobs = reinterpret_cast<const BigJobB*>(d + g.off) + k;
       const unsigned cnt = (unsigned)std::min(kMaxY, (size_t)g.count - k);

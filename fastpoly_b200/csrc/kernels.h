@@ -25,8 +25,20 @@ struct PrimeTables {
 // Per-(prime, N) tables for the two-pass (four-step) decomposition.
 // The Bailey twiddle w_N^e (e < N) is lo[e & 255] * mid[(e >> 8) & 255] *
 // hi[e >> 16]: three small tables instead of one of N entries.
+// Tile shape of one column pass: wide tiles of 2^lw1 columns; with split != 0
+// the columns past the last full wave of wide tiles (`slots` resident CTAs on
+// the device) go in narrow tiles of 2^lw2 columns.  lw1 == 0: the default
+// width, no split.  Every shape computes the same values.
+struct ColShape {
+  int lw1 = 0, lw2 = 0, split = 0, slots = 0;
+};
+struct ColShapes {
+  ColShape fwd1, fwd2, inv;  // forward pass of one operand, of two or three; inverse pass
+};
+
 struct BigTables {
   int logN = 0, logR = 0, logC = 0;
+  const ColShapes* shapes = nullptr;  // chosen column-pass tile shapes; nullptr: defaults
   const Tw2* lo_fwd = nullptr;     // w_N^y, y < 256
   const Tw2* mid_fwd = nullptr;    // w_N^(256 y), y < 256
   const Tw2* hi_fwd = nullptr;     // w_N^(65536 y), y < max(1, N / 65536)
@@ -77,6 +89,11 @@ struct SmallJob {
 cudaError_t launch_small(const PrimeTables& pt, int logN, const SmallJob& job, cudaStream_t s);
 
 // -------- two-pass transforms, N = R*C > 2^13 ----------------------------------
+// Compiled column-pass shapes for R = 2^logR, the default first; `inverse`
+// selects the kernel whose occupancy gives `slots`.  Returns how many were
+// written to out (at most max).
+int col_shape_candidates(int logR, bool inverse, ColShape* out, int max);
+
 // Pass A forward: column DIF over up to 3 operands, each to its own N-word buffer.
 cudaError_t launch_colfwd(const PrimeTables& pt, const BigTables& bt, int nops, const InOp* in,
                           uint32_t* const* out, cudaStream_t s);

@@ -81,6 +81,23 @@ uint64_t fpx_launch_count(fpx_ctx* ctx);
  * compute denominator of the transform roofline.  No context needed. */
 int fpx_measure_imad_rate(int device, double* per_second);
 
+/* ---- column-pass tile shapes (no counterpart in the reference, whose NTT plan
+ *      has one fixed schedule per size) ------------------------------------------
+ * A transform of N = 2^log_n > 2^13 points runs two column passes over tiles of
+ * 2^lw1 columns; with split != 0 the columns past the last full wave of wide
+ * tiles go in narrow tiles of 2^lw2 columns.  The shape is chosen per process,
+ * device and size by timing every compiled candidate on first use (environment:
+ * FPX_AUTOTUNE=0 keeps the defaults, FPX_AUTOTUNE_CACHE=<file> persists the
+ * choices).  kind: 0 forward pass of one operand, 1 of two or three, 2 inverse.
+ * Every shape computes the same values; _set (for tests and experiments) takes
+ * effect for every context of the process on that device. */
+typedef struct fpx_col_shape {
+  int lw1, lw2, split;
+} fpx_col_shape;
+int fpx_col_shape_candidates(fpx_ctx* ctx, int log_n, int kind, fpx_col_shape* out, int max, int* count);
+int fpx_col_shape_get(fpx_ctx* ctx, int log_n, int kind, fpx_col_shape* out);
+int fpx_col_shape_set(fpx_ctx* ctx, int log_n, int kind, const fpx_col_shape* shape);
+
 /* ---- transforms (NttPlan<M>::forward / inverse, ntt.hpp:140-192) -------------
  * In place, n a power of two with 2 <= n <= 2^v2(p-1), p < 2^30 odd.  forward
  * leaves the spectrum in the reference's bit-reversed order; inverse takes that
