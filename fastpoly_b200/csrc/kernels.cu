@@ -19,7 +19,9 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdlib>
 #include <cstring>
+#include <utility>
 #include <vector>
 
 #include "field.cuh"
@@ -29,6 +31,61 @@
 using namespace fpx_dev;
 
 namespace {
+
+// Programmatic dependent launch.  Every kernel of this file is launched with
+// programmatic stream serialization (pdl_launch), so the GPU may schedule it
+// while the stream's previous kernel is still running: its launch latency
+// hides behind the previous kernel's last wave.  The kernel lets its own
+// dependents launch at once, then waits until the previous kernel has
+// completed and its writes are visible before touching global memory; nothing
+// before pdl_enter() reads or writes global memory.
+__device__ __forceinline__ void pdl_enter() {
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+}
+
+// Which launches take the attribute, by grid size in CTAs: measured on B200,
+// back-to-back products gain 15-25 % with it at grids of up to 32 CTAs
+// (transforms up to 2^17 points) and 5-13 % at grids of two waves and more
+// (2^21 points and up), but lose 10-20 % at the grids in between (2^18-2^20
+// points: 64-256 CTAs), so those launch without it.  FPX_PDL=0 in the
+// environment turns it off everywhere; FPX_PDL_SMALL / FPX_PDL_LARGE move the
+// two bounds (for measurements).
+struct PdlPolicy {
+  bool on = true;
+  unsigned small = 32, large = 296;
+};
+const PdlPolicy& pdl_policy() {
+  static const PdlPolicy pol = [] {
+    PdlPolicy r;
+    const char* e = std::getenv("FPX_PDL");
+    r.on = !(e && e[0] == '0');
+    if (const char* v = std::getenv("FPX_PDL_SMALL")) r.small = (unsigned)std::strtoul(v, nullptr, 10);
+    if (const char* v = std::getenv("FPX_PDL_LARGE")) r.large = (unsigned)std::strtoul(v, nullptr, 10);
+    return r;
+  }();
+  return pol;
+}
+bool pdl_for(dim3 grid) {
+  const PdlPolicy& pol = pdl_policy();
+  const unsigned ctas = grid.x * grid.y * grid.z;
+  return pol.on && (ctas <= pol.small || ctas >= pol.large);
+}
+
+template <typename... KA, typename... A>
+cudaError_t pdl_launch(void (*k)(KA...), dim3 grid, dim3 block, size_t smem, cudaStream_t s, A&&... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = pdl_for(grid) ? 1 : 0;
+  return cudaLaunchKernelEx(&cfg, k, std::forward<A>(args)...);
+}
 
 struct Ptab {
   const uint2* fwd;
@@ -171,7 +228,7 @@ __device__ __forceinline__ void small_body(const SmallD& job, const Ptab& pt, in
   for (uint32_t i = job.epi.lo + tid; i < hi; i += nt) epi_store(job.epi, i, X[pad(i)], f);
 }
 
-__global__ void __launch_bounds__(512) k_small(SmallD job, Ptab pt, int logN) { small_body(job, pt, logN); }
+__global__ void __launch_bounds__(512) k_small(SmallD job, Ptab pt, int logN) { pdl_enter(); small_body(job, pt, logN); }
 
 // ---------------------------------------------------------------------------
 // Pass A forward (columns).
@@ -201,6 +258,7 @@ __device__ __forceinline__ uint32_t bailey_mul(uint32_t x, uint32_t ex, const Bi
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(512) k_rows(uint32_t* x, const uint32_t* y, int ymode, uint32_t* y_spec_out,
                                                int forward, int inverse, int logC, Ptab pt) {
+  pdl_enter();
   extern __shared__ uint32_t sm[];
   const int tid = threadIdx.x, nt = blockDim.x, C = 1 << logC;
   uint32_t* X = sm;
@@ -243,6 +301,7 @@ __global__ void __launch_bounds__(512) k_rows(uint32_t* x, const uint32_t* y, in
 // Elementwise kernels.
 // ---------------------------------------------------------------------------
 __global__ void k_pointwise(Fp f, uint32_t* a, const uint32_t* b, size_t n) {
+  pdl_enter();
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
     a[i] = mont(a[i], b[i], f);
 }
@@ -296,18 +355,22 @@ __device__ __forceinline__ void garner_body(const GarnerC& g, int primes, const 
 
 __global__ void k_garner(GarnerC g, int primes, const uint32_t* c1, const uint32_t* c2, const uint32_t* c3,
                          uint32_t* out, size_t n, int accumulate) {
+  pdl_enter();
   garner_body(g, primes, c1, c2, c3, out, n, accumulate);
 }
 
 __global__ void k_from_mont(Fp f, const uint32_t* in, uint32_t* out, size_t n) {
+  pdl_enter();
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
     out[i] = red(mont(in[i], 1u, f), f.p);
 }
 __global__ void k_bits2(const uint32_t* in, uint32_t* out, size_t n) {
+  pdl_enter();
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
     out[i] = in[i] & 1u;
 }
 __global__ void k_scale(uint32_t p, const uint32_t* in, uint32_t* out, size_t n, uint2 c) {
+  pdl_enter();
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
     out[i] = redc_any(shoup(in[i], c, p), p);
 }
@@ -324,6 +387,7 @@ __device__ uint32_t mont_pow(uint32_t base_m, uint32_t e, uint32_t one_m, const 
 
 // tab[i] = (1/i) * 2^32 mod p for 1 <= i <= n (i < p), tab[0] = 0.
 __global__ void k_inv_table(Fp f, uint2 r_sh, uint2 r2_sh, uint32_t* tab, size_t n) {
+  pdl_enter();
   const uint32_t one_m = red(shoup(1u, r_sh, f.p), f.p);
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i <= n; i += (size_t)gridDim.x * blockDim.x) {
     if (i == 0) { tab[0] = 0; continue; }
@@ -333,6 +397,7 @@ __global__ void k_inv_table(Fp f, uint2 r_sh, uint2 r2_sh, uint32_t* tab, size_t
 }
 
 __global__ void k_derivative(Fp f, uint32_t q1, uint2 r_sh, const uint32_t* a, uint32_t* r, size_t cnt1) {
+  pdl_enter();
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < cnt1; i += (size_t)gridDim.x * blockDim.x) {
     const uint32_t k = reduce_any((uint32_t)(i + 1), q1, f);
     const uint32_t t = red(mont(a[i + 1], k, f), f.p);   // a*k/R
@@ -380,6 +445,7 @@ __device__ __forceinline__ void direct_body(uint32_t p, const Fp& f, const uint3
 
 __global__ void k_direct(uint32_t p, Fp f, uint2 r_sh, const uint32_t* a, int la, const uint32_t* b, size_t lb,
                          size_t off, size_t cnt, uint32_t* out, int accumulate) {
+  pdl_enter();
   direct_body(p, f, a, la, b, lb, off, cnt, out, accumulate);
 }
 
@@ -433,7 +499,7 @@ cudaError_t launch_small(const PrimeTables& pt, int logN, const SmallJob& job, c
   if (nt < 32) nt = 32;
   if (nt > 512) nt = 512;
   const size_t smem = (size_t)2 * padded_words(N) * 4;
-  k_small<<<1, nt, smem, s>>>(d, dev_tab(pt), logN);
+  (void)pdl_launch(k_small, 1, nt, smem, s, d, dev_tab(pt), logN);
   return cudaGetLastError();
 }
 
@@ -442,13 +508,13 @@ cudaError_t launch_rows_generic(const PrimeTables& pt, const BigTables& bt, uint
   const int C = 1 << bt.logC;
   const size_t smem = (size_t)2 * padded_words(C) * 4;
   const int nt = C / 16 > 512 ? 512 : C / 16;
-  k_rows<<<1u << bt.logR, nt, smem, s>>>(x, y, ymode, y_spec_out, forward, inverse, bt.logC, dev_tab(pt));
+  (void)pdl_launch(k_rows, 1u << bt.logR, nt, smem, s, x, y, ymode, y_spec_out, forward, inverse, bt.logC, dev_tab(pt));
   return cudaGetLastError();
 }
 
 
 cudaError_t launch_pointwise(uint32_t p, uint32_t* a, const uint32_t* b, size_t n, cudaStream_t s) {
-  k_pointwise<<<grid_for(n, 256), 256, 0, s>>>(make_fp(p), a, b, n);
+  (void)pdl_launch(k_pointwise, grid_for(n, 256), 256, 0, s, make_fp(p), a, b, n);
   return cudaGetLastError();
 }
 
@@ -471,34 +537,34 @@ cudaError_t launch_garner(uint32_t target, int primes, const uint32_t* c1, const
   g.t_q1 = (uint32_t)((((uint64_t)1) << 32) / target);
   g.p1_t = shoup_const((uint32_t)(P1 % target), target);
   g.p12_t = shoup_const((uint32_t)((P1 * P2) % target), target);
-  k_garner<<<grid_for(n, 256), 256, 0, s>>>(g, primes, c1, c2, c3, out, n, accumulate);
+  (void)pdl_launch(k_garner, grid_for(n, 256), 256, 0, s, g, primes, c1, c2, c3, out, n, accumulate);
   return cudaGetLastError();
 }
 
 cudaError_t launch_from_mont(uint32_t p, const uint32_t* in, uint32_t* out, size_t n, cudaStream_t s) {
   if (n == 0) return cudaSuccess;
-  if (p == 2) k_bits2<<<grid_for(n, 256), 256, 0, s>>>(in, out, n);
-  else k_from_mont<<<grid_for(n, 256), 256, 0, s>>>(make_fp(p), in, out, n);
+  if (p == 2) (void)pdl_launch(k_bits2, grid_for(n, 256), 256, 0, s, in, out, n);
+  else (void)pdl_launch(k_from_mont, grid_for(n, 256), 256, 0, s, make_fp(p), in, out, n);
   return cudaGetLastError();
 }
 
 cudaError_t launch_to_mont(uint32_t p, const uint32_t* in, uint32_t* out, size_t n, cudaStream_t s) {
   if (n == 0) return cudaSuccess;
-  if (p == 2) k_bits2<<<grid_for(n, 256), 256, 0, s>>>(in, out, n);
-  else k_scale<<<grid_for(n, 256), 256, 0, s>>>(p, in, out, n, shoup_const((uint32_t)((((uint64_t)1) << 32) % p), p));
+  if (p == 2) (void)pdl_launch(k_bits2, grid_for(n, 256), 256, 0, s, in, out, n);
+  else (void)pdl_launch(k_scale, grid_for(n, 256), 256, 0, s, p, in, out, n, shoup_const((uint32_t)((((uint64_t)1) << 32) % p), p));
   return cudaGetLastError();
 }
 
 cudaError_t launch_scale(uint32_t p, const uint32_t* a, uint32_t* out, size_t n, uint32_t c, cudaStream_t s) {
   if (n == 0) return cudaSuccess;
-  k_scale<<<grid_for(n, 256), 256, 0, s>>>(p, a, out, n, shoup_const(c % p, p));
+  (void)pdl_launch(k_scale, grid_for(n, 256), 256, 0, s, p, a, out, n, shoup_const(c % p, p));
   return cudaGetLastError();
 }
 
 cudaError_t launch_inv_table(uint32_t p, uint32_t* tab, size_t n, cudaStream_t s) {
   const uint32_t r = (uint32_t)((((uint64_t)1) << 32) % p);
   const uint32_t r2 = (uint32_t)((uint64_t)r * r % p);
-  k_inv_table<<<grid_for(n + 1, 256), 256, 0, s>>>(make_fp(p), shoup_const(r, p), shoup_const(r2, p), tab, n);
+  (void)pdl_launch(k_inv_table, grid_for(n + 1, 256), 256, 0, s, make_fp(p), shoup_const(r, p), shoup_const(r2, p), tab, n);
   return cudaGetLastError();
 }
 
@@ -506,7 +572,7 @@ cudaError_t launch_derivative(uint32_t p, const uint32_t* a, uint32_t* r, size_t
   if (cnt <= 1) return cudaSuccess;
   const uint32_t rr = (uint32_t)((((uint64_t)1) << 32) % p);
   const uint32_t q1 = (uint32_t)((((uint64_t)1) << 32) / p);
-  k_derivative<<<grid_for(cnt - 1, 256), 256, 0, s>>>(make_fp(p), q1, shoup_const(rr, p), a, r, cnt - 1);
+  (void)pdl_launch(k_derivative, grid_for(cnt - 1, 256), 256, 0, s, make_fp(p), q1, shoup_const(rr, p), a, r, cnt - 1);
   return cudaGetLastError();
 }
 
@@ -515,7 +581,7 @@ cudaError_t launch_direct_product(uint32_t p, const uint32_t* a, size_t la, cons
   if (cnt == 0) return cudaSuccess;
   const Fp f = (p & 1u) ? make_fp(p) : Fp{p, 2 * p, 1};
   const uint32_t r = (uint32_t)((((uint64_t)1) << 32) % p);
-  k_direct<<<grid_for(cnt, 256), 256, 0, s>>>(p, f, shoup_const(r, p), a, (int)la, b, lb, off, cnt, out, accumulate);
+  (void)pdl_launch(k_direct, grid_for(cnt, 256), 256, 0, s, p, f, shoup_const(r, p), a, (int)la, b, lb, off, cnt, out, accumulate);
   return cudaGetLastError();
 }
 
@@ -596,6 +662,7 @@ __device__ __forceinline__ void seed_body(int kind, uint32_t p, const uint32_t* 
 }
 
 __global__ void k_seed(int kind, uint32_t p, const uint32_t* a, size_t la, uint32_t* out, int n, uint32_t r0) {
+  pdl_enter();
   seed_body(kind, p, a, la, out, n, r0);
 }
 
@@ -613,6 +680,7 @@ struct ExpPrepB {
   uint32_t out0;
 };
 __global__ void k_exp_prep_b(const ExpPrepB* __restrict__ jobs) {
+  pdl_enter();
   const ExpPrepB& j = jobs[blockIdx.y];
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < j.n; i += (size_t)gridDim.x * blockDim.x) {
     j.out[i] = i == 0 ? j.out0 : 0u;
@@ -629,6 +697,7 @@ __global__ void k_exp_prep_b(const ExpPrepB* __restrict__ jobs) {
 // single address).  Mode 1 reports 0 both for "index 0" and "none"; the caller
 // tells them apart.
 __global__ void __launch_bounds__(256) k_find_nonzero(const uint32_t* a, size_t n, int mode, unsigned long long* res) {
+  pdl_enter();
   unsigned long long hit = 0;  // index + 1, 0 = none
   const size_t stride = (size_t)gridDim.x * blockDim.x;
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += stride) {
@@ -654,12 +723,14 @@ __global__ void __launch_bounds__(256) k_find_nonzero(const uint32_t* a, size_t 
 }
 
 __global__ void k_reverse(const uint32_t* a, uint32_t* r, size_t n) {
+  pdl_enter();
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
     r[i] = a[n - 1 - i];
 }
 
 // r[i] = a[i] - b[i] (mod p), b missing beyond lb.
 __global__ void k_sub(uint32_t p, const uint32_t* a, const uint32_t* b, size_t lb, uint32_t* r, size_t n) {
+  pdl_enter();
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
     const uint32_t x = a[i], y = i < lb ? b[i] : 0u;
     r[i] = x >= y ? x - y : x + (p - y);
@@ -668,6 +739,7 @@ __global__ void k_sub(uint32_t p, const uint32_t* a, const uint32_t* b, size_t l
 
 // Characteristic two square root (square_root.hpp:14-23): out[i/2] = a[i] for even i.
 __global__ void k_sqrt_char2(const uint32_t* a, size_t cnt, uint32_t* out, unsigned long long* odd_flag) {
+  pdl_enter();
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < cnt; i += (size_t)gridDim.x * blockDim.x) {
     const uint32_t v = a[i] & 1u;
     if (i & 1) { if (v) atomicMax(odd_flag, 1ull); }
@@ -677,6 +749,7 @@ __global__ void k_sqrt_char2(const uint32_t* a, size_t cnt, uint32_t* out, unsig
 
 // Elementwise Montgomery-table product: out[i] = a[i] * tab[i] (tab in Montgomery form).
 __global__ void k_mul_mont_tab(Fp f, const uint32_t* a, const uint32_t* tab, uint32_t* out, size_t n) {
+  pdl_enter();
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
     out[i] = red(mont(a[i], tab[i], f), f.p);
 }
@@ -688,40 +761,40 @@ namespace fpx {
 cudaError_t launch_seed(int kind, uint32_t p, const uint32_t* a, size_t la, uint32_t* out, int n, uint32_t r0,
                         cudaStream_t s) {
   if (n <= 0) return cudaSuccess;
-  k_seed<<<1, 32, 0, s>>>(kind, p, a, la, out, n, r0);
+  (void)pdl_launch(k_seed, 1, 32, 0, s, kind, p, a, la, out, n, r0);
   return cudaGetLastError();
 }
 
 cudaError_t launch_find_nonzero(const uint32_t* a, size_t n, int mode, unsigned long long* res, cudaStream_t s) {
   if (n == 0) return cudaSuccess;
-  k_find_nonzero<<<grid_for(n, 256), 256, 0, s>>>(a, n, mode, res);
+  (void)pdl_launch(k_find_nonzero, grid_for(n, 256), 256, 0, s, a, n, mode, res);
   return cudaGetLastError();
 }
 
 cudaError_t launch_reverse(const uint32_t* a, uint32_t* r, size_t n, cudaStream_t s) {
   if (n == 0) return cudaSuccess;
-  k_reverse<<<grid_for(n, 256), 256, 0, s>>>(a, r, n);
+  (void)pdl_launch(k_reverse, grid_for(n, 256), 256, 0, s, a, r, n);
   return cudaGetLastError();
 }
 
 cudaError_t launch_sub(uint32_t p, const uint32_t* a, const uint32_t* b, size_t lb, uint32_t* r, size_t n,
                        cudaStream_t s) {
   if (n == 0) return cudaSuccess;
-  k_sub<<<grid_for(n, 256), 256, 0, s>>>(p, a, b, lb, r, n);
+  (void)pdl_launch(k_sub, grid_for(n, 256), 256, 0, s, p, a, b, lb, r, n);
   return cudaGetLastError();
 }
 
 cudaError_t launch_sqrt_char2(const uint32_t* a, size_t cnt, uint32_t* out, unsigned long long* odd_flag,
                               cudaStream_t s) {
   if (cnt == 0) return cudaSuccess;
-  k_sqrt_char2<<<grid_for(cnt, 256), 256, 0, s>>>(a, cnt, out, odd_flag);
+  (void)pdl_launch(k_sqrt_char2, grid_for(cnt, 256), 256, 0, s, a, cnt, out, odd_flag);
   return cudaGetLastError();
 }
 
 cudaError_t launch_mul_mont_tab(uint32_t p, const uint32_t* a, const uint32_t* tab, uint32_t* out, size_t n,
                                 cudaStream_t s) {
   if (n == 0) return cudaSuccess;
-  k_mul_mont_tab<<<grid_for(n, 256), 256, 0, s>>>(make_fp(p), a, tab, out, n);
+  (void)pdl_launch(k_mul_mont_tab, grid_for(n, 256), 256, 0, s, make_fp(p), a, tab, out, n);
   return cudaGetLastError();
 }
 
@@ -867,6 +940,7 @@ __device__ __forceinline__ void rows12_body(uint32_t* __restrict__ x, const uint
 __global__ void __launch_bounds__(256, 3) k_rows12(uint32_t* __restrict__ x, const uint32_t* __restrict__ y,
                                                   int ymode, uint32_t* __restrict__ y_spec_out, int forward,
                                                   int inverse, Ptab pt) {
+  pdl_enter();
   rows12_body(x, y, ymode, y_spec_out, forward, inverse, pt, blockIdx.x);
 }
 
@@ -1074,6 +1148,7 @@ __device__ __forceinline__ bool col_tile_of(const ColSplit& sp, int lw1, int lw2
 
 template <int LOGR, int LW1, int LW2>
 __global__ void __launch_bounds__(256, 3) k_colfwd_t(ColOps ops, BigD bt, Ptab pt, ColSplit sp) {
+  pdl_enter();
   int op, j0;
   const bool wide = col_tile_of(sp, LW1, LW2, op, j0);
   const InD in = op == 0 ? ops.in[0] : (op == 1 ? ops.in[1] : ops.in[2]);
@@ -1158,6 +1233,7 @@ __device__ __forceinline__ void colinv_body(const uint32_t* __restrict__ in, con
 template <int LOGR, bool PLAIN, int LW1, int LW2>
 __global__ void __launch_bounds__(256, 3) k_colinv_t(const uint32_t* __restrict__ in, BigD bt, Ptab pt, EpiD epi,
                                                      ColSplit sp) {
+  pdl_enter();
   int op, j0;
   const bool wide = col_tile_of(sp, LW1, LW2, op, j0);
   if constexpr (LW1 == LW2) {
@@ -1284,7 +1360,7 @@ cudaError_t launch_colfwd(const PrimeTables& pt, const BigTables& bt, int nops, 
   if (!fn || lw1 > bt.logC || nops < 1 || nops > 3) return cudaErrorInvalidValue;
   BigD d{bt.logR, bt.logC, lw1, reinterpret_cast<const uint2*>(bt.lo_fwd),
          reinterpret_cast<const uint2*>(bt.mid_fwd), reinterpret_cast<const uint2*>(bt.hi_fwd)};
-  fn<<<(unsigned)(nops * (sp.nbig + sp.nsmall)), 256, size_t(4) << (bt.logR + lw1), s>>>(ops, d, dev_tab(pt), sp);
+  (void)pdl_launch(fn, (unsigned)(nops * (sp.nbig + sp.nsmall)), 256, size_t(4) << (bt.logR + lw1), s, ops, d, dev_tab(pt), sp);
   return cudaGetLastError();
 }
 
@@ -1297,7 +1373,7 @@ cudaError_t launch_colinv(const PrimeTables& pt, const BigTables& bt, const uint
   if (!fn || lw1 > bt.logC) return cudaErrorInvalidValue;
   BigD d{bt.logR, bt.logC, lw1, reinterpret_cast<const uint2*>(mont_scaled ? bt.lo_inv_r : bt.lo_inv),
          reinterpret_cast<const uint2*>(bt.mid_inv), reinterpret_cast<const uint2*>(bt.hi_inv)};
-  fn<<<(unsigned)(sp.nbig + sp.nsmall), 256, size_t(4) << (bt.logR + lw1), s>>>(in, d, dev_tab(pt), dev_epi(epi),
+  (void)pdl_launch(fn, (unsigned)(sp.nbig + sp.nsmall), 256, size_t(4) << (bt.logR + lw1), s, in, d, dev_tab(pt), dev_epi(epi),
                                                                                  sp);
   return cudaGetLastError();
 }
@@ -1305,7 +1381,7 @@ cudaError_t launch_colinv(const PrimeTables& pt, const BigTables& bt, const uint
 cudaError_t launch_rows(const PrimeTables& pt, const BigTables& bt, uint32_t* x, const uint32_t* y, int ymode,
                              uint32_t* y_spec_out, int forward, int inverse, cudaStream_t s) {
   if (bt.logC != 12) return launch_rows_generic(pt, bt, x, y, ymode, y_spec_out, forward, inverse, s);
-  k_rows12<<<1u << bt.logR, 256, 0, s>>>(x, y, ymode, y_spec_out, forward, inverse, dev_tab(pt));
+  (void)pdl_launch(k_rows12, 1u << bt.logR, 256, 0, s, x, y, ymode, y_spec_out, forward, inverse, dev_tab(pt));
   return cudaGetLastError();
 }
 
@@ -1360,18 +1436,21 @@ struct GarnerJobB {
 
 template <int LOGR>
 __global__ void __launch_bounds__(256, 3) k_colfwd_b(const BigJobB* __restrict__ jobs) {
+  pdl_enter();
   const BigJobB& j = jobs[blockIdx.z];
   if ((int)blockIdx.y >= j.nops) return;
   colfwd_body<LOGR, col_logw(LOGR)>(j.in[blockIdx.y], j.t[blockIdx.y], j.bf, j.pt, blockIdx.x << col_logw(LOGR));
 }
 
 __global__ void __launch_bounds__(256, 3) k_rows12_b(const BigJobB* __restrict__ jobs) {
+  pdl_enter();
   const BigJobB& j = jobs[blockIdx.y];
   rows12_body(j.t[0], j.ymode == 1 ? j.t[1] : j.yspec, j.ymode, j.yspec_out, 1, 1, j.pt, blockIdx.x);
 }
 
 template <int LOGR, bool PLAIN>
 __global__ void __launch_bounds__(256, 3) k_colinv_b(const BigJobB* __restrict__ jobs) {
+  pdl_enter();
   const BigJobB& j = jobs[blockIdx.y];
   colinv_body<LOGR, col_logw(LOGR), PLAIN>(j.t[0], j.bi, j.pt, j.epi, blockIdx.x << col_logw(LOGR));
 }
@@ -1385,6 +1464,7 @@ struct OutBlock {
   uint32_t first;
 };
 __global__ void k_direct_b(const DirectJobB* __restrict__ jobs, const OutBlock* __restrict__ map) {
+  pdl_enter();
   const OutBlock m = map[blockIdx.x];
   const DirectJobB& j = jobs[m.job];
   direct_body(j.p, j.f, j.a, j.la, j.b, j.lb, j.off, j.cnt, j.out, j.accumulate, j.post_mont, j.negate, m.first,
@@ -1402,11 +1482,13 @@ struct SeedJobB {
   uint32_t r0;
 };
 __global__ void k_seed_b(const SeedJobB* __restrict__ jobs) {
+  pdl_enter();
   const SeedJobB& j = jobs[blockIdx.x];
   seed_body(j.kind, j.p, j.a, j.la, j.out, j.n, j.r0);
 }
 
 __global__ void k_garner_b(const GarnerJobB* __restrict__ jobs, const OutBlock* __restrict__ map) {
+  pdl_enter();
   const OutBlock m = map[blockIdx.x];
   const GarnerJobB& j = jobs[m.job];
   garner_body(j.g, j.primes, j.c1, j.c2, j.c3, j.out, j.n, j.accumulate, j.post_mont, j.negate, j.tpinv, m.first,
@@ -1430,13 +1512,13 @@ struct ColBatch {
   static cudaError_t launch(int logR, dim3 grid, const BigJobB* jobs, int smem, cudaStream_t s) {
     BatchFn fn = fwd(logR);
     if (!fn) return cudaErrorInvalidValue;
-    fn<<<grid, 256, smem, s>>>(jobs);
+    (void)pdl_launch(fn, grid, 256, smem, s, jobs);
     return cudaGetLastError();
   }
   static cudaError_t launch_inv(int logR, bool plain, dim3 grid, const BigJobB* jobs, int smem, cudaStream_t s) {
     BatchFn fn = inv(logR, plain);
     if (!fn) return cudaErrorInvalidValue;
-    fn<<<grid, 256, smem, s>>>(jobs);
+    (void)pdl_launch(fn, grid, 256, smem, s, jobs);
     return cudaGetLastError();
   }
   static cudaError_t init() {
@@ -1642,13 +1724,13 @@ cudaError_t launch_batch(const BatchPlan& b, void* host_staging, void* dev_desc,
   // block maps are at most 2^31 blocks; grid.x takes them in chunks
   constexpr size_t kMaxX = size_t(1) << 30;
   for (size_t k = 0; k < n_dmap; k += kMaxX) {
-    k_direct_b<<<(unsigned)std::min(kMaxX, n_dmap - k), 256, 0, s>>>(
+    (void)pdl_launch(k_direct_b, (unsigned)std::min(kMaxX, n_dmap - k), 256, 0, s, 
         reinterpret_cast<const DirectJobB*>(d + off_direct), reinterpret_cast<const OutBlock*>(d + off_dmap) + k);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
   }
   for (const BatchGroup& g : groups) {
     if (!g.big && g.logN == 12) {
-      k_cyc4096_b<<<g.count, 256, 0, s>>>(reinterpret_cast<const SmallJobB*>(d + g.off));
+      (void)pdl_launch(k_cyc4096_b, g.count, 256, 0, s, reinterpret_cast<const SmallJobB*>(d + g.off));
       if ((e = cudaGetLastError()) != cudaSuccess) return e;
       continue;
     }
@@ -1665,14 +1747,14 @@ cudaError_t launch_batch(const BatchPlan& b, void* host_staging, void* dev_desc,
       const unsigned cnt = (unsigned)std::min(kMaxY, (size_t)g.count - k);
       e = ColsB::launch(logR, dim3(1u << (logC - logW), 2, cnt), jobs, smem, s);
       if (e != cudaSuccess) return e;
-      k_rows12_b<<<dim3(1u << logR, cnt), 256, 0, s>>>(jobs);
+      (void)pdl_launch(k_rows12_b, dim3(1u << logR, cnt), 256, 0, s, jobs);
       if ((e = cudaGetLastError()) != cudaSuccess) return e;
       e = ColsB::launch_inv(logR, g.plain, dim3(1u << (logC - logW), cnt), jobs, smem, s);
       if (e != cudaSuccess) return e;
     }
   }
   for (size_t k = 0; k < n_gmap; k += kMaxX) {
-    k_garner_b<<<(unsigned)std::min(kMaxX, n_gmap - k), 256, 0, s>>>(
+    (void)pdl_launch(k_garner_b, (unsigned)std::min(kMaxX, n_gmap - k), 256, 0, s, 
         reinterpret_cast<const GarnerJobB*>(d + off_garner), reinterpret_cast<const OutBlock*>(d + off_gmap) + k);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
   }
@@ -1693,7 +1775,7 @@ cudaError_t launch_seeds_batch(const std::vector<SeedJob>& jobs, void* host_stag
   cudaError_t e = cudaMemcpyAsync(dev_desc, host_staging, v.size() * sizeof(SeedJobB), cudaMemcpyHostToDevice, s);
   if (e != cudaSuccess) return e;
   if (staged && (e = cudaEventRecord(staged, s)) != cudaSuccess) return e;
-  k_seed_b<<<(unsigned)v.size(), 32, 0, s>>>(static_cast<const SeedJobB*>(dev_desc));
+  (void)pdl_launch(k_seed_b, (unsigned)v.size(), 32, 0, s, static_cast<const SeedJobB*>(dev_desc));
   return cudaGetLastError();
 }
 
@@ -1713,7 +1795,7 @@ cudaError_t launch_exp_prep_batch(const std::vector<ExpPrep>& jobs, void* host_s
   if (e != cudaSuccess) return e;
   if (staged && (e = cudaEventRecord(staged, s)) != cudaSuccess) return e;
   dim3 grid((unsigned)std::min<size_t>((maxn + 255) / 256, 256), (unsigned)v.size());
-  k_exp_prep_b<<<grid, 256, 0, s>>>(static_cast<const ExpPrepB*>(dev_desc));
+  (void)pdl_launch(k_exp_prep_b, grid, 256, 0, s, static_cast<const ExpPrepB*>(dev_desc));
   return cudaGetLastError();
 }
 
@@ -1723,6 +1805,7 @@ size_t batch_aux_bytes(size_t jobs) { return jobs * std::max(sizeof(SeedJobB), s
 
 namespace {
 __global__ void k_gather_first(const uint32_t* const* __restrict__ ptrs, uint32_t* __restrict__ out, int n) {
+  pdl_enter();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) out[i] = ptrs[i] ? *ptrs[i] : 0u;
 }
@@ -1735,6 +1818,7 @@ struct ReprSegB {
   int to_mont;
 };
 __global__ void k_repr_b(const ReprSegB* __restrict__ segs) {
+  pdl_enter();
   const ReprSegB& g = segs[blockIdx.y];
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < g.n; i += (size_t)gridDim.x * blockDim.x) {
     const uint32_t x = g.ptr[i];
@@ -1779,7 +1863,7 @@ cudaError_t launch_repr_batch(const std::vector<ReprSeg>& segs, void* host_stagi
   for (size_t k = 0; k < v.size(); k += 65535) {  // grid.y limit
     const unsigned cnt = (unsigned)std::min<size_t>(65535, v.size() - k);
     dim3 grid((unsigned)std::min<size_t>((maxn + 255) / 256, 128), cnt);
-    k_repr_b<<<grid, 256, 0, s>>>(static_cast<const ReprSegB*>(dev_desc) + k);
+    (void)pdl_launch(k_repr_b, grid, 256, 0, s, static_cast<const ReprSegB*>(dev_desc) + k);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
   }
   return cudaSuccess;
@@ -1798,7 +1882,7 @@ cudaError_t launch_gather_first(const std::vector<const uint32_t*>& ptrs, void* 
   cudaError_t e = cudaMemcpyAsync(d, host_staging, bytes, cudaMemcpyHostToDevice, s);
   if (e != cudaSuccess) return e;
   uint32_t* dout = reinterpret_cast<uint32_t*>(d + ((bytes + 255) & ~size_t(255)));
-  k_gather_first<<<(unsigned)((ptrs.size() + 255) / 256), 256, 0, s>>>(reinterpret_cast<const uint32_t* const*>(d),
+  (void)pdl_launch(k_gather_first, (unsigned)((ptrs.size() + 255) / 256), 256, 0, s, reinterpret_cast<const uint32_t* const*>(d),
                                                                          dout, (int)ptrs.size());
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   return cudaMemcpyAsync(host_out, dout, ptrs.size() * 4, cudaMemcpyDeviceToHost, s);
@@ -1910,9 +1994,10 @@ __device__ __forceinline__ void cyc4096_body(const SmallD& job, const Ptab& pt) 
   for (int i = 0; i < 16; ++i) epi_store(job.epi, posA(t, i), v[0][i], f);
 }
 
-__global__ void __launch_bounds__(256) k_cyc4096(SmallD job, Ptab pt) { cyc4096_body(job, pt); }
+__global__ void __launch_bounds__(256) k_cyc4096(SmallD job, Ptab pt) { pdl_enter(); cyc4096_body(job, pt); }
 // Batched: one CTA per job (descriptors as the batched one-CTA kernel's).
 __global__ void __launch_bounds__(256) k_cyc4096_b(const SmallJobB* __restrict__ jobs) {
+  pdl_enter();
   const SmallJobB& j = jobs[blockIdx.x];
   cyc4096_body(j.d, j.pt);
 }
@@ -1932,7 +2017,7 @@ cudaError_t launch_cyc4096(const PrimeTables& pt, const SmallJob& job, cudaStrea
   d.yspec_out = job.yspec_out;
   d.spec_x = nullptr;
   d.epi = dev_epi(job.epi);
-  k_cyc4096<<<1, 256, 0, s>>>(d, dev_tab(pt));
+  (void)pdl_launch(k_cyc4096, 1, 256, 0, s, d, dev_tab(pt));
   return cudaGetLastError();
 }
 
@@ -2028,10 +2113,12 @@ __device__ __forceinline__ void cyc_small_body(const SmallD& job, const Ptab& pt
 
 template <int LOGN>
 __global__ void __launch_bounds__(512) k_cyc_small(SmallD job, Ptab pt) {
+  pdl_enter();
   cyc_small_body<LOGN>(job, pt);
 }
 template <int LOGN>
 __global__ void __launch_bounds__(512) k_cyc_small_b(const SmallJobB* __restrict__ jobs) {
+  pdl_enter();
   const SmallJobB& j = jobs[blockIdx.x];
   cyc_small_body<LOGN>(j.d, j.pt);
 }
@@ -2088,7 +2175,7 @@ cudaError_t launch_cyc_small(const PrimeTables& pt, int logN, const SmallJob& jo
   d.yspec_out = job.yspec_out;
   d.spec_x = nullptr;
   d.epi = dev_epi(job.epi);
-  fn<<<1, cyc_threads(logN), (size_t)2 * padded_words(1 << logN) * 4, s>>>(d, dev_tab(pt));
+  (void)pdl_launch(fn, 1, cyc_threads(logN), (size_t)2 * padded_words(1 << logN) * 4, s, d, dev_tab(pt));
   return cudaGetLastError();
 }
 
@@ -2098,7 +2185,7 @@ namespace {
 cudaError_t launch_cyc_small_batch(int logN, unsigned count, const SmallJobB* jobs, cudaStream_t s) {
   CycBFn fn = Cyc::batch(logN);
   if (!fn) return cudaErrorInvalidValue;
-  fn<<<count, cyc_threads(logN), (size_t)2 * padded_words(1 << logN) * 4, s>>>(jobs);
+  (void)pdl_launch(fn, count, cyc_threads(logN), (size_t)2 * padded_words(1 << logN) * 4, s, jobs);
   return cudaGetLastError();
 }
 }  // namespace
