@@ -656,8 +656,16 @@ void Engine::extend_inverse(uint32_t p, const uint32_t* a, size_t la, uint32_t* 
 void Engine::inv_into(uint32_t p, const uint32_t* a, size_t la, size_t n, uint32_t* out) {
   la = std::min(la, n);
   const size_t seed = std::min<size_t>(n, 32);
-  kcheck(launch_seed(0, p, a, la, out, (int)seed, 0, stream_), "inverse seed");
-  for (size_t m = seed; m < n; m <<= 1) extend_inverse(p, a, la, out, m, std::min(2 * m, n));
+  size_t m = seed;
+  if (native(p, newton_inv_max_log())) {
+    // 1 / a[0] and every doubling step up to 2^13 terms in one CTA
+    const size_t K = std::min(n, size_t(1) << newton_inv_max_log());
+    kcheck(launch_newton_inv(prime_plan(p).t, a, la, out, 0, K, stream_), "newton inverse");
+    m = K;
+  } else {
+    kcheck(launch_seed(0, p, a, la, out, (int)seed, 0, stream_), "inverse seed");
+  }
+  for (; m < n; m <<= 1) extend_inverse(p, a, la, out, m, std::min(2 * m, n));
 }
 
 // inv (inverse.hpp:163-188).

@@ -457,6 +457,97 @@ int grid_for(size_t n, int threads) {
 
 uint2 shoup_const(uint32_t w, uint32_t p) { return make_uint2(w, (uint32_t)(((uint64_t)w << 32) / p)); }
 
+// ---------------------------------------------------------------------------
+// Newton inverse at the small sizes in one CTA.  The doubling steps k -> 2k of
+// the series inverse (inverse.hpp:18-65) with 2k <= 2^13 points run back to
+// back in shared memory: per step the middle product h = -(a c)[k, 2k) and the
+// product (h c) mod x^(2k-k) as cyclic products of 2k points (wrap-free for
+// these windows), exactly what the per-step launches compute, with no launch,
+// global round trip or host step between them.  c[0, k0) holds the seed.
+// ---------------------------------------------------------------------------
+constexpr int kNewtonThreads = 512;
+constexpr int kNewtonMaxLog = kSmallLog;  // 2k <= 2^13: the per-prime twiddle table
+constexpr int kNewtonPW = padded_words(1 << kNewtonMaxLog);
+constexpr int kNewtonSmemWords = 2 * kNewtonPW + (1 << kNewtonMaxLog) + (1 << (kNewtonMaxLog - 1));
+
+struct NewtonInvD {
+  const uint32_t* a;  // the series (canonical, a[0] != 0), la terms
+  uint32_t la;
+  uint32_t* c;        // its inverse: c[0, k0) on entry (k0 = 0: computed here), c[0, K) on return
+  uint32_t k0, K;     // k0 0 or a power of two, K <= 2^13
+  uint32_t r1, r2;    // 2^32 and 2^64 mod p
+  uint2 scale_r[kNewtonMaxLog + 1];  // Shoup constants of 2^32 / 2^l mod p (undo N and the Montgomery factor)
+};
+
+__global__ void __launch_bounds__(kNewtonThreads) k_newton_inv(NewtonInvD d, Ptab pt) {
+  pdl_enter();
+  extern __shared__ uint32_t smn[];
+  uint32_t* X = smn;                      // transform buffer, padded
+  uint32_t* Y = smn + kNewtonPW;          // spectrum of c[0, k), padded
+  uint32_t* Cs = smn + 2 * kNewtonPW;     // c[0, K)
+  uint32_t* H = Cs + (1 << kNewtonMaxLog);  // h, < 2^12 terms
+  const int tid = threadIdx.x, nt = blockDim.x;
+  const Fp f = pt.f;
+  uint32_t k = d.k0;
+  if (k == 0) {
+    // c[0] = a[0]^(p-2) mod p by Montgomery square-and-multiply
+    if (tid == 0) {
+      const uint32_t am = mont(__ldg(d.a), d.r2, f);
+      uint32_t r = d.r1;
+      for (int b = 31 - __clz(f.p - 2); b >= 0; --b) {
+        r = mont(r, r, f);
+        if (((f.p - 2) >> b) & 1u) r = mont(r, am, f);
+      }
+      const uint32_t c0 = red(mont(r, 1u, f), f.p);
+      Cs[0] = c0;
+      d.c[0] = c0;
+    }
+    k = 1;
+  } else {
+    for (uint32_t i = tid; i < k; i += nt) Cs[i] = d.c[i];
+  }
+  __syncthreads();
+  for (; k < d.K; k <<= 1) {
+    const uint32_t want = min(2 * k, d.K), hl = want - k;
+    const int logN = 32 - __clz(2 * k - 1);
+    const uint32_t N = 1u << logN;
+    const uint32_t aw = min(d.la, want);
+    const uint2 sc = d.scale_r[logN];
+    for (uint32_t i = tid; i < N; i += nt) {
+      X[pad(i)] = i < aw ? __ldg(d.a + i) : 0u;
+      Y[pad(i)] = i < k ? Cs[i] : 0u;
+    }
+    __syncthreads();
+    tile_dif(X, logN, 0, pt.fwd, f, tid, nt);
+    __syncthreads();
+    tile_dif(Y, logN, 0, pt.fwd, f, tid, nt);
+    __syncthreads();
+    for (uint32_t i = tid; i < N; i += nt) X[pad(i)] = mont(X[pad(i)], Y[pad(i)], f);
+    __syncthreads();
+    tile_dit(X, logN, 0, pt.inv, f, tid, nt);
+    __syncthreads();
+    for (uint32_t i = tid; i < hl; i += nt) {
+      const uint32_t v = red(shoup(X[pad(k + i)], sc, f.p), f.p);
+      H[i] = v ? f.p - v : 0u;
+    }
+    __syncthreads();
+    for (uint32_t i = tid; i < N; i += nt) X[pad(i)] = i < hl ? H[i] : 0u;
+    __syncthreads();
+    tile_dif(X, logN, 0, pt.fwd, f, tid, nt);
+    __syncthreads();
+    for (uint32_t i = tid; i < N; i += nt) X[pad(i)] = mont(X[pad(i)], Y[pad(i)], f);
+    __syncthreads();
+    tile_dit(X, logN, 0, pt.inv, f, tid, nt);
+    __syncthreads();
+    for (uint32_t i = tid; i < hl; i += nt) {
+      const uint32_t v = red(shoup(X[pad(i)], sc, f.p), f.p);
+      Cs[k + i] = v;
+      d.c[k + i] = v;
+    }
+    __syncthreads();
+  }
+}
+
 }  // namespace
 
 namespace fpx {
@@ -477,6 +568,7 @@ cudaError_t kernels_init() {
   };
   set((const void*)k_small, 2 * padded_words(1 << kSmallLog) * 4);
   set((const void*)k_rows, 2 * padded_words(1 << 13) * 4);
+  set((const void*)k_newton_inv, kNewtonSmemWords * 4);
   const cudaError_t r = kernels_fast_init();
   const cudaError_t r2 = kernels_batch_init();
   const cudaError_t r3 = kernels_cyc_init();
@@ -762,6 +854,28 @@ cudaError_t launch_seed(int kind, uint32_t p, const uint32_t* a, size_t la, uint
                         cudaStream_t s) {
   if (n <= 0) return cudaSuccess;
   (void)pdl_launch(k_seed, 1, 32, 0, s, kind, p, a, la, out, n, r0);
+  return cudaGetLastError();
+}
+
+int newton_inv_max_log() { return kNewtonMaxLog; }
+
+cudaError_t launch_newton_inv(const PrimeTables& pt, const uint32_t* a, size_t la, uint32_t* c, size_t k0, size_t K,
+                              cudaStream_t s) {
+  // the last step k -> K transforms 2^ceil(log2 K) points
+  if (K > (size_t(1) << kNewtonMaxLog) || (k0 & (k0 - 1)) || k0 > K || (size_t(1) << pt.small_log) < K ||
+      !(pt.p & 1u) || pt.p >= (1u << 30))
+    return cudaErrorInvalidValue;
+  if (K == k0) return cudaSuccess;
+  NewtonInvD d;
+  d.r1 = (uint32_t)((uint64_t(1) << 32) % pt.p);
+  d.r2 = (uint32_t)((uint64_t)d.r1 * d.r1 % pt.p);
+  d.a = a;
+  d.la = (uint32_t)std::min<size_t>(la, K);
+  d.c = c;
+  d.k0 = (uint32_t)k0;
+  d.K = (uint32_t)K;
+  for (int l = 0; l <= kNewtonMaxLog; ++l) d.scale_r[l] = shoup_const(l <= pt.small_log ? pt.inv_pow2_r[l] : 0u, pt.p);
+  (void)pdl_launch(k_newton_inv, 1, kNewtonThreads, (size_t)kNewtonSmemWords * 4, s, d, dev_tab(pt));
   return cudaGetLastError();
 }
 

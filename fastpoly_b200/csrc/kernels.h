@@ -22,9 +22,6 @@ struct PrimeTables {
   uint32_t inv_pow2_r[14] = {};
 };
 
-// Per-(prime, N) tables for the two-pass (four-step) decomposition.
-// The Bailey twiddle w_N^e (e < N) is lo[e & 255] * mid[(e >> 8) & 255] *
-// hi[e >> 16]: three small tables instead of one of N entries.
 // Tile shape of one column pass: wide tiles of 2^lw1 columns; with split != 0
 // the columns past the last full wave of wide tiles (`slots` resident CTAs on
 // the device) go in narrow tiles of 2^lw2 columns.  lw1 == 0: the default
@@ -36,6 +33,9 @@ struct ColShapes {
   ColShape fwd1, fwd2, inv;  // forward pass of one operand, of two or three; inverse pass
 };
 
+// Per-(prime, N) tables for the two-pass (four-step) decomposition.
+// The Bailey twiddle w_N^e (e < N) is lo[e & 255] * mid[(e >> 8) & 255] *
+// hi[e >> 16]: three small tables instead of one of N entries.
 struct BigTables {
   int logN = 0, logR = 0, logC = 0;
   const ColShapes* shapes = nullptr;  // chosen column-pass tile shapes; nullptr: defaults
@@ -142,6 +142,12 @@ namespace fpx {
 // Seeds of the Newton loops (kind 0 inverse, 1 exp (a = a'), 2 sqrt (a = u, r0 = root)); n <= 64.
 cudaError_t launch_seed(int kind, uint32_t p, const uint32_t* a, size_t la, uint32_t* out, int n, uint32_t r0,
                         cudaStream_t s);
+// Series inverse c[k0, K) of a from c[0, k0) (k0 a power of two, or 0: from
+// c[0] = 1 / a[0], a[0] != 0), all doubling steps in one CTA: needs
+// K <= 2^small_log of pt and K <= 2^newton_inv_max_log().
+int newton_inv_max_log();
+cudaError_t launch_newton_inv(const PrimeTables& pt, const uint32_t* a, size_t la, uint32_t* c, size_t k0, size_t K,
+                              cudaStream_t s);
 // *res = min (mode 0) / max (mode 1) index with a[i] != 0; caller initialises *res.
 cudaError_t launch_find_nonzero(const uint32_t* a, size_t n, int mode, unsigned long long* res, cudaStream_t s);
 cudaError_t launch_reverse(const uint32_t* a, uint32_t* r, size_t n, cudaStream_t s);
