@@ -150,6 +150,7 @@ int fpx_pool_stats(fpx_ctx* ctx, fpx_pool_stats_t* out) {
 int fpx_release_pool(fpx_ctx* ctx) {
   return guarded(ctx, [&](fpx::Engine& e) {
     e.sync();
+    e.drop_graphs();
     e.pool().release();
   });
 }

@@ -10,6 +10,7 @@
 
 #include <algorithm>
 #include <bit>
+#include <cstdlib>
 #include <cstring>
 
 #include "fpx_b200.h"
@@ -136,6 +137,15 @@ uint32_t* Pool::get(size_t words, size_t* cls_out) {
   while (cls < bytes) cls <<= 1;
   {
     std::lock_guard<std::mutex> g(mu_);
+    if (capturing_) {
+      auto ct = cap_free_.find(cls);
+      if (ct != cap_free_.end() && !ct->second.empty()) {
+        uint32_t* p = ct->second.back();
+        ct->second.pop_back();
+        *cls_out = cls;
+        return p;
+      }
+    }
     auto it = free_.find(cls);
     if (it != free_.end() && !it->second.empty()) {
       void* p = it->second.back();
@@ -145,6 +155,7 @@ uint32_t* Pool::get(size_t words, size_t* cls_out) {
       ++cache_hits;
       in_use_bytes += cls;
       *cls_out = cls;
+      if (capturing_) cap_owned_[static_cast<uint32_t*>(p)] = cls;
       return static_cast<uint32_t*>(p);
     }
   }
@@ -166,15 +177,46 @@ uint32_t* Pool::get(size_t words, size_t* cls_out) {
   ++system_allocations;
   in_use_bytes += cls;
   *cls_out = cls;
+  if (capturing_) cap_owned_[static_cast<uint32_t*>(p)] = cls;
   return static_cast<uint32_t*>(p);
 }
 
 void Pool::put(uint32_t* p, size_t cls) {
   std::lock_guard<std::mutex> g(mu_);
+  if (capturing_ && cap_owned_.count(p)) {
+    cap_free_[cls].push_back(p);  // reused only inside the graph being captured
+    return;
+  }
   free_[cls].push_back(p);
   cached_bytes += cls;
   ++cached_blocks;
   in_use_bytes -= cls;
+}
+
+void Pool::begin_capture() {
+  std::lock_guard<std::mutex> g(mu_);
+  capturing_ = true;
+  cap_owned_.clear();
+  cap_free_.clear();
+}
+
+std::vector<std::pair<uint32_t*, size_t>> Pool::end_capture() {
+  std::lock_guard<std::mutex> g(mu_);
+  capturing_ = false;
+  std::vector<std::pair<uint32_t*, size_t>> r(cap_owned_.begin(), cap_owned_.end());
+  cap_owned_.clear();
+  cap_free_.clear();
+  return r;
+}
+
+void Pool::give_back(const std::vector<std::pair<uint32_t*, size_t>>& blocks) {
+  std::lock_guard<std::mutex> g(mu_);
+  for (const auto& [p, cls] : blocks) {
+    free_[cls].push_back(p);
+    cached_bytes += cls;
+    ++cached_blocks;
+    in_use_bytes -= cls;
+  }
 }
 
 void Pool::release() {
@@ -201,11 +243,17 @@ Engine::Engine(int device, size_t pool_limit) : device_(device), pool_(pool_limi
   check(kernels_init(), "kernel attributes");
   check(cudaMalloc(&scratch_ull_, 16), "cudaMalloc");
   check(cudaMallocHost(&host_ull_, 16), "cudaMallocHost");
+  check(cudaMallocHost(&host_one_, 4), "cudaMallocHost");
+  *host_one_ = 1;
+  const char* g = std::getenv("FPX_GRAPHS");
+  graphs_on_ = !(g && g[0] == '0');
 }
 
 Engine::~Engine() {
   cudaSetDevice(device_);
   if (stream_) cudaStreamSynchronize(stream_);
+  drop_graphs();
+  if (host_one_) cudaFreeHost(host_one_);
   primes_.clear();
   bigs_.clear();
   inv_tabs_.clear();
@@ -284,6 +332,105 @@ void Engine::set_stream(cudaStream_t s) {
   // Pool blocks are recycled in stream order; drain the old stream first.
   sync();
   stream_ = s ? s : own_stream_;
+}
+
+// ---------------------------------------------------------------- graphs
+
+namespace {
+constexpr size_t kMaxGraphs = 16;
+constexpr size_t kMaxGraphBytes = size_t(4) << 30;
+constexpr size_t kMaxSeen = 256;
+}  // namespace
+
+void Engine::free_graph(GraphEntry& g) {
+  if (g.exec) cudaGraphExecDestroy(g.exec);
+  if (g.graph) cudaGraphDestroy(g.graph);
+  pool_.give_back(g.blocks);
+  g = GraphEntry{};
+}
+
+void Engine::drop_graphs() {
+  graph_seen_.clear();
+  if (graphs_.empty()) return;
+  cudaStreamSynchronize(stream_);  // no replay in flight
+  for (auto& [k, g] : graphs_) free_graph(g);
+  graphs_.clear();
+}
+
+// Every product of a Newton operation of n terms transforms at most 2n points;
+// on a prime with roots of that order no step needs the host (CRT products go
+// through the descriptor staging ring, which waits on events).
+bool Engine::graph_native(uint32_t p, size_t n) const { return n >= 2 && native(p, std::bit_width(2 * n - 1)); }
+
+void Engine::run_graph(const GraphKey& key, const std::function<void()>& fn) {
+  if (!graphs_on_ || prof_on_) {
+    fn();
+    return;
+  }
+  auto it = graphs_.find(key);
+  if (it == graphs_.end()) {
+    if (!graph_seen_.count(key)) {
+      // first call: run it directly (this also builds every plan and table the
+      // operation needs, so the capture below makes no host round trip)
+      if (graph_seen_.size() >= kMaxSeen) graph_seen_.clear();
+      graph_seen_.insert(key);
+      fn();
+      return;
+    }
+    const uint64_t l0 = launches_;
+    pool_.begin_capture();
+    const cudaError_t be = cudaStreamBeginCapture(stream_, cudaStreamCaptureModeRelaxed);
+    if (be != cudaSuccess) {
+      cudaGetLastError();
+      pool_.give_back(pool_.end_capture());
+      throw Error{FPX_ECUDA, std::string("cudaStreamBeginCapture: ") + cudaGetErrorString(be)};
+    }
+    GraphEntry e;
+    try {
+      fn();
+    } catch (...) {
+      cudaGraph_t g = nullptr;
+      cudaStreamEndCapture(stream_, &g);
+      if (g) cudaGraphDestroy(g);
+      cudaGetLastError();
+      pool_.give_back(pool_.end_capture());
+      launches_ = l0;
+      graph_seen_.erase(key);
+      throw;
+    }
+    const cudaError_t ce = cudaStreamEndCapture(stream_, &e.graph);
+    e.blocks = pool_.end_capture();
+    if (ce != cudaSuccess) {
+      cudaGetLastError();
+      free_graph(e);
+      throw Error{FPX_ECUDA, std::string("cudaStreamEndCapture: ") + cudaGetErrorString(ce)};
+    }
+    const cudaError_t ie = cudaGraphInstantiate(&e.exec, e.graph, 0);
+    if (ie != cudaSuccess) {
+      cudaGetLastError();
+      free_graph(e);
+      throw Error{FPX_ECUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(ie)};
+    }
+    for (const auto& b : e.blocks) e.bytes += b.second;
+    e.kernels = launches_ - l0;
+    launches_ = l0;  // nothing ran during the capture
+    // keep at most kMaxGraphs graphs and kMaxGraphBytes of graph scratch
+    size_t total = e.bytes;
+    for (const auto& [k, g] : graphs_) total += g.bytes;
+    while (!graphs_.empty() && (graphs_.size() >= kMaxGraphs || total > kMaxGraphBytes)) {
+      auto old = graphs_.begin();
+      for (auto j = graphs_.begin(); j != graphs_.end(); ++j)
+        if (j->second.last_use < old->second.last_use) old = j;
+      cudaStreamSynchronize(stream_);
+      total -= old->second.bytes;
+      free_graph(old->second);
+      graphs_.erase(old);
+    }
+    it = graphs_.emplace(key, std::move(e)).first;
+  }
+  it->second.last_use = ++graph_clock_;
+  check(cudaGraphLaunch(it->second.exec, stream_), "cudaGraphLaunch");
+  launches_ += it->second.kernels;
 }
 
 uint32_t Engine::read_word(const uint32_t* d) {
@@ -672,7 +819,8 @@ void Engine::inv_into(uint32_t p, const uint32_t* a, size_t la, size_t n, uint32
 void Engine::inv(uint32_t p, const uint32_t* a, size_t la, size_t n, uint32_t* out) {
   if (n == 0) return;
   if (la == 0 || read_word(a) == 0) throw Error{FPX_EDOMAIN, "poly::inv: constant term is zero"};
-  inv_into(p, a, la, n, out);
+  if (graph_native(p, n)) run_graph(GraphKey{FPX_OP_INV, p, n, la, a, out}, [&] { inv_into(p, a, la, n, out); });
+  else inv_into(p, a, la, n, out);
 }
 
 // log (exponential.hpp:85-98): integral(a' * inv(a, n-1)) mod x^n.
@@ -698,15 +846,15 @@ void Engine::log(uint32_t p, const uint32_t* a, size_t la, size_t n, uint32_t* o
   if (n == 0) return;
   if (la == 0 || read_word(a) != 1 % p) throw Error{FPX_EDOMAIN, "poly::log: constant term must be 1"};
   if (n > p) throw Error{FPX_EDOMAIN, "poly::log: required denominators must be invertible (n <= mod)"};
-  log_into(p, a, la, n, out);
+  if (graph_native(p, n)) run_graph(GraphKey{FPX_OP_LOG, p, n, la, a, out}, [&] { log_into(p, a, la, n, out); });
+  else log_into(p, a, la, n, out);
 }
 
 // exp (exponential.hpp:107-207): Newton on the high differential residual,
 // eight transforms at N = 2m per doubling plus the running inverse of b.
 void Engine::exp_into(uint32_t p, const uint32_t* a, size_t la, size_t n, uint32_t* out) {
-  static const uint32_t one = 1;
   check(cudaMemsetAsync(out, 0, n * 4, stream_), "memset");
-  check(cudaMemcpyAsync(out, &one, 4, cudaMemcpyHostToDevice, stream_), "one");
+  check(cudaMemcpyAsync(out, host_one_, 4, cudaMemcpyHostToDevice, stream_), "one");
   const size_t cnt = std::min(la, n);
   if (cnt <= 1 || n == 1) return;
   const size_t lap = cnt - 1;
@@ -774,7 +922,8 @@ void Engine::exp(uint32_t p, const uint32_t* a, size_t la, size_t n, uint32_t* o
   if (n == 0) return;
   if (la != 0 && read_word(a) != 0) throw Error{FPX_EDOMAIN, "poly::exp: constant term must be 0"};
   if (n - 1 >= p) throw Error{FPX_EDOMAIN, "poly::inv_series: length must be < mod"};
-  exp_into(p, a, la, n, out);
+  if (graph_native(p, n)) run_graph(GraphKey{FPX_OP_EXP, p, n, la, a, out}, [&] { exp_into(p, a, la, n, out); });
+  else exp_into(p, a, la, n, out);
 }
 
 // sqrt (square_root.hpp:12-112).

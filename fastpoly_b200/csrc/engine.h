@@ -7,7 +7,10 @@
 // fused GPU passes of kernels.cu.
 #pragma once
 #include <cstdint>
+#include <functional>
 #include <map>
+#include <set>
+#include <tuple>
 #include <memory>
 #include <mutex>
 #include <string>
@@ -34,12 +37,23 @@ class Pool {
   uint32_t* get(size_t words, size_t* cls_out);
   void put(uint32_t* p, size_t cls);
   void release();
+  // Graph capture: between begin_capture and end_capture every block handed
+  // out is owned by the graph being captured; released ones are recycled only
+  // within the capture (stream order inside the graph), and end_capture hands
+  // all of them to the caller, who keeps them for the graph's lifetime and
+  // returns them with give_back.
+  void begin_capture();
+  std::vector<std::pair<uint32_t*, size_t>> end_capture();
+  void give_back(const std::vector<std::pair<uint32_t*, size_t>>& blocks);
   size_t cached_bytes = 0, cached_blocks = 0, in_use_bytes = 0, system_allocations = 0, cache_hits = 0;
   size_t limit_ = 0;
 
  private:
   std::map<size_t, std::vector<void*>> free_;
   std::mutex mu_;
+  bool capturing_ = false;
+  std::map<uint32_t*, size_t> cap_owned_;
+  std::map<size_t, std::vector<uint32_t*>> cap_free_;
 };
 
 class Engine;
@@ -135,6 +149,12 @@ class Engine {
   int col_shape_candidates(int logN, int kind, ColShape* out, int max);
   void set_col_shape(int logN, int kind, const ColShape& sh);  // throws Error(FPX_EINVAL) if not compiled
 
+  // CUDA graphs of single Newton operations (inv / log / exp on transform
+  // primes): the second call with the same (operation, prime, sizes, device
+  // pointers) captures the operation's launches into a graph, later calls
+  // replay it.  FPX_GRAPHS=0 turns this off.  drop_graphs frees them all.
+  void drop_graphs();
+
   // Per-kernel timing (CUDA events on the launching stream) and launch count.
   void profile(bool on);
   std::string profile_report();  // {"kernel": [launches, total_ms], ...}
@@ -152,6 +172,35 @@ class Engine {
   const uint32_t* inv_table(uint32_t p, size_t n);  // Montgomery form 1/i, i <= n
 
   bool native(uint32_t p, int logN) const;  // GPU NTT usable for (p, 2^logN)
+
+  // ---- graphs
+  struct GraphKey {
+    int op;
+    uint32_t p;
+    size_t n, la;
+    const void* a;
+    void* out;
+    bool operator<(const GraphKey& o) const {
+      return std::tie(op, p, n, la, a, out) < std::tie(o.op, o.p, o.n, o.la, o.a, o.out);
+    }
+  };
+  struct GraphEntry {
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    std::vector<std::pair<uint32_t*, size_t>> blocks;  // scratch owned by the graph
+    size_t bytes = 0;
+    uint64_t kernels = 0;  // launches the graph stands for
+    uint64_t last_use = 0;
+  };
+  bool graph_native(uint32_t p, size_t n) const;
+  // Runs fn, through a captured graph when `key` has been seen before.
+  void run_graph(const GraphKey& key, const std::function<void()>& fn);
+  void free_graph(GraphEntry& g);
+  bool graphs_on_ = true;
+  uint64_t graph_clock_ = 0;
+  std::map<GraphKey, GraphEntry> graphs_;
+  std::set<GraphKey> graph_seen_;
+  uint32_t* host_one_ = nullptr;  // pinned constant 1 (capturable host->device copy)
 
   // ---- transform compositions
   struct CycOp {
