@@ -864,14 +864,29 @@ void Engine::exp_into(uint32_t p, const uint32_t* a, size_t la, size_t n, uint32
   }
   Buf ap(&pool_, lap);
   kcheck(launch_derivative(p, a, ap.get(), cnt, stream_), "derivative");
-  const size_t seed = std::min<size_t>(n, 32);
-  kcheck(launch_seed(1, p, ap.get(), lap, out, (int)seed, 0, stream_), "exp seed");
-  if (n == seed) return;
   Buf c(&pool_, n / 2 + 64);
-  size_t csize = seed / 2;
-  kcheck(launch_seed(0, p, out, seed, c.get(), (int)csize, 0, stream_), "inverse seed");
   const uint32_t* tab = inv_table(p, n - 1);
-  for (size_t m = seed; m < n; m *= 2) {
+  size_t m, csize;
+  if (native(p, newton_inv_max_log())) {
+    // every doubling step up to 2^13 terms (and 1/b alongside) in one CTA
+    const size_t K = std::min(n, size_t(1) << newton_inv_max_log());
+    kcheck(launch_newton_exp(prime_plan(p).t, ap.get(), lap, tab, out, c.get(), K, stream_), "newton exp");
+    m = K;
+    csize = 1;
+    for (size_t mm = 1; mm < K;) {
+      const size_t h = std::min(2 * mm, K) - mm;
+      while (csize < h) csize = std::min(2 * csize, h);
+      mm += h;
+    }
+  } else {
+    const size_t seed = std::min<size_t>(n, 32);
+    kcheck(launch_seed(1, p, ap.get(), lap, out, (int)seed, 0, stream_), "exp seed");
+    if (n == seed) return;
+    csize = seed / 2;
+    kcheck(launch_seed(0, p, out, seed, c.get(), (int)csize, 0, stream_), "inverse seed");
+    m = seed;
+  }
+  for (; m < n; m *= 2) {
     const size_t m2 = std::min(2 * m, n), hlen = m2 - m;
     if (csize < hlen) {
       extend_inverse(p, out, m, c.get(), csize, hlen);

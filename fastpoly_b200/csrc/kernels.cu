@@ -479,6 +479,58 @@ struct NewtonInvD {
   uint2 scale_r[kNewtonMaxLog + 1];  // Shoup constants of 2^32 / 2^l mod p (undo N and the Montgomery factor)
 };
 
+// X[0, N) <- src[0, len), zero beyond (plain loads: global or shared memory).
+__device__ __forceinline__ void cta_load(uint32_t* X, const uint32_t* src, uint32_t len, uint32_t N, int tid,
+                                         int nt) {
+  for (uint32_t i = tid; i < N; i += nt) X[pad(i)] = i < len ? src[i] : 0u;
+}
+
+// X <- DIT(DIF(X) * Y) over N = 2^logN points, Y a spectrum (Montgomery
+// pointwise; the caller scales by 2^32 / N).  Call after X is loaded and
+// synchronised; returns synchronised.
+__device__ __forceinline__ void cta_mul(uint32_t* X, const uint32_t* Y, int logN, const Ptab& pt, int tid, int nt) {
+  tile_dif(X, logN, 0, pt.fwd, pt.f, tid, nt);
+  __syncthreads();
+  for (uint32_t i = tid; i < (1u << logN); i += nt) X[pad(i)] = mont(X[pad(i)], Y[pad(i)], pt.f);
+  __syncthreads();
+  tile_dit(X, logN, 0, pt.inv, pt.f, tid, nt);
+  __syncthreads();
+}
+
+// One doubling step of the series inverse: Cs[k, want) from Cs[0, k) and the
+// first aw terms of the series (want <= 2k), at N = 2k points: h = -(a c)[k, want),
+// then c[k + i] = (h c)[i].  Y holds c's spectrum afterwards.  gc: optional
+// global copy of the new terms.
+__device__ __forceinline__ void cta_inv_step(const uint32_t* series, uint32_t aw, uint32_t* Cs, uint32_t* gc,
+                                             uint32_t k, uint32_t want, uint32_t* X, uint32_t* Y, uint32_t* H,
+                                             const uint2* scale_r, const Ptab& pt, int tid, int nt) {
+  const Fp f = pt.f;
+  const uint32_t hl = want - k;
+  const int logN = 32 - __clz(2 * k - 1);
+  const uint32_t N = 1u << logN;
+  const uint2 sc = scale_r[logN];
+  cta_load(X, series, aw, N, tid, nt);
+  cta_load(Y, Cs, k, N, tid, nt);
+  __syncthreads();
+  tile_dif(Y, logN, 0, pt.fwd, f, tid, nt);
+  __syncthreads();
+  cta_mul(X, Y, logN, pt, tid, nt);
+  for (uint32_t i = tid; i < hl; i += nt) {
+    const uint32_t v = red(shoup(X[pad(k + i)], sc, f.p), f.p);
+    H[i] = v ? f.p - v : 0u;
+  }
+  __syncthreads();
+  cta_load(X, H, hl, N, tid, nt);
+  __syncthreads();
+  cta_mul(X, Y, logN, pt, tid, nt);
+  for (uint32_t i = tid; i < hl; i += nt) {
+    const uint32_t v = red(shoup(X[pad(i)], sc, f.p), f.p);
+    Cs[k + i] = v;
+    if (gc) gc[k + i] = v;
+  }
+  __syncthreads();
+}
+
 __global__ void __launch_bounds__(kNewtonThreads) k_newton_inv(NewtonInvD d, Ptab pt) {
   pdl_enter();
   extern __shared__ uint32_t smn[];
@@ -508,44 +560,91 @@ __global__ void __launch_bounds__(kNewtonThreads) k_newton_inv(NewtonInvD d, Pta
   }
   __syncthreads();
   for (; k < d.K; k <<= 1) {
-    const uint32_t want = min(2 * k, d.K), hl = want - k;
-    const int logN = 32 - __clz(2 * k - 1);
-    const uint32_t N = 1u << logN;
-    const uint32_t aw = min(d.la, want);
-    const uint2 sc = d.scale_r[logN];
-    for (uint32_t i = tid; i < N; i += nt) {
-      X[pad(i)] = i < aw ? __ldg(d.a + i) : 0u;
-      Y[pad(i)] = i < k ? Cs[i] : 0u;
+    const uint32_t want = min(2 * k, d.K);
+    cta_inv_step(d.a, min(d.la, want), Cs, d.c, k, want, X, Y, H, d.scale_r, pt, tid, nt);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Newton exponential at the small sizes in one CTA (exponential.hpp:107-207):
+// from b = 1, c = 1/b = 1, each step m -> m2 = min(2m, K) extends c to
+// m2 - m terms (inverse doubling on b), then with N = 2m points
+//   t1 = (a' b)[m-1, m2-1),  t2 = (t1 c) mod x^(m2-m) times 1/(m+i),
+//   b[m + i] = (t2 b)[i],
+// the same products as the per-step launches (wrap-free windows at N = 2m).
+// ---------------------------------------------------------------------------
+constexpr int kNewtonExpSmemWords = 3 * kNewtonPW + (1 << kNewtonMaxLog) + 2 * (1 << (kNewtonMaxLog - 1));
+
+struct NewtonExpD {
+  const uint32_t* ap;   // a' (canonical), lap terms
+  uint32_t lap;
+  const uint32_t* tab;  // 1/i in Montgomery form, i < K
+  uint32_t* b;          // exp(a): b[0, K)
+  uint32_t* c;          // 1/b: c[0, cs) on return (cs as the host computes it)
+  uint32_t K;           // <= 2^13
+  uint2 scale_r[kNewtonMaxLog + 1];
+};
+
+__global__ void __launch_bounds__(kNewtonThreads) k_newton_exp(NewtonExpD d, Ptab pt) {
+  pdl_enter();
+  extern __shared__ uint32_t smn[];
+  uint32_t* X = smn;
+  uint32_t* Y = smn + kNewtonPW;
+  uint32_t* S = smn + 2 * kNewtonPW;        // spectrum of b[0, m)
+  uint32_t* B = smn + 3 * kNewtonPW;        // b[0, K)
+  uint32_t* Cs = B + (1 << kNewtonMaxLog);  // c, < 2^12 terms
+  uint32_t* T = Cs + (1 << (kNewtonMaxLog - 1));
+  const int tid = threadIdx.x, nt = blockDim.x;
+  const Fp f = pt.f;
+  if (tid == 0) {
+    B[0] = 1u;
+    Cs[0] = 1u;
+    d.b[0] = 1u;
+  }
+  __syncthreads();
+  uint32_t m = 1, cs = 1;
+  while (m < d.K) {
+    const uint32_t m2 = min(2 * m, d.K), hl = m2 - m;
+    while (cs < hl) {
+      const uint32_t want = min(2 * cs, hl);
+      cta_inv_step(B, min(m, want), Cs, nullptr, cs, want, X, Y, T, d.scale_r, pt, tid, nt);
+      cs = want;
     }
+    const int logN = 32 - __clz(2 * m - 1);
+    const uint32_t N = 1u << logN;
+    const uint2 sc = d.scale_r[logN];
+    // t1 = (a' b)[m-1, m-1+hl)
+    cta_load(X, d.ap, min(d.lap, m2 - 1), N, tid, nt);
+    cta_load(S, B, m, N, tid, nt);
     __syncthreads();
-    tile_dif(X, logN, 0, pt.fwd, f, tid, nt);
+    tile_dif(S, logN, 0, pt.fwd, f, tid, nt);
+    __syncthreads();
+    cta_mul(X, S, logN, pt, tid, nt);
+    for (uint32_t i = tid; i < hl; i += nt) T[i] = red(shoup(X[pad(m - 1 + i)], sc, f.p), f.p);
+    __syncthreads();
+    // t2 = (t1 c) mod x^hl, times 1/(m+i)
+    cta_load(X, T, hl, N, tid, nt);
+    cta_load(Y, Cs, cs, N, tid, nt);
     __syncthreads();
     tile_dif(Y, logN, 0, pt.fwd, f, tid, nt);
     __syncthreads();
-    for (uint32_t i = tid; i < N; i += nt) X[pad(i)] = mont(X[pad(i)], Y[pad(i)], f);
+    cta_mul(X, Y, logN, pt, tid, nt);
+    for (uint32_t i = tid; i < hl; i += nt)
+      T[i] = red(mont(shoup(X[pad(i)], sc, f.p), __ldg(d.tab + m + i), f), f.p);
     __syncthreads();
-    tile_dit(X, logN, 0, pt.inv, f, tid, nt);
+    // b[m + i] = (t2 b)[i]
+    cta_load(X, T, hl, N, tid, nt);
     __syncthreads();
-    for (uint32_t i = tid; i < hl; i += nt) {
-      const uint32_t v = red(shoup(X[pad(k + i)], sc, f.p), f.p);
-      H[i] = v ? f.p - v : 0u;
-    }
-    __syncthreads();
-    for (uint32_t i = tid; i < N; i += nt) X[pad(i)] = i < hl ? H[i] : 0u;
-    __syncthreads();
-    tile_dif(X, logN, 0, pt.fwd, f, tid, nt);
-    __syncthreads();
-    for (uint32_t i = tid; i < N; i += nt) X[pad(i)] = mont(X[pad(i)], Y[pad(i)], f);
-    __syncthreads();
-    tile_dit(X, logN, 0, pt.inv, f, tid, nt);
-    __syncthreads();
+    cta_mul(X, S, logN, pt, tid, nt);
     for (uint32_t i = tid; i < hl; i += nt) {
       const uint32_t v = red(shoup(X[pad(i)], sc, f.p), f.p);
-      Cs[k + i] = v;
-      d.c[k + i] = v;
+      B[m + i] = v;
+      d.b[m + i] = v;
     }
     __syncthreads();
+    m = m2;
   }
+  for (uint32_t i = tid; i < cs; i += nt) d.c[i] = Cs[i];
 }
 
 }  // namespace
@@ -569,6 +668,7 @@ cudaError_t kernels_init() {
   set((const void*)k_small, 2 * padded_words(1 << kSmallLog) * 4);
   set((const void*)k_rows, 2 * padded_words(1 << 13) * 4);
   set((const void*)k_newton_inv, kNewtonSmemWords * 4);
+  set((const void*)k_newton_exp, kNewtonExpSmemWords * 4);
   const cudaError_t r = kernels_fast_init();
   const cudaError_t r2 = kernels_batch_init();
   const cudaError_t r3 = kernels_cyc_init();
@@ -876,6 +976,23 @@ cudaError_t launch_newton_inv(const PrimeTables& pt, const uint32_t* a, size_t l
   d.K = (uint32_t)K;
   for (int l = 0; l <= kNewtonMaxLog; ++l) d.scale_r[l] = shoup_const(l <= pt.small_log ? pt.inv_pow2_r[l] : 0u, pt.p);
   (void)pdl_launch(k_newton_inv, 1, kNewtonThreads, (size_t)kNewtonSmemWords * 4, s, d, dev_tab(pt));
+  return cudaGetLastError();
+}
+
+cudaError_t launch_newton_exp(const PrimeTables& pt, const uint32_t* ap, size_t lap, const uint32_t* tab, uint32_t* b,
+                              uint32_t* c, size_t K, cudaStream_t s) {
+  if (K < 2 || K > (size_t(1) << kNewtonMaxLog) || (size_t(1) << pt.small_log) < K || !(pt.p & 1u) ||
+      pt.p >= (1u << 30))
+    return cudaErrorInvalidValue;
+  NewtonExpD d;
+  d.ap = ap;
+  d.lap = (uint32_t)std::min<size_t>(lap, K);
+  d.tab = tab;
+  d.b = b;
+  d.c = c;
+  d.K = (uint32_t)K;
+  for (int l = 0; l <= kNewtonMaxLog; ++l) d.scale_r[l] = shoup_const(l <= pt.small_log ? pt.inv_pow2_r[l] : 0u, pt.p);
+  (void)pdl_launch(k_newton_exp, 1, kNewtonThreads, (size_t)kNewtonExpSmemWords * 4, s, d, dev_tab(pt));
   return cudaGetLastError();
 }
 

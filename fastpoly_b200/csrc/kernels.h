@@ -146,6 +146,12 @@ cudaError_t launch_seed(int kind, uint32_t p, const uint32_t* a, size_t la, uint
 // c[0] = 1 / a[0], a[0] != 0), all doubling steps in one CTA: needs
 // K <= 2^small_log of pt and K <= 2^newton_inv_max_log().
 int newton_inv_max_log();
+// exp(a) b[0, K) from a' (ap, lap terms) and the Montgomery table 1/i (i < K),
+// every doubling step in one CTA; also leaves 1/b in c[0, cs) with cs from
+// m = 1, cs = 1: while m < K { h = min(2m, K) - m; while cs < h: cs = min(2cs, h); m += h }.
+// Needs K <= 2^small_log of pt and K <= 2^newton_inv_max_log().
+cudaError_t launch_newton_exp(const PrimeTables& pt, const uint32_t* ap, size_t lap, const uint32_t* tab, uint32_t* b,
+                              uint32_t* c, size_t K, cudaStream_t s);
 cudaError_t launch_newton_inv(const PrimeTables& pt, const uint32_t* a, size_t la, uint32_t* c, size_t k0, size_t K,
                               cudaStream_t s);
 // *res = min (mode 0) / max (mode 1) index with a[i] != 0; caller initialises *res.
