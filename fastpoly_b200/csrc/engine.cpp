@@ -965,14 +965,30 @@ void Engine::sqrt(uint32_t p, const uint32_t* a, size_t la, size_t n, uint32_t* 
   const size_t inner = n - half, ulen = la - v;
   const uint32_t* u = a + v;
   uint32_t* b = out + half;
-  const size_t seed = std::min<size_t>(inner, 32);
-  kcheck(launch_seed(2, p, u, std::min(ulen, seed), b, (int)seed, root0, stream_), "sqrt seed");
-  if (inner <= seed) return;
   Buf c(&pool_, inner / 2 + 64);
-  size_t csize = seed / 2;
-  kcheck(launch_seed(0, p, b, seed, c.get(), (int)csize, 0, stream_), "inverse seed");
+  size_t m, csize;
+  if (native(p, newton_inv_max_log())) {
+    // every doubling step up to 2^13 terms (and 1/b alongside) in one CTA
+    const size_t K = std::min(inner, size_t(1) << newton_inv_max_log());
+    kcheck(launch_newton_sqrt(prime_plan(p).t, u, ulen, root0, invm(root0, p), b, c.get(), K, stream_),
+           "newton sqrt");
+    m = K;
+    csize = 1;
+    for (size_t mm = 1; mm < K;) {
+      const size_t h = std::min(2 * mm, K) - mm;
+      while (csize < h) csize = std::min(2 * csize, h);
+      mm += h;
+    }
+  } else {
+    const size_t seed = std::min<size_t>(inner, 32);
+    kcheck(launch_seed(2, p, u, std::min(ulen, seed), b, (int)seed, root0, stream_), "sqrt seed");
+    if (inner <= seed) return;
+    csize = seed / 2;
+    kcheck(launch_seed(0, p, b, seed, c.get(), (int)csize, 0, stream_), "inverse seed");
+    m = seed;
+  }
   const uint32_t half_inv = (p + 1) / 2;
-  for (size_t m = seed; m < inner; m *= 2) {
+  for (; m < inner; m *= 2) {
     const size_t m2 = std::min(2 * m, inner), hlen = m2 - m;
     if (csize < hlen) {
       extend_inverse(p, b, m, c.get(), csize, hlen);

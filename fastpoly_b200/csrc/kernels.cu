@@ -497,6 +497,16 @@ __device__ __forceinline__ void cta_mul(uint32_t* X, const uint32_t* Y, int logN
   __syncthreads();
 }
 
+// X <- DIT(DIF(X)^2) over N = 2^logN points (the caller scales by 2^32 / N).
+__device__ __forceinline__ void cta_mul_self(uint32_t* X, int logN, const Ptab& pt, int tid, int nt) {
+  tile_dif(X, logN, 0, pt.fwd, pt.f, tid, nt);
+  __syncthreads();
+  for (uint32_t i = tid; i < (1u << logN); i += nt) X[pad(i)] = mont(X[pad(i)], X[pad(i)], pt.f);
+  __syncthreads();
+  tile_dit(X, logN, 0, pt.inv, pt.f, tid, nt);
+  __syncthreads();
+}
+
 // One doubling step of the series inverse: Cs[k, want) from Cs[0, k) and the
 // first aw terms of the series (want <= 2k), at N = 2k points: h = -(a c)[k, want),
 // then c[k + i] = (h c)[i].  Y holds c's spectrum afterwards.  gc: optional
@@ -647,6 +657,81 @@ __global__ void __launch_bounds__(kNewtonThreads) k_newton_exp(NewtonExpD d, Pta
   for (uint32_t i = tid; i < cs; i += nt) d.c[i] = Cs[i];
 }
 
+// ---------------------------------------------------------------------------
+// Newton square root at the small sizes in one CTA (square_root.hpp:12-112):
+// from b = root of u[0] and c = 1/b, each step m -> m2 = min(2m, K) extends c
+// to m2 - m terms, then with N = 2m points
+//   t = u[m+i] - (b^2)[m+i],  b[m + i] = (t c)[i] / 2,
+// the same products as the per-step launches (wrap-free windows at N = 2m).
+// ---------------------------------------------------------------------------
+constexpr int kNewtonSqrtSmemWords = 2 * kNewtonPW + (1 << kNewtonMaxLog) + 2 * (1 << (kNewtonMaxLog - 1));
+
+struct NewtonSqrtD {
+  const uint32_t* u;  // the series with u[0] a nonzero square (canonical), ulen terms
+  uint32_t ulen;
+  uint32_t* b;        // sqrt(u): b[0, K)
+  uint32_t* c;        // 1/b: c[0, cs) on return (cs as for the exponential)
+  uint32_t K;         // <= 2^13
+  uint32_t root, root_inv;  // b[0] and 1/b[0]
+  uint2 scale_r[kNewtonMaxLog + 1];
+};
+
+__global__ void __launch_bounds__(kNewtonThreads) k_newton_sqrt(NewtonSqrtD d, Ptab pt) {
+  pdl_enter();
+  extern __shared__ uint32_t smn[];
+  uint32_t* X = smn;
+  uint32_t* Y = smn + kNewtonPW;
+  uint32_t* B = smn + 2 * kNewtonPW;        // b[0, K)
+  uint32_t* Cs = B + (1 << kNewtonMaxLog);  // c, < 2^12 terms
+  uint32_t* T = Cs + (1 << (kNewtonMaxLog - 1));
+  const int tid = threadIdx.x, nt = blockDim.x;
+  const Fp f = pt.f;
+  if (tid == 0) {
+    B[0] = d.root;
+    Cs[0] = d.root_inv;
+    d.b[0] = d.root;
+  }
+  __syncthreads();
+  uint32_t m = 1, cs = 1;
+  while (m < d.K) {
+    const uint32_t m2 = min(2 * m, d.K), hl = m2 - m;
+    while (cs < hl) {
+      const uint32_t want = min(2 * cs, hl);
+      cta_inv_step(B, min(m, want), Cs, nullptr, cs, want, X, Y, T, d.scale_r, pt, tid, nt);
+      cs = want;
+    }
+    const int logN = 32 - __clz(2 * m - 1);
+    const uint32_t N = 1u << logN;
+    const uint2 sc = d.scale_r[logN];
+    // t = u[m + i] - (b^2)[m + i]
+    cta_load(X, B, m, N, tid, nt);
+    __syncthreads();
+    cta_mul_self(X, logN, pt, tid, nt);
+    for (uint32_t i = tid; i < hl; i += nt) {
+      const uint32_t v = red(shoup(X[pad(m + i)], sc, f.p), f.p);
+      const uint32_t su = m + i < d.ulen ? d.u[m + i] : 0u;
+      T[i] = su >= v ? su - v : su + f.p - v;
+    }
+    __syncthreads();
+    // b[m + i] = (t c)[i] / 2
+    cta_load(X, T, hl, N, tid, nt);
+    cta_load(Y, Cs, cs, N, tid, nt);
+    __syncthreads();
+    tile_dif(Y, logN, 0, pt.fwd, f, tid, nt);
+    __syncthreads();
+    cta_mul(X, Y, logN, pt, tid, nt);
+    for (uint32_t i = tid; i < hl; i += nt) {
+      const uint32_t v = red(shoup(X[pad(i)], sc, f.p), f.p);
+      const uint32_t h = (v & 1u) ? (v + f.p) >> 1 : v >> 1;  // v / 2 mod p (p odd)
+      B[m + i] = h;
+      d.b[m + i] = h;
+    }
+    __syncthreads();
+    m = m2;
+  }
+  for (uint32_t i = tid; i < cs; i += nt) d.c[i] = Cs[i];
+}
+
 }  // namespace
 
 namespace fpx {
@@ -669,6 +754,7 @@ cudaError_t kernels_init() {
   set((const void*)k_rows, 2 * padded_words(1 << 13) * 4);
   set((const void*)k_newton_inv, kNewtonSmemWords * 4);
   set((const void*)k_newton_exp, kNewtonExpSmemWords * 4);
+  set((const void*)k_newton_sqrt, kNewtonSqrtSmemWords * 4);
   const cudaError_t r = kernels_fast_init();
   const cudaError_t r2 = kernels_batch_init();
   const cudaError_t r3 = kernels_cyc_init();
@@ -993,6 +1079,24 @@ cudaError_t launch_newton_exp(const PrimeTables& pt, const uint32_t* ap, size_t 
   d.K = (uint32_t)K;
   for (int l = 0; l <= kNewtonMaxLog; ++l) d.scale_r[l] = shoup_const(l <= pt.small_log ? pt.inv_pow2_r[l] : 0u, pt.p);
   (void)pdl_launch(k_newton_exp, 1, kNewtonThreads, (size_t)kNewtonExpSmemWords * 4, s, d, dev_tab(pt));
+  return cudaGetLastError();
+}
+
+cudaError_t launch_newton_sqrt(const PrimeTables& pt, const uint32_t* u, size_t ulen, uint32_t root, uint32_t root_inv,
+                               uint32_t* b, uint32_t* c, size_t K, cudaStream_t s) {
+  if (K < 1 || K > (size_t(1) << kNewtonMaxLog) || (size_t(1) << pt.small_log) < K || !(pt.p & 1u) ||
+      pt.p >= (1u << 30))
+    return cudaErrorInvalidValue;
+  NewtonSqrtD d;
+  d.u = u;
+  d.ulen = (uint32_t)std::min<size_t>(ulen, K);
+  d.b = b;
+  d.c = c;
+  d.K = (uint32_t)K;
+  d.root = root;
+  d.root_inv = root_inv;
+  for (int l = 0; l <= kNewtonMaxLog; ++l) d.scale_r[l] = shoup_const(l <= pt.small_log ? pt.inv_pow2_r[l] : 0u, pt.p);
+  (void)pdl_launch(k_newton_sqrt, 1, kNewtonThreads, (size_t)kNewtonSqrtSmemWords * 4, s, d, dev_tab(pt));
   return cudaGetLastError();
 }
 

@@ -150,6 +150,10 @@ int newton_inv_max_log();
 // every doubling step in one CTA; also leaves 1/b in c[0, cs) with cs from
 // m = 1, cs = 1: while m < K { h = min(2m, K) - m; while cs < h: cs = min(2cs, h); m += h }.
 // Needs K <= 2^small_log of pt and K <= 2^newton_inv_max_log().
+// sqrt(u) b[0, K) with b[0] = root (1/root = root_inv), every doubling step in
+// one CTA; leaves 1/b in c[0, cs) with cs as for launch_newton_exp.
+cudaError_t launch_newton_sqrt(const PrimeTables& pt, const uint32_t* u, size_t ulen, uint32_t root, uint32_t root_inv,
+                               uint32_t* b, uint32_t* c, size_t K, cudaStream_t s);
 cudaError_t launch_newton_exp(const PrimeTables& pt, const uint32_t* ap, size_t lap, const uint32_t* tab, uint32_t* b,
                               uint32_t* c, size_t K, cudaStream_t s);
 cudaError_t launch_newton_inv(const PrimeTables& pt, const uint32_t* a, size_t la, uint32_t* c, size_t k0, size_t K,
