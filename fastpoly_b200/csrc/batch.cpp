@@ -414,16 +414,26 @@ void Engine::batch(fpx_job* jobs, size_t count) {
     }
   }
 
-  // ---- convolutions: one flush
+  // ---- convolutions: one flush per output-size class, largest first, so the
+  // GPU works through the big products while the host records the small ones
+  // (recording all of them before the first launch left the GPU idle for the
+  // whole recording time)
   {
-    BatchRec rec(*this);
-    for (size_t i = 0; i < count; ++i) {
-      if (route[i] != kConv) continue;
-      const fpx_job& j = jobs[i];
-      rec.product(j.p, j.a, std::min(j.la, j.n), j.b, std::min(j.lb, j.n), 0, conv_len[i], j.out, 0, nullptr,
-                  false);
+    std::vector<size_t> order;
+    for (size_t i = 0; i < count; ++i)
+      if (route[i] == kConv) order.push_back(i);
+    auto cls = [&](size_t i) { return std::bit_width(conv_len[i]); };
+    std::stable_sort(order.begin(), order.end(), [&](size_t x, size_t y) { return cls(x) > cls(y); });
+    for (size_t k = 0; k < order.size();) {
+      BatchRec rec(*this);
+      const int c = cls(order[k]);
+      for (; k < order.size() && cls(order[k]) == c; ++k) {
+        const fpx_job& j = jobs[order[k]];
+        rec.product(j.p, j.a, std::min(j.la, j.n), j.b, std::min(j.lb, j.n), 0, conv_len[order[k]], j.out, 0,
+                    nullptr, false);
+      }
+      rec.flush();
     }
-    rec.flush();
   }
 
   // ---- series: scratch, preparation, seeds

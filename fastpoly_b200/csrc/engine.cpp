@@ -57,7 +57,27 @@ uint32_t primitive_root(uint32_t p) {
   return 0;
 }
 
+namespace {
+bool is_prime_mr(uint32_t n);
+}  // namespace
+
+// Batches check the modulus of every job, a handful of distinct primes over
+// thousands of jobs: the last few answers are kept per thread.
 bool is_prime(uint32_t n) {
+  thread_local uint32_t seen[8] = {};
+  thread_local bool ans[8] = {};
+  thread_local int next = 0;
+  for (int i = 0; i < 8; ++i)
+    if (seen[i] == n && n) return ans[i];
+  const bool r = is_prime_mr(n);
+  seen[next] = n;
+  ans[next] = r;
+  next = (next + 1) & 7;
+  return r;
+}
+
+namespace {
+bool is_prime_mr(uint32_t n) {
   if (n < 2) return false;
   for (uint32_t q : {2u, 3u, 5u, 7u, 11u, 13u})
     if (n % q == 0) return n == q;
@@ -76,6 +96,7 @@ bool is_prime(uint32_t n) {
   }
   return true;
 }
+}  // namespace
 
 // modint.hpp:139-166, the reference's root choice (Tonelli-Shanks, z from 2).
 bool sqrt_mod(uint32_t x, uint32_t p, uint32_t* out) {
