@@ -1617,11 +1617,18 @@ struct ColTable<ColK<R, A, B>...> {
 };
 template <int L>
 using ColD = ColK<L, col_logw(L), col_logw(L)>;
-// Default widths for every R; for R = 2^9 .. 2^12 (transforms of 2^21 .. 2^24
-// points, whose grids span several waves) also half-width tiles and the split
-// grids the tuner chooses from.  Narrow tiles keep 2^LW >= 4 columns below
+// Default widths for every R, and narrower tiles the tuner chooses from: for
+// R <= 2^8 (transforms of at most 2^20 points, grids below one wave) tiles of
+// 1/2, 1/4 and 1/8 the default width, more CTAs with less work each; for
+// R = 2^9 .. 2^12 (2^21 .. 2^24 points, grids of several waves) half-width
+// tiles and the split grids.  Narrow tiles keep 2^LW >= 4 columns below
 // R = 2^12: at two columns the swizzle leaves 4-way bank conflicts there.
-using Cols = ColTable<ColD<2>, ColD<3>, ColD<4>, ColD<5>, ColD<6>, ColD<7>, ColD<8>,
+template <int L, int K>
+using ColN = ColK<L, col_logw(L) - K, col_logw(L) - K>;
+using Cols = ColTable<ColD<2>, ColN<2, 1>, ColN<2, 2>, ColN<2, 3>, ColD<3>, ColN<3, 1>, ColN<3, 2>, ColN<3, 3>,
+                      ColD<4>, ColN<4, 1>, ColN<4, 2>, ColN<4, 3>, ColD<5>, ColN<5, 1>, ColN<5, 2>, ColN<5, 3>,
+                      ColD<6>, ColN<6, 1>, ColN<6, 2>, ColN<6, 3>, ColD<7>, ColN<7, 1>, ColN<7, 2>, ColN<7, 3>,
+                      ColD<8>, ColN<8, 1>, ColN<8, 2>, ColN<8, 3>,
                       ColD<9>, ColK<9, 3, 3>, ColK<9, 4, 3>, ColK<9, 4, 2>,
                       ColD<10>, ColK<10, 2, 2>, ColK<10, 3, 2>,
                       ColD<11>, ColK<11, 2, 2>, ColK<11, 3, 2>,

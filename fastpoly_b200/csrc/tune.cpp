@@ -45,7 +45,7 @@ ShapeStore& store() {
   return s;
 }
 
-bool tunable(const BigTables& bt) { return bt.logC == 12 && bt.logR >= 9 && bt.logR <= 12; }
+bool tunable(const BigTables& bt) { return bt.logC == 12 && bt.logR >= 2 && bt.logR <= 12; }
 
 bool autotune_on() {
   const char* e = std::getenv("FPX_AUTOTUNE");

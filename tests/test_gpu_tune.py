@@ -41,7 +41,7 @@ def _run_all(ctx, log_n, rng_seed):
     return c, sq, fx, ix
 
 
-@pytest.mark.parametrize("log_n", [21, 22, 23, 24])
+@pytest.mark.parametrize("log_n", [14, 16, 18, 20, 21, 22, 23, 24])
 def test_every_shape_same_values(ctx, log_n):
     kinds = (F.COL_FWD1, F.COL_FWD2, F.COL_INV)
     cands = {k: ctx.col_shape_candidates(log_n, k) for k in kinds}
