@@ -256,16 +256,16 @@ void Engine::count_batch(const BatchPlan& b) {
   for (const XJob& j : b.xjobs) sizes.push_back(j.logN);
   std::sort(sizes.begin(), sizes.end());
   sizes.erase(std::unique(sizes.begin(), sizes.end()), sizes.end());
-  for (int s : sizes) launches_ += s <= small_kernel_max_log() ? 1 : 3;
-  launches_ += (b.direct.empty() ? 0 : 1) + (b.garner.empty() ? 0 : 1);
+  uint64_t n = (b.direct.empty() ? 0 : 1) + (b.garner.empty() ? 0 : 1);
+  for (int s : sizes) n += s <= small_kernel_max_log() ? 1 : 3;
+  if (n) launches_ += n - 1;  // the flush's prof_end counted one
 }
 
 void Engine::gather_first(const std::vector<const uint32_t*>& ptrs, uint32_t* host_out) {
   Stage& st = stage(ptrs.size() * 12 + 512);
   prof_begin();
   check(launch_gather_first(ptrs, st.host, st.dev.get(), host_out, stream_), "gather");
-  prof_end("gather");
-  ++launches_;
+  prof_end("gather");  // counts the launch
   sync();
 }
 
@@ -330,7 +330,9 @@ void Engine::ext_phase2(BatchRec& rec, const ExtJob& j) {
 // ------------------------------------------------------------------ batch
 
 namespace {
-enum Route : uint8_t { kNone, kConv, kInv, kLog, kExp, kSingle };
+// kInvF / kExpF: inverse / exp on a transform prime up to 2^13 terms, one CTA
+// per job in one launch (k_newton_b); kInv / kExp: the lockstep doubling loop.
+enum Route : uint8_t { kNone, kConv, kInv, kLog, kExp, kSingle, kInvF, kExpF };
 }
 
 void Engine::batch(fpx_job* jobs, size_t count) {
@@ -410,7 +412,11 @@ void Engine::batch(fpx_job* jobs, size_t count) {
         j.status = FPX_EDOMAIN;
         j.out_len = 0;
         route[i] = kNone;
+        continue;
       }
+      const bool small = native(p, newton_inv_max_log()) && j.n <= (size_t(1) << newton_inv_max_log());
+      if (small && route[i] == kInv) route[i] = kInvF;
+      if (small && route[i] == kExp && std::min(j.la, j.n) > 1 && j.n > 1) route[i] = kExpF;
     }
   }
 
@@ -464,6 +470,11 @@ void Engine::batch(fpx_job* jobs, size_t count) {
     const fpx_job& j = jobs[i];
     const size_t n = j.n, cnt = std::min(j.la, n);
     if (route[i] == kInv) words += round64(2 * n) + round64(n);
+    if (route[i] == kExpF) {
+      words += round64(n) + round64(n / 2 + 64);
+      size_t& t = tab_need[j.p];
+      t = std::max(t, n - 1);
+    }
     if (route[i] == kLog && cnt > 1) {
       words += 3 * round64(n) + round64(2 * n);
       size_t& t = tab_need[j.p];
@@ -478,7 +489,8 @@ void Engine::batch(fpx_job* jobs, size_t count) {
     }
   }
   bool any_series = false;
-  for (size_t i = 0; i < count; ++i) any_series |= route[i] == kInv || route[i] == kLog || route[i] == kExp;
+  for (size_t i = 0; i < count; ++i)
+    any_series |= route[i] == kInv || route[i] == kLog || route[i] == kExp || route[i] == kInvF || route[i] == kExpF;
   if (any_series) {
     for (auto& [p, need] : tab_need) inv_table(p, need);  // grow once per prime, before any pointer is kept
     Buf arena(&pool_, words ? words : 1);
@@ -490,10 +502,18 @@ void Engine::batch(fpx_job* jobs, size_t count) {
     };
     std::vector<ExpPrep> preps;
     std::vector<SeedJob> seeds1, seeds2;
+    std::vector<NewtonJob> fused;
     for (size_t i = 0; i < count; ++i) {
       fpx_job& j = jobs[i];
       const size_t n = j.n, cnt = std::min(j.la, n);
-      if (route[i] == kInv) {
+      if (route[i] == kInvF) {
+        fused.push_back(NewtonJob{0, &prime_plan(j.p).t, j.a, cnt, nullptr, j.out, nullptr, n});
+      } else if (route[i] == kExpF) {
+        uint32_t* ap = take(n);
+        preps.push_back(ExpPrep{j.p, j.a, cnt, ap, j.out, n});  // a' (and out = 1, 0, ...)
+        fused.push_back(NewtonJob{1, &prime_plan(j.p).t, ap, cnt - 1, inv_table(j.p, n - 1), j.out,
+                                  take(n / 2 + 64), n});
+      } else if (route[i] == kInv) {
         InvT t{j.p, j.a, cnt, n, j.out, take(2 * n), take(n)};
         invs.push_back(t);
         seeds1.push_back(SeedJob{0, j.p, j.a, cnt, j.out, (int)std::min<size_t>(n, 32), 0});
@@ -542,21 +562,57 @@ void Engine::batch(fpx_job* jobs, size_t count) {
       prof_begin();
       check(launch_exp_prep_batch(preps, st.host, st.dev.get(), stream_, st.ev), "prep");
       prof_end("prep");
-      ++launches_;
+    }
+    // the one-CTA Newton jobs depend on nothing the lockstep loop computes:
+    // they run on the side stream, joined back before the arena is released
+    // (their descriptors get a device buffer of their own: the staging ring's
+    // device slots are reused in stream_ order, which the side stream does not follow)
+    const bool side = !fused.empty() && !prof_on_;
+    Buf fdesc;
+    // joins the side stream back into stream_ before fdesc and the arena go back
+    // to the pool, also when an error unwinds this block
+    struct SideJoin {
+      Engine& e;
+      bool active = false;
+      void join() {
+        if (!active) return;
+        active = false;
+        e.check(cudaEventRecord(e.side_join_, e.side_), "cudaEventRecord");
+        e.check(cudaStreamWaitEvent(e.stream_, e.side_join_, 0), "cudaStreamWaitEvent");
+      }
+      ~SideJoin() {
+        if (active) {
+          cudaEventRecord(e.side_join_, e.side_);
+          cudaStreamWaitEvent(e.stream_, e.side_join_, 0);
+        }
+      }
+    } side_join{*this};
+    if (!fused.empty()) {
+      Stage& st = stage(batch_newton_bytes(fused.size()));
+      fdesc = Buf(&pool_, batch_newton_bytes(fused.size()) / 4 + 1);
+      if (side) {
+        check(cudaEventRecord(side_fork_, stream_), "cudaEventRecord");
+        check(cudaStreamWaitEvent(side_, side_fork_, 0), "cudaStreamWaitEvent");
+        side_join.active = true;
+        check(launch_newton_batch(fused, st.host, fdesc.get(), side_, st.ev), "newton");
+        ++launches_;
+      } else {
+        prof_begin();
+        check(launch_newton_batch(fused, st.host, fdesc.get(), stream_, st.ev), "newton");
+        prof_end("newton");
+      }
     }
     if (!seeds1.empty()) {
       Stage& st = stage(batch_aux_bytes(seeds1.size()));
       prof_begin();
       check(launch_seeds_batch(seeds1, st.host, st.dev.get(), stream_, st.ev), "seed");
       prof_end("seed");
-      ++launches_;
     }
     if (!seeds2.empty()) {
       Stage& st = stage(batch_aux_bytes(seeds2.size()));
       prof_begin();
       check(launch_seeds_batch(seeds2, st.host, st.dev.get(), stream_, st.ev), "seed");
       prof_end("seed");
-      ++launches_;
     }
 
     // ---- lockstep doubling
@@ -644,6 +700,8 @@ void Engine::batch(fpx_job* jobs, size_t count) {
       }
       r5.flush();
     }
+
+    side_join.join();
 
     // ---- log: integral(a' * inv(a)) (exponential.hpp:92-97)
     if (!logs.empty()) {

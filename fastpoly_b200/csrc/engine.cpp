@@ -266,6 +266,9 @@ Engine::Engine(int device, size_t pool_limit) : device_(device), pool_(pool_limi
   check(cudaMallocHost(&host_ull_, 16), "cudaMallocHost");
   check(cudaMallocHost(&host_one_, 4), "cudaMallocHost");
   *host_one_ = 1;
+  check(cudaStreamCreateWithFlags(&side_, cudaStreamNonBlocking), "cudaStreamCreate");
+  check(cudaEventCreateWithFlags(&side_fork_, cudaEventDisableTiming), "cudaEventCreate");
+  check(cudaEventCreateWithFlags(&side_join_, cudaEventDisableTiming), "cudaEventCreate");
   const char* g = std::getenv("FPX_GRAPHS");
   graphs_on_ = !(g && g[0] == '0');
 }
@@ -275,6 +278,12 @@ Engine::~Engine() {
   if (stream_) cudaStreamSynchronize(stream_);
   drop_graphs();
   if (host_one_) cudaFreeHost(host_one_);
+  if (side_) {
+    cudaStreamSynchronize(side_);
+    cudaStreamDestroy(side_);
+  }
+  if (side_fork_) cudaEventDestroy(side_fork_);
+  if (side_join_) cudaEventDestroy(side_join_);
   primes_.clear();
   bigs_.clear();
   inv_tabs_.clear();

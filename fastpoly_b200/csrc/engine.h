@@ -201,6 +201,10 @@ class Engine {
   std::map<GraphKey, GraphEntry> graphs_;
   std::set<GraphKey> graph_seen_;
   uint32_t* host_one_ = nullptr;  // pinned constant 1 (capturable host->device copy)
+  // Side stream for independent batch work (the one-CTA Newton jobs run there
+  // beside the lockstep loop); joined back into stream_ by events.
+  cudaStream_t side_ = nullptr;
+  cudaEvent_t side_fork_ = nullptr, side_join_ = nullptr;
 
   // ---- transform compositions
   struct CycOp {

@@ -541,8 +541,7 @@ __device__ __forceinline__ void cta_inv_step(const uint32_t* series, uint32_t aw
   __syncthreads();
 }
 
-__global__ void __launch_bounds__(kNewtonThreads) k_newton_inv(NewtonInvD d, Ptab pt) {
-  pdl_enter();
+__device__ __forceinline__ void newton_inv_body(const NewtonInvD& d, const Ptab& pt) {
   extern __shared__ uint32_t smn[];
   uint32_t* X = smn;                      // transform buffer, padded
   uint32_t* Y = smn + kNewtonPW;          // spectrum of c[0, k), padded
@@ -575,6 +574,11 @@ __global__ void __launch_bounds__(kNewtonThreads) k_newton_inv(NewtonInvD d, Pta
   }
 }
 
+__global__ void __launch_bounds__(kNewtonThreads) k_newton_inv(NewtonInvD d, Ptab pt) {
+  pdl_enter();
+  newton_inv_body(d, pt);
+}
+
 // ---------------------------------------------------------------------------
 // Newton exponential at the small sizes in one CTA (exponential.hpp:107-207):
 // from b = 1, c = 1/b = 1, each step m -> m2 = min(2m, K) extends c to
@@ -595,8 +599,7 @@ struct NewtonExpD {
   uint2 scale_r[kNewtonMaxLog + 1];
 };
 
-__global__ void __launch_bounds__(kNewtonThreads) k_newton_exp(NewtonExpD d, Ptab pt) {
-  pdl_enter();
+__device__ __forceinline__ void newton_exp_body(const NewtonExpD& d, const Ptab& pt) {
   extern __shared__ uint32_t smn[];
   uint32_t* X = smn;
   uint32_t* Y = smn + kNewtonPW;
@@ -655,6 +658,25 @@ __global__ void __launch_bounds__(kNewtonThreads) k_newton_exp(NewtonExpD d, Pta
     m = m2;
   }
   for (uint32_t i = tid; i < cs; i += nt) d.c[i] = Cs[i];
+}
+
+__global__ void __launch_bounds__(kNewtonThreads) k_newton_exp(NewtonExpD d, Ptab pt) {
+  pdl_enter();
+  newton_exp_body(d, pt);
+}
+
+// Many small Newton inverses and exponentials (batches), one CTA per job.
+struct NewtonJobB {
+  int kind;  // 0 inverse, 1 exponential
+  Ptab pt;
+  NewtonInvD inv;
+  NewtonExpD exp;
+};
+__global__ void __launch_bounds__(kNewtonThreads) k_newton_b(const NewtonJobB* __restrict__ jobs) {
+  pdl_enter();
+  const NewtonJobB& j = jobs[blockIdx.x];
+  if (j.kind == 0) newton_inv_body(j.inv, j.pt);
+  else newton_exp_body(j.exp, j.pt);
 }
 
 // ---------------------------------------------------------------------------
@@ -754,6 +776,7 @@ cudaError_t kernels_init() {
   set((const void*)k_rows, 2 * padded_words(1 << 13) * 4);
   set((const void*)k_newton_inv, kNewtonSmemWords * 4);
   set((const void*)k_newton_exp, kNewtonExpSmemWords * 4);
+  set((const void*)k_newton_b, kNewtonExpSmemWords * 4);
   set((const void*)k_newton_sqrt, kNewtonSqrtSmemWords * 4);
   const cudaError_t r = kernels_fast_init();
   const cudaError_t r2 = kernels_batch_init();
@@ -1079,6 +1102,57 @@ cudaError_t launch_newton_exp(const PrimeTables& pt, const uint32_t* ap, size_t 
   d.K = (uint32_t)K;
   for (int l = 0; l <= kNewtonMaxLog; ++l) d.scale_r[l] = shoup_const(l <= pt.small_log ? pt.inv_pow2_r[l] : 0u, pt.p);
   (void)pdl_launch(k_newton_exp, 1, kNewtonThreads, (size_t)kNewtonExpSmemWords * 4, s, d, dev_tab(pt));
+  return cudaGetLastError();
+}
+
+namespace {
+void fill_newton_inv(NewtonInvD& d, const PrimeTables& pt, const uint32_t* a, size_t la, uint32_t* c, size_t K) {
+  d.a = a;
+  d.la = (uint32_t)std::min<size_t>(la, K);
+  d.c = c;
+  d.k0 = 0;
+  d.K = (uint32_t)K;
+  d.r1 = (uint32_t)((uint64_t(1) << 32) % pt.p);
+  d.r2 = (uint32_t)((uint64_t)d.r1 * d.r1 % pt.p);
+  for (int l = 0; l <= kNewtonMaxLog; ++l) d.scale_r[l] = shoup_const(l <= pt.small_log ? pt.inv_pow2_r[l] : 0u, pt.p);
+}
+void fill_newton_exp(NewtonExpD& d, const PrimeTables& pt, const uint32_t* ap, size_t lap, const uint32_t* tab,
+                     uint32_t* b, uint32_t* c, size_t K) {
+  d.ap = ap;
+  d.lap = (uint32_t)std::min<size_t>(lap, K);
+  d.tab = tab;
+  d.b = b;
+  d.c = c;
+  d.K = (uint32_t)K;
+  for (int l = 0; l <= kNewtonMaxLog; ++l) d.scale_r[l] = shoup_const(l <= pt.small_log ? pt.inv_pow2_r[l] : 0u, pt.p);
+}
+}  // namespace
+
+size_t batch_newton_bytes(size_t jobs) { return jobs * sizeof(NewtonJobB) + 256; }
+
+cudaError_t launch_newton_batch(const std::vector<NewtonJob>& jobs, void* host_staging, void* dev_desc,
+                                cudaStream_t s, cudaEvent_t staged) {
+  if (jobs.empty()) return cudaSuccess;
+  std::vector<NewtonJobB> v(jobs.size());
+  for (size_t i = 0; i < jobs.size(); ++i) {
+    const NewtonJob& x = jobs[i];
+    const PrimeTables& pt = *x.pt;
+    if (x.K < 1 || x.K > (size_t(1) << kNewtonMaxLog) || (size_t(1) << pt.small_log) < x.K || !(pt.p & 1u) ||
+        pt.p >= (1u << 30) || (x.kind == 1 && x.K < 2))
+      return cudaErrorInvalidValue;
+    NewtonJobB& j = v[i];
+    std::memset(&j, 0, sizeof j);
+    j.kind = x.kind;
+    j.pt = dev_tab(pt);
+    if (x.kind == 0) fill_newton_inv(j.inv, pt, x.a, x.la, x.out, x.K);
+    else fill_newton_exp(j.exp, pt, x.a, x.la, x.tab, x.out, x.c, x.K);
+  }
+  std::memcpy(host_staging, v.data(), v.size() * sizeof(NewtonJobB));
+  cudaError_t e = cudaMemcpyAsync(dev_desc, host_staging, v.size() * sizeof(NewtonJobB), cudaMemcpyHostToDevice, s);
+  if (e != cudaSuccess) return e;
+  if (staged && (e = cudaEventRecord(staged, s)) != cudaSuccess) return e;
+  (void)pdl_launch(k_newton_b, (unsigned)v.size(), kNewtonThreads, (size_t)kNewtonExpSmemWords * 4, s,
+                   static_cast<const NewtonJobB*>(dev_desc));
   return cudaGetLastError();
 }
 

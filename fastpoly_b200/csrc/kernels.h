@@ -2,6 +2,8 @@
 // Only plain types cross this header; the engine (engine.cpp) composes them.
 #pragma once
 #include <cstdint>
+#include <vector>
+
 #include <cuda_runtime.h>
 
 namespace fpx {
@@ -154,6 +156,22 @@ int newton_inv_max_log();
 // one CTA; leaves 1/b in c[0, cs) with cs as for launch_newton_exp.
 cudaError_t launch_newton_sqrt(const PrimeTables& pt, const uint32_t* u, size_t ulen, uint32_t root, uint32_t root_inv,
                                uint32_t* b, uint32_t* c, size_t K, cudaStream_t s);
+// Many Newton inverses (kind 0: out = 1/a to K terms, a with la terms) and
+// exponentials (kind 1: out = exp with a = a' of la terms, tab = 1/i Montgomery,
+// c scratch of K/2 words) up to K <= 2^13 terms, one CTA per job, one launch.
+struct NewtonJob {
+  int kind;
+  const PrimeTables* pt;
+  const uint32_t* a;
+  size_t la;
+  const uint32_t* tab;
+  uint32_t* out;
+  uint32_t* c;
+  size_t K;
+};
+size_t batch_newton_bytes(size_t jobs);
+cudaError_t launch_newton_batch(const std::vector<NewtonJob>& jobs, void* host_staging, void* dev_desc,
+                                cudaStream_t s, cudaEvent_t staged = nullptr);
 cudaError_t launch_newton_exp(const PrimeTables& pt, const uint32_t* ap, size_t lap, const uint32_t* tab, uint32_t* b,
                               uint32_t* c, size_t K, cudaStream_t s);
 cudaError_t launch_newton_inv(const PrimeTables& pt, const uint32_t* a, size_t la, uint32_t* c, size_t k0, size_t K,
