@@ -11,7 +11,9 @@ seeded uniform residues.  Metric: output Mcoeff/s.
          launching stream around each step, L2 flushed (512 MiB write) between
          steps outside the events; whole-job (all ranks) coefficients / max time.
 `e2e`    the same metric through the public host-buffer C ABI (fpx_conv) from
-         pinned host memory: H2D of both inputs and D2H of the product per step.
+         pinned host memory: H2D of both inputs and D2H of the product per step,
+         --e2e-callers host threads (default 4, one context each) calling back
+         to back, as the reference baseline runs concurrent calls.
 `roofline` the dominant kernel's algorithmic bytes per launch / its average
          CUDA-event duration measured over the timed region, against the
          measured HBM copy bandwidth.
@@ -273,20 +275,44 @@ def run_fpx(args):
     launches = ctx.launch_count() - launches0
     total_ms = float(sum(step_ms))
 
-    # e2e through the host-buffer C ABI from pinned memory
-    pa = torch.from_numpy(a.view(np.int32)).pin_memory().numpy().view(np.uint32)
-    pb = torch.from_numpy(b.view(np.int32)).pin_memory().numpy().view(np.uint32)
-    po = torch.empty(N_OUT, dtype=torch.int32).pin_memory().numpy().view(np.uint32)
-    ctx.conv(P, pa, pb, out=po)
+    # e2e through the host-buffer C ABI from pinned memory: `callers` host
+    # threads, each with its own context and pinned buffers, call fpx_conv
+    # back to back (like the reference baseline's concurrent calls); one
+    # caller's upload overlaps another's download on the full-duplex link
+    import threading
+    callers = max(1, args.e2e_callers)
     e2e_steps = max(3, min(args.steps, 50))
+    e2e_steps += (-e2e_steps) % callers
+    pinned = []
+    ctxs = [ctx] + [F.Context(local) for _ in range(callers - 1)]
+    for c in ctxs:
+        pa = torch.from_numpy(a.view(np.int32)).pin_memory().numpy().view(np.uint32)
+        pb = torch.from_numpy(b.view(np.int32)).pin_memory().numpy().view(np.uint32)
+        po = torch.empty(N_OUT, dtype=torch.int32).pin_memory().numpy().view(np.uint32)
+        c.conv(P, pa, pb, out=po)
+        pinned.append((c, pa, pb, po))
+    go = threading.Barrier(callers + 1)
+
+    def caller(c, pa, pb, po):
+        go.wait()
+        for _ in range(e2e_steps // callers):
+            c.conv(P, pa, pb, out=po)
+
+    threads = [threading.Thread(target=caller, args=t) for t in pinned]
+    for t in threads:
+        t.start()
     if dist:
         dist.barrier()
     t0 = time.perf_counter()
-    for _ in range(e2e_steps):
-        ctx.conv(P, pa, pb, out=po)
+    go.wait()
+    for t in threads:
+        t.join()
     e2e_s = time.perf_counter() - t0
     clk = clocks.stop()
-    assert int(po[0]) == want0
+    for _, _, _, po in pinned:
+        assert int(po[0]) == want0
+    for c in ctxs[1:]:
+        c.close()
 
     total_ms, e2e_s = max_over_ranks(dist, [total_ms, e2e_s], device="cuda")
     ms_per_step, value, e2e_value = whole_job_rates(world, args.steps, total_ms, e2e_steps, e2e_s)
@@ -326,8 +352,8 @@ def run_fpx(args):
                 "config": {"workload": WORKLOAD, "p": P, "n_in": N_IN, "n_out": N_OUT, "transform_points": N_FFT,
                            "parallelism": f"replicas x{world}", "l2": "flushed between steps (512 MiB write)"},
                 "e2e": {"value": round(e2e_value, 1), "unit": "Mcoeff/s", "h2d_bytes_per_step": 2 * N_IN * 4,
-                        "d2h_bytes_per_step": N_OUT * 4, "steps": e2e_steps,
-                        "api": "fpx_conv (host buffers, pinned)"},
+                        "d2h_bytes_per_step": N_OUT * 4, "steps": e2e_steps, "callers": callers,
+                        "api": f"fpx_conv (host buffers, pinned), {callers} concurrent callers, one context each"},
                 "gpu_launches": int(launches), "roofline": roof, "clocks": clk}
         if world == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_reference_sample(reps=3)
@@ -849,6 +875,8 @@ def main():
     ap.add_argument("--workers", type=int, default=2, help="serve: micro-batches in flight")
     ap.add_argument("--clients", type=int, default=32, help="serve: callers of the closed-loop saturation run")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--e2e-callers", type=int, default=4,
+                    help="conv: concurrent host threads (one context each) of the end-to-end measurement")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.workload == "batch":
