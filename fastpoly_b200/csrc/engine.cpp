@@ -713,11 +713,75 @@ void Engine::product(uint32_t p, const uint32_t* a, size_t la, const uint32_t* b
 // (:132-182): block pairs of at most 2^23 terms, each an exact integer product
 // modulo 1, 2 or 3 auxiliary primes (lifted on load) and a Garner epilogue
 // accumulating into the target field.
+// Blocked CRT product with every block transformed once (crt_convolution.hpp
+// multiplies the 2^23-term blocks pairwise).  Per auxiliary prime: the spectra
+// of all blocks of a and b at N = 2^24, then for every output block s the sum
+// of SA_i * SB_j over i + j = s in the spectral domain, one inverse transform,
+// and the window added into that prime's residues at s * 2^23; one Garner pass
+// at the end.  nA + nB forward and nA + nB - 1 inverse transforms per prime
+// instead of 3 nA nB.  The whole coefficient is reconstructed at once, so this
+// needs (p-1)^2 min(la, lb) below the auxiliary primes' product (false: not
+// taken; crt_product's per-pair path reconstructs each pair separately).
+bool Engine::crt_blocked(uint32_t p, const uint32_t* a, size_t la, const uint32_t* b, size_t lb, size_t outn,
+                         uint32_t* out, bool accumulate) {
+  const size_t B = kCrtBlock;
+  const size_t nA = (la + B - 1) / B, nB = (lb + B - 1) / B;
+  if (nA * nB < 2 || std::min(la, lb) <= kNaive) return false;
+  if (const char* e = std::getenv("FPX_CRT_BLOCKED"); e && e[0] == '0') return false;  // the per-pair path
+  const unsigned __int128 P123 = (unsigned __int128)kCrtPrimes[0] * kCrtPrimes[1] * kCrtPrimes[2];
+  if ((unsigned __int128)(p - 1) * (p - 1) * std::min(la, lb) >= P123) return false;
+  const int logN = std::bit_width(2 * B - 1);
+  for (uint32_t q : kCrtPrimes)
+    if (!native(q, logN)) return false;
+  const size_t N = size_t(1) << logN;
+  const bool square = a == b && la == lb;
+  std::vector<Buf> sa(nA), sb(square ? 0 : nB);
+  for (auto& x : sa) x = Buf(&pool_, N);
+  for (auto& x : sb) x = Buf(&pool_, N);
+  Buf acc(&pool_, N);
+  Buf res[3];
+  for (int k = 0; k < 3; ++k) {
+    const uint32_t q = kCrtPrimes[k];
+    const PrimeTables& pt = prime_plan(q).t;
+    const BigTables& bt = big_plan(q, logN).t;
+    res[k] = Buf(&pool_, outn);
+    check(cudaMemsetAsync(res[k].get(), 0, outn * 4, stream_), "memset");
+    auto forward = [&](const uint32_t* src, size_t cnt, uint32_t* dst) {
+      InOp in{src, (uint32_t)cnt, 1};  // target residues, reduced mod q on load
+      uint32_t* outs[1] = {dst};
+      kcheck(launch_colfwd(pt, bt, 1, &in, outs, stream_), "colfwd");
+      kcheck(launch_rows(pt, bt, dst, nullptr, 0, nullptr, 1, 0, stream_), "rows");
+    };
+    for (size_t i = 0; i < nA; ++i) forward(a + i * B, std::min(B, la - i * B), sa[i].get());
+    for (size_t j = 0; j < sb.size(); ++j) forward(b + j * B, std::min(B, lb - j * B), sb[j].get());
+    for (size_t s = 0; s + 1 < nA + nB && s * B < outn; ++s) {
+      std::vector<const uint32_t*> xs, ys;
+      for (size_t i = 0; i < nA; ++i)
+        if (s >= i && s - i < nB) {
+          xs.push_back(sa[i].get());
+          ys.push_back(square ? sa[s - i].get() : sb[s - i].get());
+        }
+      kcheck(launch_spec_mac(q, xs.data(), ys.data(), (int)xs.size(), acc.get(), N, 0, stream_), "spectral mac");
+      kcheck(launch_rows(pt, bt, acc.get(), nullptr, 0, nullptr, 0, 1, stream_), "rows");
+      Epi e;  // 2^32 / N undoes the Montgomery factor of the products and the transform size
+      e.out = res[k].get() + s * B;
+      e.lo = 0;
+      e.hi = (uint32_t)std::min(2 * B - 1, outn - s * B);
+      e.accumulate = 1;
+      kcheck(launch_colinv(pt, bt, acc.get(), 1, e, stream_), "colinv");
+    }
+  }
+  kcheck(launch_garner(p, 3, res[0].get(), res[1].get(), res[2].get(), out, outn, accumulate ? 1 : 0, stream_),
+         "garner");
+  return true;
+}
+
 void Engine::crt_product(uint32_t p, const uint32_t* a, size_t la, const uint32_t* b, size_t lb, size_t outn,
                          uint32_t* out, bool accumulate) {
-  if (!accumulate) check(cudaMemsetAsync(out, 0, outn * 4, stream_), "memset");
   la = std::min(la, outn);
   lb = std::min(lb, outn);
+  if (crt_blocked(p, a, la, b, lb, outn, out, accumulate)) return;
+  if (!accumulate) check(cudaMemsetAsync(out, 0, outn * 4, stream_), "memset");
   for (size_t ai = 0; ai < la;) {
     const size_t na = std::min(kCrtBlock, la - ai);
     for (size_t bi = 0; bi < lb && bi < outn - ai;) {

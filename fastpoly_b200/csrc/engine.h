@@ -223,6 +223,8 @@ class Engine {
                const uint32_t* post_mont = nullptr, bool accumulate = false);
   void crt_product(uint32_t p, const uint32_t* a, size_t la, const uint32_t* b, size_t lb, size_t outn,
                    uint32_t* out, bool accumulate);
+  bool crt_blocked(uint32_t p, const uint32_t* a, size_t la, const uint32_t* b, size_t lb, size_t outn,
+                   uint32_t* out, bool accumulate);
   // Exact coefficients [off, off+cnt) of a*b.
   // The same window through the batch recorder (batch.cpp): one launch set,
   // 3-prime CRT with batched Garner for non-native primes; cyc_log > 0 is a

@@ -306,6 +306,33 @@ __global__ void k_pointwise(Fp f, uint32_t* a, const uint32_t* b, size_t n) {
     a[i] = mont(a[i], b[i], f);
 }
 
+// Sum of pointwise products of spectra, the spectral side of a blocked
+// product: acc[i] (+)= sum_t x_t[i] y_t[i] * 2^-32 mod p, canonical; inputs
+// lazy below 4p.  Four words per thread per step (16-byte loads).
+constexpr int kMacPairs = 16;
+struct MacPairs {
+  const uint4* x[kMacPairs];
+  const uint4* y[kMacPairs];
+  int n;
+};
+__device__ __forceinline__ uint32_t mac1(uint32_t acc, uint32_t x, uint32_t y, const Fp& f) {
+  return red(acc + red(mont(canon4(x, f), canon4(y, f), f), f.p), f.p);
+}
+__global__ void k_spec_mac(Fp f, MacPairs pr, uint4* acc, size_t n4, int accumulate) {
+  pdl_enter();
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n4; i += (size_t)gridDim.x * blockDim.x) {
+    uint4 s = accumulate ? acc[i] : make_uint4(0u, 0u, 0u, 0u);
+    for (int t = 0; t < pr.n; ++t) {
+      const uint4 x = __ldg(pr.x[t] + i), y = __ldg(pr.y[t] + i);
+      s.x = mac1(s.x, x.x, y.x, f);
+      s.y = mac1(s.y, x.y, y.y, f);
+      s.z = mac1(s.z, x.z, y.z, f);
+      s.w = mac1(s.w, x.w, y.w, f);
+    }
+    acc[i] = s;
+  }
+}
+
 struct GarnerC {
   uint32_t P1, P2, P3;
   uint2 inv12;      // P1^-1 mod P2 (Shoup)
@@ -816,6 +843,22 @@ cudaError_t launch_rows_generic(const PrimeTables& pt, const BigTables& bt, uint
 
 cudaError_t launch_pointwise(uint32_t p, uint32_t* a, const uint32_t* b, size_t n, cudaStream_t s) {
   (void)pdl_launch(k_pointwise, grid_for(n, 256), 256, 0, s, make_fp(p), a, b, n);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_spec_mac(uint32_t p, const uint32_t* const* x, const uint32_t* const* y, int npairs, uint32_t* acc,
+                            size_t n, int accumulate, cudaStream_t s) {
+  if (n % 4 || npairs < 1) return cudaErrorInvalidValue;
+  for (int t0 = 0; t0 < npairs; t0 += kMacPairs) {
+    MacPairs pr{};
+    pr.n = std::min(kMacPairs, npairs - t0);
+    for (int t = 0; t < pr.n; ++t) {
+      pr.x[t] = reinterpret_cast<const uint4*>(x[t0 + t]);
+      pr.y[t] = reinterpret_cast<const uint4*>(y[t0 + t]);
+    }
+    (void)pdl_launch(k_spec_mac, grid_for(n / 4, 256), 256, 0, s, make_fp(p), pr, reinterpret_cast<uint4*>(acc), n / 4,
+                     (accumulate || t0) ? 1 : 0);
+  }
   return cudaGetLastError();
 }
 

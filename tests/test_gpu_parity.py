@@ -252,3 +252,38 @@ def test_device_api(fpx, oracle):
     fpx.inv_device(p, da, a.size, 50000, o2)
     fpx.synchronize()
     eq(o2.cpu().numpy().view(np.uint32), oracle.inv(p, a, 50000), "device inv")
+
+
+def _coeff(a, b, t, p):
+    """Exact coefficient t of a * b mod p (numpy, products below 2^60)."""
+    lo, hi = max(0, t - (b.size - 1)), min(t, a.size - 1)
+    if lo > hi:
+        return 0
+    u = np.arange(lo, hi + 1)
+    prod = (a[u].astype(np.uint64) * b[t - u].astype(np.uint64)) % np.uint64(p)
+    return int(prod.sum(dtype=np.uint64) % np.uint64(p))
+
+
+def test_crt_blocked_product(fpx):
+    """Products of more than one 2^23-term block on a prime without 2^24 roots:
+    the spectra-reusing blocked path against the per-pair path of the
+    reference's block scheme, bit for bit, and exact coefficients."""
+    import os
+    p = 1000000007
+    rng = np.random.default_rng(25)
+    a = rnd(rng, p, (1 << 23) + 1001)
+    b = rnd(rng, p, (1 << 23) + 77)
+    got = fpx.conv(p, a, b)
+    sq = fpx.conv(p, a, a)
+    os.environ["FPX_CRT_BLOCKED"] = "0"
+    try:
+        want = fpx.conv(p, a, b)
+        want_sq = fpx.conv(p, a, a)
+    finally:
+        del os.environ["FPX_CRT_BLOCKED"]
+    eq(got, want, "blocked conv")
+    eq(sq, want_sq, "blocked square")
+    for t in (0, 7, (1 << 23) - 1, 1 << 23, (1 << 23) + 500, (1 << 24) + 1000, got.size - 1):
+        assert int(got[t]) == _coeff(a, b, t, p), t
+    trunc = fpx.conv(p, a, b, (1 << 23) + 12345)
+    eq(trunc, got[: (1 << 23) + 12345], "blocked truncated")
