@@ -846,6 +846,22 @@ cudaError_t launch_pointwise(uint32_t p, uint32_t* a, const uint32_t* b, size_t 
   return cudaGetLastError();
 }
 
+namespace {
+__global__ void k_add_into(uint32_t p, uint32_t* __restrict__ dst, const uint32_t* __restrict__ src, size_t n) {
+  pdl_enter();
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    const uint32_t v = dst[i] + __ldg(src + i);
+    dst[i] = v >= p ? v - p : v;
+  }
+}
+}  // namespace
+
+cudaError_t launch_add_into(uint32_t p, uint32_t* dst, const uint32_t* src, size_t n, cudaStream_t s) {
+  if (n == 0) return cudaSuccess;
+  (void)pdl_launch(k_add_into, grid_for(n, 256), 256, 0, s, p, dst, src, n);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_spec_mac(uint32_t p, const uint32_t* const* x, const uint32_t* const* y, int npairs, uint32_t* acc,
                             size_t n, int accumulate, cudaStream_t s) {
   if (n % 4 || npairs < 1) return cudaErrorInvalidValue;

@@ -110,6 +110,8 @@ cudaError_t launch_colinv(const PrimeTables& pt, const BigTables& bt, const uint
 // -------- elementwise ------------------------------------------------------------
 // out[i] = mont(a[i], b[i]) for lazy spectra (result in (0, 2p)).
 cudaError_t launch_pointwise(uint32_t p, uint32_t* a, const uint32_t* b, size_t n, cudaStream_t s);
+// dst[i] = dst[i] + src[i] mod p, canonical inputs, i < n.
+cudaError_t launch_add_into(uint32_t p, uint32_t* dst, const uint32_t* src, size_t n, cudaStream_t s);
 // acc[i] (+)= sum_t x[t][i] * y[t][i] * 2^-32 mod p (canonical) over npairs
 // spectra of n words (n a multiple of 4, inputs lazy below 4p).
 cudaError_t launch_spec_mac(uint32_t p, const uint32_t* const* x, const uint32_t* const* y, int npairs, uint32_t* acc,
