@@ -735,16 +735,24 @@ bool Engine::crt_blocked(uint32_t p, const uint32_t* a, size_t la, const uint32_
     if (!native(q, logN)) return false;
   const size_t N = size_t(1) << logN;
   const bool square = a == b && la == lb;
+  // all scratch up front: without the memory (pool limit) the per-pair path,
+  // which needs far less, takes over before anything is written
   std::vector<Buf> sa(nA), sb(square ? 0 : nB);
-  for (auto& x : sa) x = Buf(&pool_, N);
-  for (auto& x : sb) x = Buf(&pool_, N);
-  Buf acc(&pool_, N), win(&pool_, N);
-  Buf res[3];
+  Buf acc, win, res[3];
+  try {
+    for (auto& x : sa) x = Buf(&pool_, N);
+    for (auto& x : sb) x = Buf(&pool_, N);
+    acc = Buf(&pool_, N);
+    win = Buf(&pool_, N);
+    for (auto& r : res) r = Buf(&pool_, outn);
+  } catch (const Error& e) {
+    if (e.code != FPX_ENOMEM) throw;
+    return false;
+  }
   for (int k = 0; k < 3; ++k) {
     const uint32_t q = kCrtPrimes[k];
     const PrimeTables& pt = prime_plan(q).t;
     const BigTables& bt = big_plan(q, logN).t;
-    res[k] = Buf(&pool_, outn);
     check(cudaMemsetAsync(res[k].get(), 0, outn * 4, stream_), "memset");
     auto forward = [&](const uint32_t* src, size_t cnt, uint32_t* dst) {
       InOp in{src, (uint32_t)cnt, 1};  // target residues, reduced mod q on load

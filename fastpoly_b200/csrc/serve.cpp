@@ -44,11 +44,17 @@ size_t pow2_at_least(size_t x) { return x <= 1 ? 1 : size_t(1) << std::bit_width
 extern "C" size_t fpx_serve_plan_bytes(const fpx_job* j) {
   if (!j || j->p < 2) return 0;
   const uint32_t p = j->p;
-  auto prod = [&](size_t full) -> size_t {  // scratch words of one product with `full` terms
+  const size_t B = size_t(1) << 23;  // CRT block (crt_convolution.hpp:19)
+  auto prod2 = [&](size_t la, size_t lb) -> size_t {  // scratch words of one la x lb product
+    const size_t full = la + lb - 1;
     const size_t N = pow2_at_least(full);
     const int logN = std::countr_zero(N);
-    return native_size(p, logN) ? 2 * N : 3 * (2 * N + full);
+    if (native_size(p, logN)) return 2 * N;
+    if (la > B || lb > B)  // blocked: every block's spectrum at 2^24 points, two work buffers, three residue arrays
+      return ((la + B - 1) / B + (lb + B - 1) / B + 2) * (2 * B) + 3 * full;
+    return 3 * (2 * N + full);
   };
+  auto prod = [&](size_t full) -> size_t { return prod2(full / 2 + 1, full / 2 + 1); };
   size_t in = 0, out = 0, scratch = 0;
   switch (j->op) {
     case FPX_OP_CONV: {
@@ -56,7 +62,7 @@ extern "C" size_t fpx_serve_plan_bytes(const fpx_job* j) {
       if (!la || !lb) return 64;
       in = la + lb;
       out = std::min(la + lb - 1, j->n);
-      scratch = prod(la + lb - 1);
+      scratch = prod2(la, lb);
       break;
     }
     case FPX_OP_INV:
