@@ -393,8 +393,13 @@ void Engine::drop_graphs() {
 bool Engine::graph_native(uint32_t p, size_t n) const { return n >= 2 && native(p, std::bit_width(2 * n - 1)); }
 
 void Engine::run_graph(const GraphKey& key, const std::function<void()>& fn) {
-  if (!graphs_on_ || prof_on_) {
-    fn();
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(stream_, &cs) != cudaSuccess) {
+    cudaGetLastError();
+    cs = cudaStreamCaptureStatusNone;
+  }
+  if (!graphs_on_ || prof_on_ || cs != cudaStreamCaptureStatusNone) {
+    fn();  // (a caller capturing this stream records the launches itself)
     return;
   }
   auto it = graphs_.find(key);
