@@ -602,6 +602,37 @@ const BigPlan& Engine::big_plan(uint32_t p, int logN) {
   plan->t.lo_inv_r = reinterpret_cast<const Tw2*>(upload(*this, plan->lo_inv_r, lo_ir));
   plan->t.mid_inv = reinterpret_cast<const Tw2*>(upload(*this, plan->mid_inv, mid_i));
   plan->t.hi_inv = reinterpret_cast<const Tw2*>(upload(*this, plan->hi_inv, hi_i));
+  // Column factors (BigTables::cf_fwd): for R >= 2^5 points per column, where
+  // the column passes have at least two butterfly groups.  FPX_COL_FACTOR=0
+  // keeps the three small-table products per point.
+  const char* cfe = std::getenv("FPX_COL_FACTOR");
+  if (plan->t.logR >= 5 && !(cfe && cfe[0] == '0')) {
+    const int G = col_last_group_log(plan->t.logR);
+    const size_t C = size_t(1) << plan->t.logC, P = size_t(1) << G;
+    std::vector<Tw2> cf(C * P), ci(C * P);
+    const uint32_t step = powm(wN, uint64_t(1) << (plan->t.logR - G), p);
+    const uint32_t stepi = invm(step, p);
+    std::vector<uint32_t> pw(P), pwi(P);
+    uint64_t u = 1, ui = 1;  // U_j, U_j^-1
+    for (size_t j = 0; j < C; ++j) {
+      pw[0] = pwi[0] = 1;
+      for (size_t k = 1; k < P; ++k) {
+        pw[k] = (uint32_t)(pw[k - 1] * u % p);
+        pwi[k] = (uint32_t)(pwi[k - 1] * ui % p);
+      }
+      for (size_t i = 0; i < P; ++i) {
+        size_t k = 0;  // bitrev_G(i)
+        for (int b = 0; b < G; ++b) k |= ((i >> b) & 1) << (G - 1 - b);
+        const size_t idx = 2 * ((j >> 1) * P + i) + (j & 1);
+        cf[idx] = shoup_pair(pw[k], p);
+        ci[idx] = shoup_pair(pwi[k], p);
+      }
+      u = u * step % p;
+      ui = ui * stepi % p;
+    }
+    plan->t.cf_fwd = reinterpret_cast<const Tw2*>(upload(*this, plan->cf_fwd, cf));
+    plan->t.cf_inv = reinterpret_cast<const Tw2*>(upload(*this, plan->cf_inv, ci));
+  }
   plan->t.shapes = tuned_shapes_locked(p, plan->t);
   auto& ref = *plan;
   bigs_[key] = std::move(plan);

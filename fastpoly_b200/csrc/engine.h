@@ -94,7 +94,7 @@ struct PrimePlan {
 };
 struct BigPlan {
   BigTables t;
-  Buf lo_fwd, mid_fwd, hi_fwd, lo_inv, lo_inv_r, mid_inv, hi_inv;
+  Buf lo_fwd, mid_fwd, hi_fwd, lo_inv, lo_inv_r, mid_inv, hi_inv, cf_fwd, cf_inv;
 };
 
 // Host-side number theory.

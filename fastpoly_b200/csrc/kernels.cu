@@ -242,6 +242,8 @@ struct BigD {
   const uint2* lo;   // w_N^y, y < 256
   const uint2* mid;  // w_N^(256 y), y < 256
   const uint2* hi;   // w_N^(65536 y), y < max(1, N / 65536)
+  const uint4* cf;   // column factors of a column pair (BigTables::cf_fwd / cf_inv), or nullptr
+  uint2 r32;         // 2^32 mod p with its Shoup quotient
 };
 
 // Bailey twiddle w_N^ex from the three small tables (5 KiB for N = 2^23, L1
@@ -1540,6 +1542,21 @@ struct BaileyCol {
   }
 };
 
+// Factored form of the same twiddle: w_N^eb (the block's part, the same for
+// all 2^G rows of the block) once per block in Montgomery form, times the
+// column factor U_j^bitrev_G(i) from the table.  A point then costs one Shoup
+// product by the factor and one Montgomery product by the block's part, both
+// lazy in [0, 2p) (the Montgomery product needs a*b < p 2^32: 2p * 2p is, for
+// p < 2^30), instead of three Shoup products and three table loads.
+static_assert(ColGroups<5>::size(ColGroups<5>::K - 1) == 5 / ((5 + 3) / 4), "col_last_group_log");
+static_assert(ColGroups<9>::size(ColGroups<9>::K - 1) == 9 / ((9 + 3) / 4), "col_last_group_log");
+static_assert(ColGroups<11>::size(ColGroups<11>::K - 1) == 11 / ((11 + 3) / 4), "col_last_group_log");
+static_assert(ColGroups<12>::size(ColGroups<12>::K - 1) == 12 / ((12 + 3) / 4), "col_last_group_log");
+__device__ __forceinline__ uint32_t col_block_factor(uint32_t j, int b, int logr, int g, const BigD& bt,
+                                                     const Fp& f) {
+  return shoup(bailey_mul(1u, j * brev_c(b, logr - g), bt, f), bt.r32, f.p);
+}
+
 template <int LOGR, int LOGW>
 __device__ __forceinline__ void colfwd_body(const InD& in, uint32_t* __restrict__ out, const BigD& bt, const Ptab& pt,
                                             int j0) {
@@ -1583,11 +1600,22 @@ __device__ __forceinline__ void colfwd_body(const InD& in, uint32_t* __restrict_
     }
     bf_group<G, G, false, 2, true>(v, pt.fwd, 0, f);
     const uint32_t j = j0 + c;
-    const BaileyCol w0(j, b, LOGR, G), w1(j + 1, b, LOGR, G);
+    if (LOGR >= 5 && bt.cf != nullptr) {
+      const uint4* tp = bt.cf + ((size_t)(j >> 1) << G);
+      const uint32_t a0 = col_block_factor(j, b, LOGR, G, bt, f), a1 = col_block_factor(j + 1, b, LOGR, G, bt, f);
 #pragma unroll
-    for (int i = 0; i < (1 << G); ++i)
-      *reinterpret_cast<uint2*>(out + ((size_t)(p0 + i) << logC) + j) =
-          make_uint2(w0.apply(v[0][i], i, G, bt, f), w1.apply(v[1][i], i, G, bt, f));
+      for (int i = 0; i < (1 << G); ++i) {
+        const uint4 t = __ldg(tp + i);
+        *reinterpret_cast<uint2*>(out + ((size_t)(p0 + i) << logC) + j) =
+            make_uint2(mont(shoup(v[0][i], t.x, t.y, f.p), a0, f), mont(shoup(v[1][i], t.z, t.w, f.p), a1, f));
+      }
+    } else {
+      const BaileyCol w0(j, b, LOGR, G), w1(j + 1, b, LOGR, G);
+#pragma unroll
+      for (int i = 0; i < (1 << G); ++i)
+        *reinterpret_cast<uint2*>(out + ((size_t)(p0 + i) << logC) + j) =
+            make_uint2(w0.apply(v[0][i], i, G, bt, f), w1.apply(v[1][i], i, G, bt, f));
+    }
   }
 }
 
@@ -1650,17 +1678,30 @@ __device__ __forceinline__ void colinv_body(const uint32_t* __restrict__ in, con
       const int b = inst >> LP;
       const int p0 = b << G;
       const uint32_t j = j0 + c;
-      const BaileyCol w0(j, b, LOGR, G), w1(j + 1, b, LOGR, G);
       using A = typename C::P::template Group<C::LOGW, G>;
       int ab[A::P];
       A::bases((p0 << C::LOGW) + c, ab);
       uint32_t v[2][1 << G];
+      if (LOGR >= 5 && bt.cf != nullptr) {
+        const uint4* tp = bt.cf + ((size_t)(j >> 1) << G);
+        const uint32_t a0 = col_block_factor(j, b, LOGR, G, bt, f), a1 = col_block_factor(j + 1, b, LOGR, G, bt, f);
 #pragma unroll
-      for (int i = 0; i < (1 << G); ++i) {
-        uint32_t x0, x1;
-        lds_pair(sm + A::addr(ab, i), x0, x1);
-        v[0][i] = w0.apply(x0, i, G, bt, f);
-        v[1][i] = w1.apply(x1, i, G, bt, f);
+        for (int i = 0; i < (1 << G); ++i) {
+          uint32_t x0, x1;
+          lds_pair(sm + A::addr(ab, i), x0, x1);
+          const uint4 t = __ldg(tp + i);
+          v[0][i] = mont(shoup(x0, t.x, t.y, f.p), a0, f);
+          v[1][i] = mont(shoup(x1, t.z, t.w, f.p), a1, f);
+        }
+      } else {
+        const BaileyCol w0(j, b, LOGR, G), w1(j + 1, b, LOGR, G);
+#pragma unroll
+        for (int i = 0; i < (1 << G); ++i) {
+          uint32_t x0, x1;
+          lds_pair(sm + A::addr(ab, i), x0, x1);
+          v[0][i] = w0.apply(x0, i, G, bt, f);
+          v[1][i] = w1.apply(x1, i, G, bt, f);
+        }
       }
       bf_group<G, G, true, 2, true>(v, pt.inv, 0, f);
       if constexpr (K == 1) {
@@ -1819,6 +1860,20 @@ ColSplit col_split(const BigTables& bt, const ColShape& sh, int nops, int& lw1, 
   }
   return sp;
 }
+
+// Bailey tables of one column pass.  The inverse pass scales by 1/N, or by
+// 2^32/N after a Montgomery pointwise product (mont_scaled), on its lo table.
+BigD big_d(const BigTables& bt, int lw, bool inverse, bool mont_scaled, uint32_t p) {
+  const uint32_t r = (uint32_t)((uint64_t(1) << 32) % p);
+  const uint2 r32 = make_uint2(r, (uint32_t)(((uint64_t)r << 32) / p));
+  if (!inverse)
+    return BigD{bt.logR, bt.logC, lw, reinterpret_cast<const uint2*>(bt.lo_fwd),
+                reinterpret_cast<const uint2*>(bt.mid_fwd), reinterpret_cast<const uint2*>(bt.hi_fwd),
+                reinterpret_cast<const uint4*>(bt.cf_fwd), r32};
+  return BigD{bt.logR, bt.logC, lw, reinterpret_cast<const uint2*>(mont_scaled ? bt.lo_inv_r : bt.lo_inv),
+              reinterpret_cast<const uint2*>(bt.mid_inv), reinterpret_cast<const uint2*>(bt.hi_inv),
+              reinterpret_cast<const uint4*>(bt.cf_inv), r32};
+}
 }  // namespace
 
 cudaError_t launch_colfwd(const PrimeTables& pt, const BigTables& bt, int nops, const InOp* in,
@@ -1833,8 +1888,7 @@ cudaError_t launch_colfwd(const PrimeTables& pt, const BigTables& bt, int nops, 
   const ColSplit sp = col_split(bt, sh, nops, lw1, lw2);
   ColFwdFn fn = Cols::fwd(bt.logR, lw1, lw2);
   if (!fn || lw1 > bt.logC || nops < 1 || nops > 3) return cudaErrorInvalidValue;
-  BigD d{bt.logR, bt.logC, lw1, reinterpret_cast<const uint2*>(bt.lo_fwd),
-         reinterpret_cast<const uint2*>(bt.mid_fwd), reinterpret_cast<const uint2*>(bt.hi_fwd)};
+  const BigD d = big_d(bt, lw1, false, false, pt.p);
   (void)pdl_launch(fn, (unsigned)(nops * (sp.nbig + sp.nsmall)), 256, size_t(4) << (bt.logR + lw1), s, ops, d, dev_tab(pt), sp);
   return cudaGetLastError();
 }
@@ -1846,8 +1900,7 @@ cudaError_t launch_colinv(const PrimeTables& pt, const BigTables& bt, const uint
   const ColSplit sp = col_split(bt, sh, 1, lw1, lw2);
   ColInvFn fn = Cols::inv(bt.logR, lw1, lw2, host_epi_plain(epi));
   if (!fn || lw1 > bt.logC) return cudaErrorInvalidValue;
-  BigD d{bt.logR, bt.logC, lw1, reinterpret_cast<const uint2*>(mont_scaled ? bt.lo_inv_r : bt.lo_inv),
-         reinterpret_cast<const uint2*>(bt.mid_inv), reinterpret_cast<const uint2*>(bt.hi_inv)};
+  const BigD d = big_d(bt, lw1, true, mont_scaled != 0, pt.p);
   (void)pdl_launch(fn, (unsigned)(sp.nbig + sp.nsmall), 256, size_t(4) << (bt.logR + lw1), s, in, d, dev_tab(pt), dev_epi(epi),
                                                                                  sp);
   return cudaGetLastError();
@@ -2107,11 +2160,8 @@ cudaError_t launch_batch(const BatchPlan& b, void* host_staging, void* dev_desc,
         const BigTables& bt = *x.bt;
         BigJobB j{};
         j.pt = pt;
-        j.bf = BigD{bt.logR, bt.logC, col_logw(bt.logR), reinterpret_cast<const uint2*>(bt.lo_fwd),
-                    reinterpret_cast<const uint2*>(bt.mid_fwd), reinterpret_cast<const uint2*>(bt.hi_fwd)};
-        j.bi = BigD{bt.logR, bt.logC, col_logw(bt.logR),
-                    reinterpret_cast<const uint2*>(x.ymode != 0 ? bt.lo_inv_r : bt.lo_inv),
-                    reinterpret_cast<const uint2*>(bt.mid_inv), reinterpret_cast<const uint2*>(bt.hi_inv)};
+        j.bf = big_d(bt, col_logw(bt.logR), false, false, pt.f.p);
+        j.bi = big_d(bt, col_logw(bt.logR), true, x.ymode != 0, pt.f.p);
         j.in[0] = dev_in(x.x);
         j.in[1] = dev_in(x.y);
         j.t[0] = x.t1;

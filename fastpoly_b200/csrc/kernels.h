@@ -48,7 +48,20 @@ struct BigTables {
   const Tw2* lo_inv_r = nullptr;   // w_N^-y * 2^32 / N  (after a Montgomery pointwise)
   const Tw2* mid_inv = nullptr;    // w_N^-(256 y)
   const Tw2* hi_inv = nullptr;     // w_N^-(65536 y)
+  // Column factors of the Bailey twiddle at the column passes' last (forward)
+  // or first (inverse) butterfly group of 2^G rows, G = col_last_group_log(logR):
+  // the twiddle of column j, row 2^G b + i is w_N^(j bitrev(b)) * U_j^bitrev_G(i)
+  // with U_j = w_N^(j 2^(logR - G)).  Entry 2((j/2) 2^G + i) + (j & 1) holds
+  // U_j^bitrev_G(i) (cf_inv: U_j^-bitrev_G(i), no 1/N) with its Shoup quotient,
+  // so a column pair reads both of its factors in one 16-byte load.
+  // nullptr: three small-table products per point instead.
+  const Tw2* cf_fwd = nullptr;
+  const Tw2* cf_inv = nullptr;
 };
+
+// log2 of the row count of the column passes' last forward group, which the
+// column factors (BigTables::cf_fwd / cf_inv) are built for.
+inline int col_last_group_log(int logR) { return logR / ((logR + 3) / 4); }
 
 // A forward-transform input: values at ptr[0, count), zero beyond.
 struct InOp {

@@ -1,9 +1,11 @@
 """The environment switches give the same values as the defaults.
 
 FPX_PDL=0 (no programmatic dependent launch), FPX_GRAPHS=0 (no graph replay of
-repeated Newton calls) and FPX_AUTOTUNE=0 (default tile shapes) change how the
-work is launched, never what it computes: a child process with all three off
-must print the same checksums as one with the defaults.
+repeated Newton calls), FPX_AUTOTUNE=0 (default tile shapes) and
+FPX_COL_FACTOR=0 (Bailey twiddles from three small tables per point instead of
+column factors) change how the work is launched, never what it computes: a
+child process with all of them off must print the same checksums as one with
+the defaults.
 """
 import json
 import os
@@ -49,6 +51,6 @@ def _run(env):
 def test_switches_same_values():
     base = dict(os.environ)
     default = _run(base)
-    off = _run(dict(base, FPX_PDL="0", FPX_GRAPHS="0", FPX_AUTOTUNE="0"))
+    off = _run(dict(base, FPX_PDL="0", FPX_GRAPHS="0", FPX_AUTOTUNE="0", FPX_COL_FACTOR="0"))
     assert default == off
     assert default["998244353:inv"] == default["998244353:inv2"]
