@@ -1587,6 +1587,13 @@ __device__ __forceinline__ void colfwd_body(const InD& in, uint32_t* __restrict_
     const int c = (inst & ((1 << LP) - 1)) << 1;
     const int b = inst >> LP;
     const int p0 = b << G;
+    const uint32_t j = j0 + c;
+    const bool fact = LOGR >= 5 && bt.cf != nullptr;
+    uint32_t a0 = 0, a1 = 0;
+    if (fact) {  // the block's factors first: their table loads overlap the butterflies
+      a0 = col_block_factor(j, b, LOGR, G, bt, f);
+      a1 = col_block_factor(j + 1, b, LOGR, G, bt, f);
+    }
     using A = typename C::P::template Group<C::LOGW, G>;
     int ab[A::P];
     A::bases((p0 << C::LOGW) + c, ab);
@@ -1599,10 +1606,8 @@ __device__ __forceinline__ void colfwd_body(const InD& in, uint32_t* __restrict_
       v[1][i] = reduce_here ? reduce_any(x1, pt.q1, f) : x1;
     }
     bf_group<G, G, false, 2, true>(v, pt.fwd, 0, f);
-    const uint32_t j = j0 + c;
-    if (LOGR >= 5 && bt.cf != nullptr) {
+    if (fact) {
       const uint4* tp = bt.cf + ((size_t)(j >> 1) << G);
-      const uint32_t a0 = col_block_factor(j, b, LOGR, G, bt, f), a1 = col_block_factor(j + 1, b, LOGR, G, bt, f);
 #pragma unroll
       for (int i = 0; i < (1 << G); ++i) {
         const uint4 t = __ldg(tp + i);
@@ -1682,16 +1687,23 @@ __device__ __forceinline__ void colinv_body(const uint32_t* __restrict__ in, con
       int ab[A::P];
       A::bases((p0 << C::LOGW) + c, ab);
       uint32_t v[2][1 << G];
-      if (LOGR >= 5 && bt.cf != nullptr) {
+      // Factored twiddle: the column factors on the way in, the block's factor
+      // (the same for the block's 2^G rows) after the block's butterflies, which
+      // are linear, so that its table loads overlap them.  Made canonical: it
+      // multiplies DIT outputs in [0, 4p), and 4p * p < p 2^32.
+      const bool fact = LOGR >= 5 && bt.cf != nullptr;
+      uint32_t a0 = 0, a1 = 0;
+      if (fact) {
+        a0 = red(col_block_factor(j, b, LOGR, G, bt, f), f.p);
+        a1 = red(col_block_factor(j + 1, b, LOGR, G, bt, f), f.p);
         const uint4* tp = bt.cf + ((size_t)(j >> 1) << G);
-        const uint32_t a0 = col_block_factor(j, b, LOGR, G, bt, f), a1 = col_block_factor(j + 1, b, LOGR, G, bt, f);
 #pragma unroll
         for (int i = 0; i < (1 << G); ++i) {
           uint32_t x0, x1;
           lds_pair(sm + A::addr(ab, i), x0, x1);
           const uint4 t = __ldg(tp + i);
-          v[0][i] = mont(shoup(x0, t.x, t.y, f.p), a0, f);
-          v[1][i] = mont(shoup(x1, t.z, t.w, f.p), a1, f);
+          v[0][i] = shoup(x0, t.x, t.y, f.p);
+          v[1][i] = shoup(x1, t.z, t.w, f.p);
         }
       } else {
         const BaileyCol w0(j, b, LOGR, G), w1(j + 1, b, LOGR, G);
@@ -1704,6 +1716,13 @@ __device__ __forceinline__ void colinv_body(const uint32_t* __restrict__ in, con
         }
       }
       bf_group<G, G, true, 2, true>(v, pt.inv, 0, f);
+      if (fact) {
+#pragma unroll
+        for (int i = 0; i < (1 << G); ++i) {
+          v[0][i] = mont(v[0][i], a0, f);
+          v[1][i] = mont(v[1][i], a1, f);
+        }
+      }
       if constexpr (K == 1) {
 #pragma unroll
         for (int i = 0; i < (1 << G); ++i)
