@@ -602,11 +602,13 @@ const BigPlan& Engine::big_plan(uint32_t p, int logN) {
   plan->t.lo_inv_r = reinterpret_cast<const Tw2*>(upload(*this, plan->lo_inv_r, lo_ir));
   plan->t.mid_inv = reinterpret_cast<const Tw2*>(upload(*this, plan->mid_inv, mid_i));
   plan->t.hi_inv = reinterpret_cast<const Tw2*>(upload(*this, plan->hi_inv, hi_i));
-  // Column factors (BigTables::cf_fwd): for R >= 2^5 points per column, where
-  // the column passes have at least two butterfly groups.  FPX_COL_FACTOR=0
-  // keeps the three small-table products per point.
+  // Column factors (BigTables::cf_fwd): for R >= 2^9 points per column
+  // (transforms of 2^21 points and up), where they measured faster; smaller
+  // transforms were as fast or slightly slower with them.  FPX_COL_FACTOR=0
+  // keeps the three small-table products per point everywhere.  The column
+  // kernels take the factored path for R >= 2^9 only.
   const char* cfe = std::getenv("FPX_COL_FACTOR");
-  if (plan->t.logR >= 5 && !(cfe && cfe[0] == '0')) {
+  if (plan->t.logR >= 9 && !(cfe && cfe[0] == '0')) {
     const int G = col_last_group_log(plan->t.logR);
     const size_t C = size_t(1) << plan->t.logC, P = size_t(1) << G;
     std::vector<Tw2> cf(C * P), ci(C * P);

@@ -1588,7 +1588,7 @@ __device__ __forceinline__ void colfwd_body(const InD& in, uint32_t* __restrict_
     const int b = inst >> LP;
     const int p0 = b << G;
     const uint32_t j = j0 + c;
-    const bool fact = LOGR >= 5 && bt.cf != nullptr;
+    const bool fact = LOGR >= 9 && bt.cf != nullptr;
     uint32_t a0 = 0, a1 = 0;
     if (fact) {  // the block's factors first: their table loads overlap the butterflies
       a0 = col_block_factor(j, b, LOGR, G, bt, f);
@@ -1691,7 +1691,7 @@ __device__ __forceinline__ void colinv_body(const uint32_t* __restrict__ in, con
       // (the same for the block's 2^G rows) after the block's butterflies, which
       // are linear, so that its table loads overlap them.  Made canonical: it
       // multiplies DIT outputs in [0, 4p), and 4p * p < p 2^32.
-      const bool fact = LOGR >= 5 && bt.cf != nullptr;
+      const bool fact = LOGR >= 9 && bt.cf != nullptr;
       uint32_t a0 = 0, a1 = 0;
       if (fact) {
         a0 = red(col_block_factor(j, b, LOGR, G, bt, f), f.p);
