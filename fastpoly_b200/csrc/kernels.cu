@@ -1418,6 +1418,12 @@ __global__ void __launch_bounds__(256, 3) k_rows12(uint32_t* __restrict__ x, con
 // R = 2^10 and 2^14 words (64 KiB) above, so that three CTAs fit on an SM.
 __host__ __device__ constexpr int col_logw(int logr) { return logr >= 11 ? 14 - logr : 13 - logr; }
 
+// Threads of a column-pass CTA and the resident CTAs per SM it is compiled for
+// (80 registers a thread; shared memory also allows three 64 KB tiles).  512
+// threads in two CTAs (64 registers) measured 5-9 % slower from 2^21 points up.
+constexpr int kColNT = 256;
+constexpr int kColMinBlocks = 3;
+
 template <int LOGR, int LW = col_logw(LOGR)>
 struct ColCfg {
   static constexpr int LOGW = LW;
@@ -1439,13 +1445,13 @@ __device__ __forceinline__ void col_tile_load(uint32_t* sm, const uint32_t* src,
   using C = ColCfg<LOGR, LOGW>;
   constexpr int TL = HALF ? C::TE / 2 : C::TE;
   if (src == nullptr || count == 0) {
-    for (int e = tid; e < C::SMEM_WORDS; e += 256) sm[e] = 0u;
+    for (int e = tid; e < C::SMEM_WORDS; e += kColNT) sm[e] = 0u;
     return;
   }
   if (C::W >= 4 && ((uintptr_t)src & 15u) == 0) {
     constexpr int CPR = C::W >= 4 ? C::W / 4 : 1;  // 16-byte chunks per row segment
 #pragma unroll 4
-    for (int q = tid; q < TL / 4; q += 256) {
+    for (int q = tid; q < TL / 4; q += kColNT) {
       const int t = q / CPR, cc = (q % CPR) * 4;
       const uint32_t gi = ((uint32_t)t << logC) + j0 + cc;
       const int valid = gi < count ? (int)min(4u, count - gi) : 0;
@@ -1453,7 +1459,7 @@ __device__ __forceinline__ void col_tile_load(uint32_t* sm, const uint32_t* src,
     }
   } else {
 #pragma unroll 4
-    for (int e = tid; e < TL; e += 256) {
+    for (int e = tid; e < TL; e += kColNT) {
       const int t = e >> C::LOGW, c = e & (C::W - 1);
       const uint32_t gi = ((uint32_t)t << logC) + j0 + c;
       const bool v = gi < count;
@@ -1487,7 +1493,7 @@ __device__ __forceinline__ void col_group_smem(uint32_t* sm, const uint2* tw, co
   constexpr int LP = C::LOGW - 1;  // column pairs per row: 2^LP
   constexpr int NINST = C::TE >> (G + 1);
 #pragma unroll 1
-  for (int inst = tid; inst < NINST; inst += 256) {
+  for (int inst = tid; inst < NINST; inst += kColNT) {
     const int c = (inst & ((1 << LP) - 1)) << 1;
     const int rest = inst >> LP;
     const int base = rest & ((1 << S) - 1);
@@ -1583,7 +1589,7 @@ __device__ __forceinline__ void colfwd_body(const InD& in, uint32_t* __restrict_
   constexpr int NINST = C::TE >> (G + 1);
   const bool reduce_here = K == 1 && in.reduce;
 #pragma unroll 1
-  for (int inst = tid; inst < NINST; inst += 256) {
+  for (int inst = tid; inst < NINST; inst += kColNT) {
     const int c = (inst & ((1 << LP) - 1)) << 1;
     const int b = inst >> LP;
     const int p0 = b << G;
@@ -1648,7 +1654,7 @@ __device__ __forceinline__ bool col_tile_of(const ColSplit& sp, int lw1, int lw2
 }
 
 template <int LOGR, int LW1, int LW2>
-__global__ void __launch_bounds__(256, 3) k_colfwd_t(ColOps ops, BigD bt, Ptab pt, ColSplit sp) {
+__global__ void __launch_bounds__(kColNT, kColMinBlocks) k_colfwd_t(ColOps ops, BigD bt, Ptab pt, ColSplit sp) {
   pdl_enter();
   int op, j0;
   const bool wide = col_tile_of(sp, LW1, LW2, op, j0);
@@ -1678,7 +1684,7 @@ __device__ __forceinline__ void colinv_body(const uint32_t* __restrict__ in, con
     constexpr int G = C::GL;
     constexpr int NINST = C::TE >> (G + 1);
 #pragma unroll 1
-    for (int inst = tid; inst < NINST; inst += 256) {
+    for (int inst = tid; inst < NINST; inst += kColNT) {
       const int c = (inst & ((1 << LP) - 1)) << 1;
       const int b = inst >> LP;
       const int p0 = b << G;
@@ -1741,7 +1747,7 @@ __device__ __forceinline__ void colinv_body(const uint32_t* __restrict__ in, con
     constexpr int S = LOGR - G;
     constexpr int NINST = C::TE >> (G + 1);
 #pragma unroll 1
-    for (int inst = tid; inst < NINST; inst += 256) {
+    for (int inst = tid; inst < NINST; inst += kColNT) {
       const int c = (inst & ((1 << LP) - 1)) << 1;
       const int base = inst >> LP;
       using A = typename C::P::template Group<S + C::LOGW, G>;
@@ -1759,7 +1765,7 @@ __device__ __forceinline__ void colinv_body(const uint32_t* __restrict__ in, con
 }
 
 template <int LOGR, bool PLAIN, int LW1, int LW2>
-__global__ void __launch_bounds__(256, 3) k_colinv_t(const uint32_t* __restrict__ in, BigD bt, Ptab pt, EpiD epi,
+__global__ void __launch_bounds__(kColNT, kColMinBlocks) k_colinv_t(const uint32_t* __restrict__ in, BigD bt, Ptab pt, EpiD epi,
                                                      ColSplit sp) {
   pdl_enter();
   int op, j0;
@@ -1847,7 +1853,7 @@ int col_shape_candidates(int logR, bool inverse, ColShape* out, int max) {
       int dev = 0, sms = 0, per_sm = 0;
       if (cudaGetDevice(&dev) != cudaSuccess ||
           cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
-          cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, 256, (size_t(4) << (logR + lw1))) !=
+          cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kColNT, (size_t(4) << (logR + lw1))) !=
               cudaSuccess) {
         cudaGetLastError();
         return;
@@ -1908,7 +1914,7 @@ cudaError_t launch_colfwd(const PrimeTables& pt, const BigTables& bt, int nops, 
   ColFwdFn fn = Cols::fwd(bt.logR, lw1, lw2);
   if (!fn || lw1 > bt.logC || nops < 1 || nops > 3) return cudaErrorInvalidValue;
   const BigD d = big_d(bt, lw1, false, false, pt.p);
-  (void)pdl_launch(fn, (unsigned)(nops * (sp.nbig + sp.nsmall)), 256, size_t(4) << (bt.logR + lw1), s, ops, d, dev_tab(pt), sp);
+  (void)pdl_launch(fn, (unsigned)(nops * (sp.nbig + sp.nsmall)), kColNT, size_t(4) << (bt.logR + lw1), s, ops, d, dev_tab(pt), sp);
   return cudaGetLastError();
 }
 
@@ -1920,7 +1926,7 @@ cudaError_t launch_colinv(const PrimeTables& pt, const BigTables& bt, const uint
   ColInvFn fn = Cols::inv(bt.logR, lw1, lw2, host_epi_plain(epi));
   if (!fn || lw1 > bt.logC) return cudaErrorInvalidValue;
   const BigD d = big_d(bt, lw1, true, mont_scaled != 0, pt.p);
-  (void)pdl_launch(fn, (unsigned)(sp.nbig + sp.nsmall), 256, size_t(4) << (bt.logR + lw1), s, in, d, dev_tab(pt), dev_epi(epi),
+  (void)pdl_launch(fn, (unsigned)(sp.nbig + sp.nsmall), kColNT, size_t(4) << (bt.logR + lw1), s, in, d, dev_tab(pt), dev_epi(epi),
                                                                                  sp);
   return cudaGetLastError();
 }
@@ -1982,7 +1988,7 @@ struct GarnerJobB {
 
 
 template <int LOGR>
-__global__ void __launch_bounds__(256, 3) k_colfwd_b(const BigJobB* __restrict__ jobs) {
+__global__ void __launch_bounds__(kColNT, kColMinBlocks) k_colfwd_b(const BigJobB* __restrict__ jobs) {
   pdl_enter();
   const BigJobB& j = jobs[blockIdx.z];
   if ((int)blockIdx.y >= j.nops) return;
@@ -1996,7 +2002,7 @@ __global__ void __launch_bounds__(256, 3) k_rows12_b(const BigJobB* __restrict__
 }
 
 template <int LOGR, bool PLAIN>
-__global__ void __launch_bounds__(256, 3) k_colinv_b(const BigJobB* __restrict__ jobs) {
+__global__ void __launch_bounds__(kColNT, kColMinBlocks) k_colinv_b(const BigJobB* __restrict__ jobs) {
   pdl_enter();
   const BigJobB& j = jobs[blockIdx.y];
   colinv_body<LOGR, col_logw(LOGR), PLAIN>(j.t[0], j.bi, j.pt, j.epi, blockIdx.x << col_logw(LOGR));
@@ -2059,13 +2065,13 @@ struct ColBatch {
   static cudaError_t launch(int logR, dim3 grid, const BigJobB* jobs, int smem, cudaStream_t s) {
     BatchFn fn = fwd(logR);
     if (!fn) return cudaErrorInvalidValue;
-    (void)pdl_launch(fn, grid, 256, smem, s, jobs);
+    (void)pdl_launch(fn, grid, kColNT, smem, s, jobs);
     return cudaGetLastError();
   }
   static cudaError_t launch_inv(int logR, bool plain, dim3 grid, const BigJobB* jobs, int smem, cudaStream_t s) {
     BatchFn fn = inv(logR, plain);
     if (!fn) return cudaErrorInvalidValue;
-    (void)pdl_launch(fn, grid, 256, smem, s, jobs);
+    (void)pdl_launch(fn, grid, kColNT, smem, s, jobs);
     return cudaGetLastError();
   }
   static cudaError_t init() {
