@@ -514,24 +514,107 @@ __device__ __forceinline__ void cta_load(uint32_t* X, const uint32_t* src, uint3
   for (uint32_t i = tid; i < N; i += nt) X[pad(i)] = i < len ? src[i] : 0u;
 }
 
+// Forward (DIF) groups of the one-CTA products, with the pointwise product
+// folded into the last group: after its butterflies a thread holds final
+// spectrum values and multiplies them at once (Montgomery; DIF outputs are in
+// [0, 2p), so every product is below p 2^32), saving a shared-memory pass and
+// a barrier per product.  Modes: kNtMulSpec X <- DIF(X) * S (S a spectrum);
+// kNtPair Y <- DIF(Y) and X <- DIF(X) * DIF(Y), both transforms in one pass per
+// group (the same positions, so the same twiddles and the products in
+// registers); kNtSquare X <- DIF(X)^2.  Grouping and butterflies are those of
+// tile_dif, so every value is the one tile_dif and a separate pointwise pass
+// give.
+enum { kNtMulSpec = 1, kNtPair = 2, kNtSquare = 3 };
+
+template <int G, int MODE>
+__device__ __forceinline__ void nt_group(uint32_t* X, uint32_t* Y, const uint32_t* S, int logN, int lL, bool last,
+                                         const uint2* __restrict__ tw, const Fp& f, int tid, int nt) {
+  constexpr int E = 1 << G;
+  constexpr bool PAIR = MODE == kNtPair;
+  const int s_log = lL - G;
+  const int ninst = 1 << (logN - G);
+  for (int inst = tid; inst < ninst; inst += nt) {
+    const int base = inst & ((1 << s_log) - 1);
+    const int p0 = ((inst >> s_log) << lL) + base;
+    uint32_t x[E], y[PAIR ? E : 1];
+#pragma unroll
+    for (int i = 0; i < E; ++i) {
+      x[i] = X[pad(p0 + (i << s_log))];
+      if constexpr (PAIR) y[i] = Y[pad(p0 + (i << s_log))];
+    }
+#pragma unroll
+    for (int l = 0; l < G; ++l) {
+      const int hs = 1 << (G - 1 - l);
+      const int half = 1 << (lL - 1 - l);
+      uint2 w[E / 2];
+#pragma unroll
+      for (int j = 0; j < hs; ++j) w[j] = __ldg(&tw[half + base + (j << s_log)]);
+#pragma unroll
+      for (int i = 0; i < E; ++i)
+        if (!(i & hs)) {
+          dif_bf(x[i], x[i + hs], w[i & (hs - 1)], f);
+          if constexpr (PAIR) dif_bf(y[i], y[i + hs], w[i & (hs - 1)], f);
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < E; ++i) {
+      const int q = pad(p0 + (i << s_log));
+      if constexpr (PAIR) Y[q] = y[i];
+      if (last) {
+        const uint32_t m = MODE == kNtPair ? y[PAIR ? i : 0] : (MODE == kNtMulSpec ? S[q] : x[i]);
+        X[q] = mont(x[i], m, f);
+      } else {
+        X[q] = x[i];
+      }
+    }
+  }
+}
+
+// The forward transform(s) of `nt_group` over N = 2^logN points; returns
+// synchronised.
+template <int MODE>
+__device__ __forceinline__ void nt_fwd_mul(uint32_t* X, uint32_t* Y, const uint32_t* S, int logN, const Ptab& pt,
+                                           int tid, int nt) {
+  if (logN == 0) {  // one point: the pointwise product alone
+    if (tid == 0) X[0] = mont(X[0], MODE == kNtPair ? Y[0] : (MODE == kNtMulSpec ? S[0] : X[0]), pt.f);
+    __syncthreads();
+    return;
+  }
+  int lL = logN;
+  while (lL > 0) {
+    const int G = lL >= 4 ? 4 : lL;
+    const bool last = lL == G;
+    switch (G) {
+      case 4: nt_group<4, MODE>(X, Y, S, logN, lL, last, pt.fwd, pt.f, tid, nt); break;
+      case 3: nt_group<3, MODE>(X, Y, S, logN, lL, last, pt.fwd, pt.f, tid, nt); break;
+      case 2: nt_group<2, MODE>(X, Y, S, logN, lL, last, pt.fwd, pt.f, tid, nt); break;
+      default: nt_group<1, MODE>(X, Y, S, logN, lL, last, pt.fwd, pt.f, tid, nt); break;
+    }
+    lL -= G;
+    __syncthreads();
+  }
+}
+
 // X <- DIT(DIF(X) * Y) over N = 2^logN points, Y a spectrum (Montgomery
 // pointwise; the caller scales by 2^32 / N).  Call after X is loaded and
 // synchronised; returns synchronised.
 __device__ __forceinline__ void cta_mul(uint32_t* X, const uint32_t* Y, int logN, const Ptab& pt, int tid, int nt) {
-  tile_dif(X, logN, 0, pt.fwd, pt.f, tid, nt);
+  nt_fwd_mul<kNtMulSpec>(X, nullptr, Y, logN, pt, tid, nt);
+  tile_dit(X, logN, 0, pt.inv, pt.f, tid, nt);
   __syncthreads();
-  for (uint32_t i = tid; i < (1u << logN); i += nt) X[pad(i)] = mont(X[pad(i)], Y[pad(i)], pt.f);
-  __syncthreads();
+}
+
+// Y <- DIF(Y), X <- DIT(DIF(X) * DIF(Y)): both operands loaded and
+// synchronised; Y keeps its spectrum for later products.
+__device__ __forceinline__ void cta_mul2(uint32_t* X, uint32_t* Y, int logN, const Ptab& pt, int tid, int nt) {
+  nt_fwd_mul<kNtPair>(X, Y, nullptr, logN, pt, tid, nt);
   tile_dit(X, logN, 0, pt.inv, pt.f, tid, nt);
   __syncthreads();
 }
 
 // X <- DIT(DIF(X)^2) over N = 2^logN points (the caller scales by 2^32 / N).
 __device__ __forceinline__ void cta_mul_self(uint32_t* X, int logN, const Ptab& pt, int tid, int nt) {
-  tile_dif(X, logN, 0, pt.fwd, pt.f, tid, nt);
-  __syncthreads();
-  for (uint32_t i = tid; i < (1u << logN); i += nt) X[pad(i)] = mont(X[pad(i)], X[pad(i)], pt.f);
-  __syncthreads();
+  nt_fwd_mul<kNtSquare>(X, nullptr, nullptr, logN, pt, tid, nt);
   tile_dit(X, logN, 0, pt.inv, pt.f, tid, nt);
   __syncthreads();
 }
@@ -551,9 +634,7 @@ __device__ __forceinline__ void cta_inv_step(const uint32_t* series, uint32_t aw
   cta_load(X, series, aw, N, tid, nt);
   cta_load(Y, Cs, k, N, tid, nt);
   __syncthreads();
-  tile_dif(Y, logN, 0, pt.fwd, f, tid, nt);
-  __syncthreads();
-  cta_mul(X, Y, logN, pt, tid, nt);
+  cta_mul2(X, Y, logN, pt, tid, nt);
   for (uint32_t i = tid; i < hl; i += nt) {
     const uint32_t v = red(shoup(X[pad(k + i)], sc, f.p), f.p);
     H[i] = v ? f.p - v : 0u;
@@ -659,18 +740,14 @@ __device__ __forceinline__ void newton_exp_body(const NewtonExpD& d, const Ptab&
     cta_load(X, d.ap, min(d.lap, m2 - 1), N, tid, nt);
     cta_load(S, B, m, N, tid, nt);
     __syncthreads();
-    tile_dif(S, logN, 0, pt.fwd, f, tid, nt);
-    __syncthreads();
-    cta_mul(X, S, logN, pt, tid, nt);
+    cta_mul2(X, S, logN, pt, tid, nt);
     for (uint32_t i = tid; i < hl; i += nt) T[i] = red(shoup(X[pad(m - 1 + i)], sc, f.p), f.p);
     __syncthreads();
     // t2 = (t1 c) mod x^hl, times 1/(m+i)
     cta_load(X, T, hl, N, tid, nt);
     cta_load(Y, Cs, cs, N, tid, nt);
     __syncthreads();
-    tile_dif(Y, logN, 0, pt.fwd, f, tid, nt);
-    __syncthreads();
-    cta_mul(X, Y, logN, pt, tid, nt);
+    cta_mul2(X, Y, logN, pt, tid, nt);
     for (uint32_t i = tid; i < hl; i += nt)
       T[i] = red(mont(shoup(X[pad(i)], sc, f.p), __ldg(d.tab + m + i), f), f.p);
     __syncthreads();
@@ -768,9 +845,7 @@ __global__ void __launch_bounds__(kNewtonThreads) k_newton_sqrt(NewtonSqrtD d, P
     cta_load(X, T, hl, N, tid, nt);
     cta_load(Y, Cs, cs, N, tid, nt);
     __syncthreads();
-    tile_dif(Y, logN, 0, pt.fwd, f, tid, nt);
-    __syncthreads();
-    cta_mul(X, Y, logN, pt, tid, nt);
+    cta_mul2(X, Y, logN, pt, tid, nt);
     for (uint32_t i = tid; i < hl; i += nt) {
       const uint32_t v = red(shoup(X[pad(i)], sc, f.p), f.p);
       const uint32_t h = (v & 1u) ? (v + f.p) >> 1 : v >> 1;  // v / 2 mod p (p odd)
