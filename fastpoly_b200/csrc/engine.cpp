@@ -943,6 +943,16 @@ void Engine::extend_inverse(uint32_t p, const uint32_t* a, size_t la, uint32_t* 
   product(p, e.get(), hlen, c, k, hlen, c + k);
 }
 
+// The fused CRT inverse for the small sizes (k_newton_inv_crt); FPX_CRT_NEWTON=0
+// keeps the 32-term seed and per-step CRT products.
+static bool crt_newton_on() {
+  static const bool on = [] {
+    const char* e = std::getenv("FPX_CRT_NEWTON");
+    return !(e && e[0] == '0');
+  }();
+  return on;
+}
+
 void Engine::inv_into(uint32_t p, const uint32_t* a, size_t la, size_t n, uint32_t* out) {
   la = std::min(la, n);
   const size_t seed = std::min<size_t>(n, 32);
@@ -951,6 +961,13 @@ void Engine::inv_into(uint32_t p, const uint32_t* a, size_t la, size_t n, uint32
     // 1 / a[0] and every doubling step up to 2^13 terms in one CTA
     const size_t K = std::min(n, size_t(1) << newton_inv_max_log());
     kcheck(launch_newton_inv(prime_plan(p).t, a, la, out, 0, K, stream_), "newton inverse");
+    m = K;
+  } else if (crt_newton_on()) {
+    // the same steps with three-prime CRT products, in one CTA
+    const size_t K = std::min(n, size_t(1) << newton_inv_max_log());
+    const PrimeTables aux[3] = {prime_plan(kCrtPrimes[0]).t, prime_plan(kCrtPrimes[1]).t,
+                                prime_plan(kCrtPrimes[2]).t};
+    kcheck(launch_newton_inv_crt(aux, p, a, la, out, K, stream_), "newton inverse (CRT)");
     m = K;
   } else {
     kcheck(launch_seed(0, p, a, la, out, (int)seed, 0, stream_), "inverse seed");

@@ -16,6 +16,7 @@
 //     The spectrum of this factorisation sits at position t*C+u as
 //     X[bitrev_R(t) + R*bitrev_C(u)] = X[bitrev_N(t*C+u)]: exactly the
 //     reference's bit-reversed DIF order.
+#include <cooperative_groups.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -858,6 +859,99 @@ __global__ void __launch_bounds__(kNewtonThreads) k_newton_sqrt(NewtonSqrtD d, P
   for (uint32_t i = tid; i < cs; i += nt) d.c[i] = Cs[i];
 }
 
+// ---------------------------------------------------------------------------
+// Newton inverse at the small sizes for a prime modulus P without the roots of
+// unity (1e9+7, 2^31-1, small primes), on a cluster of three CTAs, one per
+// transform prime 167772161, 469762049, 754974721: the doubling steps of the
+// series inverse (inverse.hpp:18-65), every product a three-prime CRT product
+// (crt_convolution.hpp:25-127).  Each CTA lifts the operands into its prime and
+// runs the cyclic product of 2k points in shared memory; after a cluster
+// barrier every CTA reads the three residue windows (its own and, through
+// distributed shared memory, the other two) and runs Garner back to P, so each
+// holds the new terms for the next product.  The windows are the per-step
+// path's (h = -(a c)[k, 2k) is wrap-free at 2k points; (h c) mod x^k does not
+// wrap) and every coefficient is below k (P-1)^2 < 2^76, inside the three
+// primes' product, so the terms are the same.  c[0] = a[0]^(P-2) mod P.
+// ---------------------------------------------------------------------------
+constexpr int kNewtonCrtSmemWords = 2 * kNewtonPW + (1 << kNewtonMaxLog) + 3 * (1 << (kNewtonMaxLog - 1));
+
+struct NewtonCrtD {
+  const uint32_t* a;  // the series (canonical mod P, a[0] != 0), la terms
+  uint32_t la;
+  uint32_t* c;        // its inverse mod P: c[0, K) on return
+  uint32_t K;         // <= 2^13
+  uint32_t P;         // the modulus, prime
+  Ptab q[3];          // 167772161, 469762049, 754974721
+  uint2 scale_r[3][kNewtonMaxLog + 1];
+  GarnerC g;          // Garner constants with target P
+};
+
+// X[0, N) <- src[0, len) mod the transform prime q, zero beyond.
+__device__ __forceinline__ void crt_lift_load(uint32_t* X, const uint32_t* src, uint32_t len, uint32_t N,
+                                              const Ptab& q, int tid, int nt) {
+  for (uint32_t i = tid; i < N; i += nt) X[pad(i)] = i < len ? reduce_any(src[i], q.q1, q.f) : 0u;
+}
+
+// R[i] = (x y)[off + i] mod q for i < hl, x = x_src[0, xl), y = Cs[0, k), at
+// N = 2^logN points.
+__device__ __forceinline__ void crt_window(const Ptab& q, const uint2* scale_r, const uint32_t* x_src, uint32_t xl,
+                                          const uint32_t* Cs, uint32_t k, uint32_t off, uint32_t hl, int logN,
+                                          uint32_t* X, uint32_t* Y, uint32_t* R, int tid, int nt) {
+  const uint32_t N = 1u << logN;
+  crt_lift_load(X, x_src, xl, N, q, tid, nt);
+  crt_lift_load(Y, Cs, k, N, q, tid, nt);
+  __syncthreads();
+  cta_mul2(X, Y, logN, q, tid, nt);
+  const uint2 sc = scale_r[logN];
+  for (uint32_t i = tid; i < hl; i += nt) R[i] = red(shoup(X[pad(off + i)], sc, q.f.p), q.f.p);
+}
+
+__global__ void __launch_bounds__(kNewtonThreads) k_newton_inv_crt(NewtonCrtD d) {
+  pdl_enter();
+  namespace cg = cooperative_groups;
+  cg::cluster_group cl = cg::this_cluster();
+  extern __shared__ uint32_t smn[];
+  uint32_t* X = smn;
+  uint32_t* Y = smn + kNewtonPW;
+  uint32_t* Cs = smn + 2 * kNewtonPW;       // c[0, K)
+  uint32_t* H = Cs + (1 << kNewtonMaxLog);  // h, < 2^12 terms
+  uint32_t* Ra = H + (1 << (kNewtonMaxLog - 1));   // this prime's residues of the first product
+  uint32_t* Rb = Ra + (1 << (kNewtonMaxLog - 1));  // and of the second (two buffers: one barrier each)
+  const int tid = threadIdx.x, nt = blockDim.x;
+  const unsigned qi = cl.block_rank();
+  const Ptab q = d.q[qi];
+  const uint32_t* ra[3] = {cl.map_shared_rank(Ra, 0), cl.map_shared_rank(Ra, 1), cl.map_shared_rank(Ra, 2)};
+  const uint32_t* rb[3] = {cl.map_shared_rank(Rb, 0), cl.map_shared_rank(Rb, 1), cl.map_shared_rank(Rb, 2)};
+  if (tid == 0) {
+    const uint64_t P = d.P;
+    uint64_t r = 1 % P, b = __ldg(d.a) % P;
+    for (uint32_t e = d.P - 2; e; e >>= 1) {
+      if (e & 1u) r = r * b % P;
+      b = b * b % P;
+    }
+    Cs[0] = (uint32_t)r;
+    if (qi == 0) d.c[0] = (uint32_t)r;
+  }
+  __syncthreads();
+  for (uint32_t k = 1; k < d.K; k <<= 1) {
+    const uint32_t want = min(2 * k, d.K), hl = want - k;
+    const int logN = 32 - __clz(2 * k - 1);
+    // h = -(a c)[k, want) mod P
+    crt_window(q, d.scale_r[qi], d.a, min(d.la, want), Cs, k, k, hl, logN, X, Y, Ra, tid, nt);
+    cl.sync();
+    garner_body(d.g, 3, ra[0], ra[1], ra[2], H, hl, 0, nullptr, 1, 0, 0, hl);
+    __syncthreads();
+    // c[k + i] = (h c)[i] mod P
+    crt_window(q, d.scale_r[qi], H, hl, Cs, k, 0, hl, logN, X, Y, Rb, tid, nt);
+    cl.sync();
+    garner_body(d.g, 3, rb[0], rb[1], rb[2], Cs + k, hl, 0, nullptr, 0, 0, 0, hl);
+    __syncthreads();
+    if (qi == 0)
+      for (uint32_t i = tid; i < hl; i += nt) d.c[k + i] = Cs[k + i];
+  }
+  cl.sync();  // no CTA leaves while another may still read its residues
+}
+
 }  // namespace
 
 namespace fpx {
@@ -882,6 +976,7 @@ cudaError_t kernels_init() {
   set((const void*)k_newton_exp, kNewtonExpSmemWords * 4);
   set((const void*)k_newton_b, kNewtonExpSmemWords * 4);
   set((const void*)k_newton_sqrt, kNewtonSqrtSmemWords * 4);
+  set((const void*)k_newton_inv_crt, kNewtonCrtSmemWords * 4);
   const cudaError_t r = kernels_fast_init();
   const cudaError_t r2 = kernels_batch_init();
   const cudaError_t r3 = kernels_cyc_init();
@@ -2814,3 +2909,40 @@ cudaError_t launch_cyc_small_batch(int logN, unsigned count, const SmallJobB* jo
   return cudaGetLastError();
 }
 }  // namespace
+
+namespace fpx {
+
+cudaError_t launch_newton_inv_crt(const PrimeTables* aux, uint32_t P, const uint32_t* a, size_t la, uint32_t* c,
+                                  size_t K, cudaStream_t s) {
+  static const uint32_t kAux[3] = {167772161u, 469762049u, 754974721u};
+  if (K < 1 || K > (size_t(1) << kNewtonMaxLog) || P < 2) return cudaErrorInvalidValue;
+  for (int i = 0; i < 3; ++i)
+    if (aux[i].p != kAux[i] || aux[i].small_log < kNewtonMaxLog) return cudaErrorInvalidValue;
+  NewtonCrtD d;
+  d.a = a;
+  d.la = (uint32_t)std::min<size_t>(la, K);
+  d.c = c;
+  d.K = (uint32_t)K;
+  d.P = P;
+  for (int i = 0; i < 3; ++i) {
+    d.q[i] = dev_tab(aux[i]);
+    for (int l = 0; l <= kNewtonMaxLog; ++l) d.scale_r[i][l] = shoup_const(aux[i].inv_pow2_r[l], aux[i].p);
+  }
+  d.g = garner_consts(P);
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(3);
+  cfg.blockDim = dim3(kNewtonThreads);
+  cfg.dynamicSmemBytes = (size_t)kNewtonCrtSmemWords * 4;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = 3;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  const cudaError_t e = cudaLaunchKernelEx(&cfg, k_newton_inv_crt, d);
+  return e != cudaSuccess ? e : cudaGetLastError();
+}
+
+}  // namespace fpx

@@ -195,6 +195,11 @@ cudaError_t launch_newton_exp(const PrimeTables& pt, const uint32_t* ap, size_t 
                               uint32_t* c, size_t K, cudaStream_t s);
 cudaError_t launch_newton_inv(const PrimeTables& pt, const uint32_t* a, size_t la, uint32_t* c, size_t k0, size_t K,
                               cudaStream_t s);
+// c[0, K) = 1 / a mod x^K mod the prime P (a canonical, a[0] != 0), every
+// product a three-prime CRT product, in one CTA: aux = the plans of 167772161,
+// 469762049 and 754974721 in that order; K <= 2^newton_inv_max_log().
+cudaError_t launch_newton_inv_crt(const PrimeTables* aux, uint32_t P, const uint32_t* a, size_t la, uint32_t* c,
+                                  size_t K, cudaStream_t s);
 // *res = min (mode 0) / max (mode 1) index with a[i] != 0; caller initialises *res.
 cudaError_t launch_find_nonzero(const uint32_t* a, size_t n, int mode, unsigned long long* res, cudaStream_t s);
 cudaError_t launch_reverse(const uint32_t* a, uint32_t* r, size_t n, cudaStream_t s);

@@ -3,9 +3,10 @@
 FPX_PDL=0 (no programmatic dependent launch), FPX_GRAPHS=0 (no graph replay of
 repeated Newton calls), FPX_AUTOTUNE=0 (default tile shapes) and
 FPX_COL_FACTOR=0 (Bailey twiddles from three small tables per point instead of
-column factors) change how the work is launched, never what it computes: a
-child process with all of them off must print the same checksums as one with
-the defaults.
+column factors) and FPX_CRT_NEWTON=0 (32-term seed and per-step CRT products
+instead of the one-CTA CRT inverse) change how the work is launched, never what
+it computes: a child process with all of them off must print the same
+checksums as one with the defaults.
 """
 import json
 import os
@@ -51,6 +52,7 @@ def _run(env):
 def test_switches_same_values():
     base = dict(os.environ)
     default = _run(base)
-    off = _run(dict(base, FPX_PDL="0", FPX_GRAPHS="0", FPX_AUTOTUNE="0", FPX_COL_FACTOR="0"))
+    off = _run(dict(base, FPX_PDL="0", FPX_GRAPHS="0", FPX_AUTOTUNE="0", FPX_COL_FACTOR="0",
+                    FPX_CRT_NEWTON="0"))
     assert default == off
     assert default["998244353:inv"] == default["998244353:inv2"]
