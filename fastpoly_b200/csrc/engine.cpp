@@ -943,8 +943,20 @@ void Engine::extend_inverse(uint32_t p, const uint32_t* a, size_t la, uint32_t* 
   product(p, e.get(), hlen, c, k, hlen, c + k);
 }
 
-// The fused CRT inverse for the small sizes (k_newton_inv_crt); FPX_CRT_NEWTON=0
-// keeps the 32-term seed and per-step CRT products.
+// How many terms of 1/b the fused exp / sqrt kernels leave after K terms of b:
+// their schedule extends c to each step's length m2 - m by doublings.
+static size_t fused_newton_csize(size_t K) {
+  size_t csize = 1;
+  for (size_t mm = 1; mm < K;) {
+    const size_t h = std::min(2 * mm, K) - mm;
+    while (csize < h) csize = std::min(2 * csize, h);
+    mm += h;
+  }
+  return csize;
+}
+
+// The fused CRT Newton kernels for the small sizes (k_newton_*_crt);
+// FPX_CRT_NEWTON=0 keeps the 32-term seeds and per-step CRT products.
 static bool crt_newton_on() {
   static const bool on = [] {
     const char* e = std::getenv("FPX_CRT_NEWTON");
@@ -1032,12 +1044,15 @@ void Engine::exp_into(uint32_t p, const uint32_t* a, size_t la, size_t n, uint32
     const size_t K = std::min(n, size_t(1) << newton_inv_max_log());
     kcheck(launch_newton_exp(prime_plan(p).t, ap.get(), lap, tab, out, c.get(), K, stream_), "newton exp");
     m = K;
-    csize = 1;
-    for (size_t mm = 1; mm < K;) {
-      const size_t h = std::min(2 * mm, K) - mm;
-      while (csize < h) csize = std::min(2 * csize, h);
-      mm += h;
-    }
+    csize = fused_newton_csize(K);
+  } else if (crt_newton_on()) {
+    // the same steps with three-prime CRT products, on a three-CTA cluster
+    const size_t K = std::min(n, size_t(1) << newton_inv_max_log());
+    const PrimeTables aux[3] = {prime_plan(kCrtPrimes[0]).t, prime_plan(kCrtPrimes[1]).t,
+                                prime_plan(kCrtPrimes[2]).t};
+    kcheck(launch_newton_exp_crt(aux, p, ap.get(), lap, tab, out, c.get(), K, stream_), "newton exp (CRT)");
+    m = K;
+    csize = fused_newton_csize(K);
   } else {
     const size_t seed = std::min<size_t>(n, 32);
     kcheck(launch_seed(1, p, ap.get(), lap, out, (int)seed, 0, stream_), "exp seed");
@@ -1133,12 +1148,15 @@ void Engine::sqrt(uint32_t p, const uint32_t* a, size_t la, size_t n, uint32_t* 
     kcheck(launch_newton_sqrt(prime_plan(p).t, u, ulen, root0, invm(root0, p), b, c.get(), K, stream_),
            "newton sqrt");
     m = K;
-    csize = 1;
-    for (size_t mm = 1; mm < K;) {
-      const size_t h = std::min(2 * mm, K) - mm;
-      while (csize < h) csize = std::min(2 * csize, h);
-      mm += h;
-    }
+    csize = fused_newton_csize(K);
+  } else if (crt_newton_on()) {
+    const size_t K = std::min(inner, size_t(1) << newton_inv_max_log());
+    const PrimeTables aux[3] = {prime_plan(kCrtPrimes[0]).t, prime_plan(kCrtPrimes[1]).t,
+                                prime_plan(kCrtPrimes[2]).t};
+    kcheck(launch_newton_sqrt_crt(aux, p, u, ulen, root0, invm(root0, p), b, c.get(), K, stream_),
+           "newton sqrt (CRT)");
+    m = K;
+    csize = fused_newton_csize(K);
   } else {
     const size_t seed = std::min<size_t>(inner, 32);
     kcheck(launch_seed(2, p, u, std::min(ulen, seed), b, (int)seed, root0, stream_), "sqrt seed");

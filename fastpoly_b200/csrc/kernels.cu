@@ -860,30 +860,57 @@ __global__ void __launch_bounds__(kNewtonThreads) k_newton_sqrt(NewtonSqrtD d, P
 }
 
 // ---------------------------------------------------------------------------
-// Newton inverse at the small sizes for a prime modulus P without the roots of
-// unity (1e9+7, 2^31-1, small primes), on a cluster of three CTAs, one per
-// transform prime 167772161, 469762049, 754974721: the doubling steps of the
-// series inverse (inverse.hpp:18-65), every product a three-prime CRT product
-// (crt_convolution.hpp:25-127).  Each CTA lifts the operands into its prime and
-// runs the cyclic product of 2k points in shared memory; after a cluster
-// barrier every CTA reads the three residue windows (its own and, through
-// distributed shared memory, the other two) and runs Garner back to P, so each
-// holds the new terms for the next product.  The windows are the per-step
-// path's (h = -(a c)[k, 2k) is wrap-free at 2k points; (h c) mod x^k does not
-// wrap) and every coefficient is below k (P-1)^2 < 2^76, inside the three
-// primes' product, so the terms are the same.  c[0] = a[0]^(P-2) mod P.
+// Newton inverse, exponential and square root at the small sizes for a prime
+// modulus P without the roots of unity (1e9+7, 2^31-1, small primes), on a
+// cluster of three CTAs, one per transform prime 167772161, 469762049,
+// 754974721: the doubling steps of inverse.hpp:18-65, exponential.hpp:107-207
+// and square_root.hpp:12-112, every product a three-prime CRT product
+// (crt_convolution.hpp:25-127).  For a product each CTA lifts the operands into
+// its prime and runs the cyclic product of 2k points in shared memory; after a
+// cluster barrier every CTA reads the three residue windows (its own and,
+// through distributed shared memory, the other two) and runs Garner back to P,
+// so each CTA holds the product's terms for the next one.  Two residue buffers
+// alternate, so one cluster barrier per product suffices: a CTA overwrites a
+// buffer only after the next product's barrier, which every CTA reaches after
+// reading it.  The windows are the per-step path's (wrap-free at 2k points)
+// and every coefficient is below 2^13 (P-1)^2 < 2^75, inside the three primes'
+// product, so the terms are the same.
 // ---------------------------------------------------------------------------
-constexpr int kNewtonCrtSmemWords = 2 * kNewtonPW + (1 << kNewtonMaxLog) + 3 * (1 << (kNewtonMaxLog - 1));
+constexpr int kNewtonCrtSmemWords = 2 * kNewtonPW + (1 << kNewtonMaxLog) + 4 * (1 << (kNewtonMaxLog - 1));
+constexpr uint32_t kCrtHW = 1u << (kNewtonMaxLog - 1);
+
+struct CrtCl {
+  Ptab q[3];  // 167772161, 469762049, 754974721
+  uint2 scale_r[3][kNewtonMaxLog + 1];
+  GarnerC g;      // Garner constants with target P
+  uint32_t P;     // the modulus, prime
+  uint32_t pinv;  // P^-1 mod 2^32 (Montgomery products in the target field, P odd)
+};
 
 struct NewtonCrtD {
   const uint32_t* a;  // the series (canonical mod P, a[0] != 0), la terms
   uint32_t la;
   uint32_t* c;        // its inverse mod P: c[0, K) on return
   uint32_t K;         // <= 2^13
-  uint32_t P;         // the modulus, prime
-  Ptab q[3];          // 167772161, 469762049, 754974721
-  uint2 scale_r[3][kNewtonMaxLog + 1];
-  GarnerC g;          // Garner constants with target P
+  CrtCl cc;
+};
+struct NewtonExpCrtD {
+  const uint32_t* ap;   // a' (canonical), lap terms
+  uint32_t lap;
+  const uint32_t* tab;  // 1/i mod P in Montgomery form, i < K
+  uint32_t* b;          // exp(a): b[0, K)
+  uint32_t* c;          // 1/b: c[0, cs) on return (cs as the host computes it)
+  uint32_t K;
+  CrtCl cc;
+};
+struct NewtonSqrtCrtD {
+  const uint32_t* u;  // the series with u[0] a nonzero square (canonical), ulen terms
+  uint32_t ulen;
+  uint32_t* b;        // sqrt(u): b[0, K)
+  uint32_t* c;        // 1/b: c[0, cs) on return
+  uint32_t K;
+  uint32_t root, root_inv;
+  CrtCl cc;
 };
 
 // X[0, N) <- src[0, len) mod the transform prime q, zero beyond.
@@ -892,18 +919,42 @@ __device__ __forceinline__ void crt_lift_load(uint32_t* X, const uint32_t* src, 
   for (uint32_t i = tid; i < N; i += nt) X[pad(i)] = i < len ? reduce_any(src[i], q.q1, q.f) : 0u;
 }
 
-// R[i] = (x y)[off + i] mod q for i < hl, x = x_src[0, xl), y = Cs[0, k), at
-// N = 2^logN points.
-__device__ __forceinline__ void crt_window(const Ptab& q, const uint2* scale_r, const uint32_t* x_src, uint32_t xl,
-                                          const uint32_t* Cs, uint32_t k, uint32_t off, uint32_t hl, int logN,
-                                          uint32_t* X, uint32_t* Y, uint32_t* R, int tid, int nt) {
+// out[i] = (x y)[off + i] mod P for i < hl (negated, or times post[i] in
+// Montgomery form, on request), x = x[0, xl), y = y[0, yl), at N = 2^logN
+// points; out in every CTA's shared memory.  All of the cluster's CTAs call it
+// with the same arguments.
+__device__ __forceinline__ void crt_cl_window(const CrtCl& cc, const uint32_t* x, uint32_t xl, const uint32_t* y,
+                                             uint32_t yl, uint32_t off, uint32_t hl, int logN, uint32_t* X,
+                                             uint32_t* Y, uint32_t* R2, int& par, uint32_t* out, int negate,
+                                             const uint32_t* post, int tid, int nt) {
+  namespace cg = cooperative_groups;
+  cg::cluster_group cl = cg::this_cluster();
+  const unsigned qi = cl.block_rank();
+  const Ptab q = cc.q[qi];
+  uint32_t* R = R2 + par * kCrtHW;
   const uint32_t N = 1u << logN;
-  crt_lift_load(X, x_src, xl, N, q, tid, nt);
-  crt_lift_load(Y, Cs, k, N, q, tid, nt);
+  crt_lift_load(X, x, xl, N, q, tid, nt);
+  crt_lift_load(Y, y, yl, N, q, tid, nt);
   __syncthreads();
   cta_mul2(X, Y, logN, q, tid, nt);
-  const uint2 sc = scale_r[logN];
+  const uint2 sc = cc.scale_r[qi][logN];
   for (uint32_t i = tid; i < hl; i += nt) R[i] = red(shoup(X[pad(off + i)], sc, q.f.p), q.f.p);
+  cl.sync();
+  garner_body(cc.g, 3, cl.map_shared_rank(R, 0), cl.map_shared_rank(R, 1), cl.map_shared_rank(R, 2), out, hl, 0,
+              post, negate, cc.pinv, 0, hl);
+  __syncthreads();
+  par ^= 1;
+}
+
+// One doubling step of the series inverse: Cs[k, want) from Cs[0, k) and the
+// first aw terms of the series (H: scratch of want - k words).
+__device__ __forceinline__ void crt_cl_inv_step(const CrtCl& cc, const uint32_t* series, uint32_t aw, uint32_t* Cs,
+                                               uint32_t k, uint32_t want, uint32_t* X, uint32_t* Y, uint32_t* H,
+                                               uint32_t* R2, int& par, int tid, int nt) {
+  const uint32_t hl = want - k;
+  const int logN = 32 - __clz(2 * k - 1);
+  crt_cl_window(cc, series, aw, Cs, k, k, hl, logN, X, Y, R2, par, H, 1, nullptr, tid, nt);  // -(a c)[k, want)
+  crt_cl_window(cc, H, hl, Cs, k, 0, hl, logN, X, Y, R2, par, Cs + k, 0, nullptr, tid, nt);  // (h c) mod x^hl
 }
 
 __global__ void __launch_bounds__(kNewtonThreads) k_newton_inv_crt(NewtonCrtD d) {
@@ -915,41 +966,123 @@ __global__ void __launch_bounds__(kNewtonThreads) k_newton_inv_crt(NewtonCrtD d)
   uint32_t* Y = smn + kNewtonPW;
   uint32_t* Cs = smn + 2 * kNewtonPW;       // c[0, K)
   uint32_t* H = Cs + (1 << kNewtonMaxLog);  // h, < 2^12 terms
-  uint32_t* Ra = H + (1 << (kNewtonMaxLog - 1));   // this prime's residues of the first product
-  uint32_t* Rb = Ra + (1 << (kNewtonMaxLog - 1));  // and of the second (two buffers: one barrier each)
+  uint32_t* R2 = H + kCrtHW;                // two residue buffers
   const int tid = threadIdx.x, nt = blockDim.x;
-  const unsigned qi = cl.block_rank();
-  const Ptab q = d.q[qi];
-  const uint32_t* ra[3] = {cl.map_shared_rank(Ra, 0), cl.map_shared_rank(Ra, 1), cl.map_shared_rank(Ra, 2)};
-  const uint32_t* rb[3] = {cl.map_shared_rank(Rb, 0), cl.map_shared_rank(Rb, 1), cl.map_shared_rank(Rb, 2)};
-  if (tid == 0) {
-    const uint64_t P = d.P;
+  const bool lead = cl.block_rank() == 0;
+  if (tid == 0) {  // c[0] = a[0]^(P-2) mod P
+    const uint64_t P = d.cc.P;
     uint64_t r = 1 % P, b = __ldg(d.a) % P;
-    for (uint32_t e = d.P - 2; e; e >>= 1) {
+    for (uint32_t e = d.cc.P - 2; e; e >>= 1) {
       if (e & 1u) r = r * b % P;
       b = b * b % P;
     }
     Cs[0] = (uint32_t)r;
-    if (qi == 0) d.c[0] = (uint32_t)r;
+    if (lead) d.c[0] = (uint32_t)r;
   }
   __syncthreads();
+  int par = 0;
   for (uint32_t k = 1; k < d.K; k <<= 1) {
-    const uint32_t want = min(2 * k, d.K), hl = want - k;
-    const int logN = 32 - __clz(2 * k - 1);
-    // h = -(a c)[k, want) mod P
-    crt_window(q, d.scale_r[qi], d.a, min(d.la, want), Cs, k, k, hl, logN, X, Y, Ra, tid, nt);
-    cl.sync();
-    garner_body(d.g, 3, ra[0], ra[1], ra[2], H, hl, 0, nullptr, 1, 0, 0, hl);
-    __syncthreads();
-    // c[k + i] = (h c)[i] mod P
-    crt_window(q, d.scale_r[qi], H, hl, Cs, k, 0, hl, logN, X, Y, Rb, tid, nt);
-    cl.sync();
-    garner_body(d.g, 3, rb[0], rb[1], rb[2], Cs + k, hl, 0, nullptr, 0, 0, 0, hl);
-    __syncthreads();
-    if (qi == 0)
-      for (uint32_t i = tid; i < hl; i += nt) d.c[k + i] = Cs[k + i];
+    const uint32_t want = min(2 * k, d.K);
+    crt_cl_inv_step(d.cc, d.a, min(d.la, want), Cs, k, want, X, Y, H, R2, par, tid, nt);
+    if (lead)
+      for (uint32_t i = k + tid; i < want; i += nt) d.c[i] = Cs[i];
   }
   cl.sync();  // no CTA leaves while another may still read its residues
+}
+
+__global__ void __launch_bounds__(kNewtonThreads) k_newton_exp_crt(NewtonExpCrtD d) {
+  pdl_enter();
+  namespace cg = cooperative_groups;
+  cg::cluster_group cl = cg::this_cluster();
+  extern __shared__ uint32_t smn[];
+  uint32_t* X = smn;
+  uint32_t* Y = smn + kNewtonPW;
+  uint32_t* B = smn + 2 * kNewtonPW;        // b[0, K)
+  uint32_t* Cs = B + (1 << kNewtonMaxLog);  // c, < 2^12 terms
+  uint32_t* T = Cs + kCrtHW;
+  uint32_t* R2 = T + kCrtHW;
+  const int tid = threadIdx.x, nt = blockDim.x;
+  const bool lead = cl.block_rank() == 0;
+  if (tid == 0) {
+    B[0] = 1u;
+    Cs[0] = 1u;
+    if (lead) d.b[0] = 1u;
+  }
+  __syncthreads();
+  int par = 0;
+  uint32_t m = 1, cs = 1;
+  while (m < d.K) {
+    const uint32_t m2 = min(2 * m, d.K), hl = m2 - m;
+    while (cs < hl) {
+      const uint32_t want = min(2 * cs, hl);
+      crt_cl_inv_step(d.cc, B, min(m, want), Cs, cs, want, X, Y, T, R2, par, tid, nt);
+      cs = want;
+    }
+    const int logN = 32 - __clz(2 * m - 1);
+    // t1 = (a' b)[m-1, m-1+hl); t2 = (t1 c) mod x^hl times 1/(m+i); b[m + i] = (t2 b)[i]
+    crt_cl_window(d.cc, d.ap, min(d.lap, m2 - 1), B, m, m - 1, hl, logN, X, Y, R2, par, T, 0, nullptr, tid, nt);
+    crt_cl_window(d.cc, T, hl, Cs, cs, 0, hl, logN, X, Y, R2, par, T, 0, d.tab + m, tid, nt);
+    crt_cl_window(d.cc, T, hl, B, m, 0, hl, logN, X, Y, R2, par, B + m, 0, nullptr, tid, nt);
+    if (lead)
+      for (uint32_t i = tid; i < hl; i += nt) d.b[m + i] = B[m + i];
+    m = m2;
+  }
+  if (lead)
+    for (uint32_t i = tid; i < cs; i += nt) d.c[i] = Cs[i];
+  cl.sync();
+}
+
+__global__ void __launch_bounds__(kNewtonThreads) k_newton_sqrt_crt(NewtonSqrtCrtD d) {
+  pdl_enter();
+  namespace cg = cooperative_groups;
+  cg::cluster_group cl = cg::this_cluster();
+  extern __shared__ uint32_t smn[];
+  uint32_t* X = smn;
+  uint32_t* Y = smn + kNewtonPW;
+  uint32_t* B = smn + 2 * kNewtonPW;        // b[0, K)
+  uint32_t* Cs = B + (1 << kNewtonMaxLog);  // c, < 2^12 terms
+  uint32_t* T = Cs + kCrtHW;
+  uint32_t* R2 = T + kCrtHW;
+  const int tid = threadIdx.x, nt = blockDim.x;
+  const bool lead = cl.block_rank() == 0;
+  const uint32_t P = d.cc.P;
+  if (tid == 0) {
+    B[0] = d.root;
+    Cs[0] = d.root_inv;
+    if (lead) d.b[0] = d.root;
+  }
+  __syncthreads();
+  int par = 0;
+  uint32_t m = 1, cs = 1;
+  while (m < d.K) {
+    const uint32_t m2 = min(2 * m, d.K), hl = m2 - m;
+    while (cs < hl) {
+      const uint32_t want = min(2 * cs, hl);
+      crt_cl_inv_step(d.cc, B, min(m, want), Cs, cs, want, X, Y, T, R2, par, tid, nt);
+      cs = want;
+    }
+    const int logN = 32 - __clz(2 * m - 1);
+    // t = u[m + i] - (b^2)[m + i];  b[m + i] = (t c)[i] / 2
+    crt_cl_window(d.cc, B, m, B, m, m, hl, logN, X, Y, R2, par, T, 0, nullptr, tid, nt);
+    for (uint32_t i = tid; i < hl; i += nt) {
+      const uint32_t v = T[i];
+      const uint32_t su = m + i < d.ulen ? d.u[m + i] : 0u;
+      T[i] = su >= v ? su - v : su + P - v;
+    }
+    __syncthreads();
+    crt_cl_window(d.cc, T, hl, Cs, cs, 0, hl, logN, X, Y, R2, par, B + m, 0, nullptr, tid, nt);
+    for (uint32_t i = tid; i < hl; i += nt) {
+      const uint32_t v = B[m + i];
+      const uint32_t h = (v & 1u) ? (uint32_t)(((uint64_t)v + P) >> 1) : v >> 1;  // v / 2 mod P (P odd)
+      B[m + i] = h;
+      if (lead) d.b[m + i] = h;
+    }
+    __syncthreads();
+    m = m2;
+  }
+  if (lead)
+    for (uint32_t i = tid; i < cs; i += nt) d.c[i] = Cs[i];
+  cl.sync();
 }
 
 }  // namespace
@@ -977,6 +1110,8 @@ cudaError_t kernels_init() {
   set((const void*)k_newton_b, kNewtonExpSmemWords * 4);
   set((const void*)k_newton_sqrt, kNewtonSqrtSmemWords * 4);
   set((const void*)k_newton_inv_crt, kNewtonCrtSmemWords * 4);
+  set((const void*)k_newton_exp_crt, kNewtonCrtSmemWords * 4);
+  set((const void*)k_newton_sqrt_crt, kNewtonCrtSmemWords * 4);
   const cudaError_t r = kernels_fast_init();
   const cudaError_t r2 = kernels_batch_init();
   const cudaError_t r3 = kernels_cyc_init();
@@ -2912,23 +3047,24 @@ cudaError_t launch_cyc_small_batch(int logN, unsigned count, const SmallJobB* jo
 
 namespace fpx {
 
-cudaError_t launch_newton_inv_crt(const PrimeTables* aux, uint32_t P, const uint32_t* a, size_t la, uint32_t* c,
-                                  size_t K, cudaStream_t s) {
+namespace {
+bool crt_cl_fill(const PrimeTables* aux, uint32_t P, CrtCl& cc) {
   static const uint32_t kAux[3] = {167772161u, 469762049u, 754974721u};
-  if (K < 1 || K > (size_t(1) << kNewtonMaxLog) || P < 2) return cudaErrorInvalidValue;
-  for (int i = 0; i < 3; ++i)
-    if (aux[i].p != kAux[i] || aux[i].small_log < kNewtonMaxLog) return cudaErrorInvalidValue;
-  NewtonCrtD d;
-  d.a = a;
-  d.la = (uint32_t)std::min<size_t>(la, K);
-  d.c = c;
-  d.K = (uint32_t)K;
-  d.P = P;
+  if (P < 2) return false;
   for (int i = 0; i < 3; ++i) {
-    d.q[i] = dev_tab(aux[i]);
-    for (int l = 0; l <= kNewtonMaxLog; ++l) d.scale_r[i][l] = shoup_const(aux[i].inv_pow2_r[l], aux[i].p);
+    if (aux[i].p != kAux[i] || aux[i].small_log < kNewtonMaxLog) return false;
+    cc.q[i] = dev_tab(aux[i]);
+    for (int l = 0; l <= kNewtonMaxLog; ++l) cc.scale_r[i][l] = shoup_const(aux[i].inv_pow2_r[l], aux[i].p);
   }
-  d.g = garner_consts(P);
+  cc.g = garner_consts(P);
+  cc.P = P;
+  cc.pinv = (P & 1u) ? inv_mod_2_32(P) : 0u;
+  return true;
+}
+
+// One cluster of three CTAs, one per transform prime.
+template <typename D>
+cudaError_t crt_cl_launch(void (*k)(D), const D& d, cudaStream_t s) {
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(3);
   cfg.blockDim = dim3(kNewtonThreads);
@@ -2941,8 +3077,49 @@ cudaError_t launch_newton_inv_crt(const PrimeTables* aux, uint32_t P, const uint
   attr[0].val.clusterDim.z = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  const cudaError_t e = cudaLaunchKernelEx(&cfg, k_newton_inv_crt, d);
+  const cudaError_t e = cudaLaunchKernelEx(&cfg, k, d);
   return e != cudaSuccess ? e : cudaGetLastError();
+}
+}  // namespace
+
+cudaError_t launch_newton_inv_crt(const PrimeTables* aux, uint32_t P, const uint32_t* a, size_t la, uint32_t* c,
+                                  size_t K, cudaStream_t s) {
+  NewtonCrtD d;
+  if (K < 1 || K > (size_t(1) << kNewtonMaxLog) || !crt_cl_fill(aux, P, d.cc)) return cudaErrorInvalidValue;
+  d.a = a;
+  d.la = (uint32_t)std::min<size_t>(la, K);
+  d.c = c;
+  d.K = (uint32_t)K;
+  return crt_cl_launch(k_newton_inv_crt, d, s);
+}
+
+cudaError_t launch_newton_exp_crt(const PrimeTables* aux, uint32_t P, const uint32_t* ap, size_t lap,
+                                  const uint32_t* tab, uint32_t* b, uint32_t* c, size_t K, cudaStream_t s) {
+  NewtonExpCrtD d;
+  if (K < 2 || K > (size_t(1) << kNewtonMaxLog) || !(P & 1u) || !crt_cl_fill(aux, P, d.cc))
+    return cudaErrorInvalidValue;
+  d.ap = ap;
+  d.lap = (uint32_t)std::min<size_t>(lap, K);
+  d.tab = tab;
+  d.b = b;
+  d.c = c;
+  d.K = (uint32_t)K;
+  return crt_cl_launch(k_newton_exp_crt, d, s);
+}
+
+cudaError_t launch_newton_sqrt_crt(const PrimeTables* aux, uint32_t P, const uint32_t* u, size_t ulen, uint32_t root,
+                                   uint32_t root_inv, uint32_t* b, uint32_t* c, size_t K, cudaStream_t s) {
+  NewtonSqrtCrtD d;
+  if (K < 1 || K > (size_t(1) << kNewtonMaxLog) || !(P & 1u) || !crt_cl_fill(aux, P, d.cc))
+    return cudaErrorInvalidValue;
+  d.u = u;
+  d.ulen = (uint32_t)std::min<size_t>(ulen, K);
+  d.b = b;
+  d.c = c;
+  d.K = (uint32_t)K;
+  d.root = root;
+  d.root_inv = root_inv;
+  return crt_cl_launch(k_newton_sqrt_crt, d, s);
 }
 
 }  // namespace fpx

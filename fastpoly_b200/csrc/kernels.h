@@ -200,6 +200,12 @@ cudaError_t launch_newton_inv(const PrimeTables& pt, const uint32_t* a, size_t l
 // 469762049 and 754974721 in that order; K <= 2^newton_inv_max_log().
 cudaError_t launch_newton_inv_crt(const PrimeTables* aux, uint32_t P, const uint32_t* a, size_t la, uint32_t* c,
                                   size_t K, cudaStream_t s);
+// The exponential and square-root counterparts of launch_newton_exp / _sqrt for
+// such a modulus (P odd): b[0, K) and c = 1/b on the same schedule.
+cudaError_t launch_newton_exp_crt(const PrimeTables* aux, uint32_t P, const uint32_t* ap, size_t lap,
+                                  const uint32_t* tab, uint32_t* b, uint32_t* c, size_t K, cudaStream_t s);
+cudaError_t launch_newton_sqrt_crt(const PrimeTables* aux, uint32_t P, const uint32_t* u, size_t ulen, uint32_t root,
+                                   uint32_t root_inv, uint32_t* b, uint32_t* c, size_t K, cudaStream_t s);
 // *res = min (mode 0) / max (mode 1) index with a[i] != 0; caller initialises *res.
 cudaError_t launch_find_nonzero(const uint32_t* a, size_t n, int mode, unsigned long long* res, cudaStream_t s);
 cudaError_t launch_reverse(const uint32_t* a, uint32_t* r, size_t n, cudaStream_t s);

@@ -3,8 +3,8 @@
 FPX_PDL=0 (no programmatic dependent launch), FPX_GRAPHS=0 (no graph replay of
 repeated Newton calls), FPX_AUTOTUNE=0 (default tile shapes) and
 FPX_COL_FACTOR=0 (Bailey twiddles from three small tables per point instead of
-column factors) and FPX_CRT_NEWTON=0 (32-term seed and per-step CRT products
-instead of the one-CTA CRT inverse) change how the work is launched, never what
+column factors) and FPX_CRT_NEWTON=0 (32-term seeds and per-step CRT products
+instead of the cluster CRT Newton kernels) change how the work is launched, never what
 it computes: a child process with all of them off must print the same
 checksums as one with the defaults.
 """
