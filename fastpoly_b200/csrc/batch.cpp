@@ -414,7 +414,10 @@ void Engine::batch(fpx_job* jobs, size_t count) {
         route[i] = kNone;
         continue;
       }
-      const bool small = native(p, newton_inv_max_log()) && j.n <= (size_t(1) << newton_inv_max_log());
+      // one CTA (transform primes) or one cluster of three (CRT, odd p for exp)
+      const bool small = j.n <= (size_t(1) << newton_inv_max_log()) &&
+                         (native(p, newton_inv_max_log()) ||
+                          (crt_newton_on() && (route[i] != kExp || (p & 1u))));
       if (small && route[i] == kInv) route[i] = kInvF;
       if (small && route[i] == kExp && std::min(j.la, j.n) > 1 && j.n > 1) route[i] = kExpF;
     }
@@ -503,16 +506,32 @@ void Engine::batch(fpx_job* jobs, size_t count) {
     std::vector<ExpPrep> preps;
     std::vector<SeedJob> seeds1, seeds2;
     std::vector<NewtonJob> fused;
+    PrimeTables aux3[3];  // the CRT primes' plans, for the cluster jobs
+    bool aux_set = false;
+    auto crt_aux = [&]() -> const PrimeTables* {
+      if (!aux_set) {
+        const uint32_t ps[3] = {167772161u, 469762049u, 754974721u};
+        for (int t = 0; t < 3; ++t) aux3[t] = prime_plan(ps[t]).t;
+        aux_set = true;
+      }
+      return aux3;
+    };
     for (size_t i = 0; i < count; ++i) {
       fpx_job& j = jobs[i];
       const size_t n = j.n, cnt = std::min(j.la, n);
+      const bool nat = native(j.p, newton_inv_max_log());
       if (route[i] == kInvF) {
-        fused.push_back(NewtonJob{0, &prime_plan(j.p).t, j.a, cnt, nullptr, j.out, nullptr, n});
+        if (nat) fused.push_back(NewtonJob{0, &prime_plan(j.p).t, j.a, cnt, nullptr, j.out, nullptr, n});
+        else fused.push_back(NewtonJob{0, nullptr, j.a, cnt, nullptr, j.out, nullptr, n, crt_aux(), j.p});
       } else if (route[i] == kExpF) {
         uint32_t* ap = take(n);
         preps.push_back(ExpPrep{j.p, j.a, cnt, ap, j.out, n});  // a' (and out = 1, 0, ...)
-        fused.push_back(NewtonJob{1, &prime_plan(j.p).t, ap, cnt - 1, inv_table(j.p, n - 1), j.out,
-                                  take(n / 2 + 64), n});
+        if (nat)
+          fused.push_back(NewtonJob{1, &prime_plan(j.p).t, ap, cnt - 1, inv_table(j.p, n - 1), j.out,
+                                    take(n / 2 + 64), n});
+        else
+          fused.push_back(NewtonJob{1, nullptr, ap, cnt - 1, inv_table(j.p, n - 1), j.out, take(n / 2 + 64), n,
+                                    crt_aux(), j.p});
       } else if (route[i] == kInv) {
         InvT t{j.p, j.a, cnt, n, j.out, take(2 * n), take(n)};
         invs.push_back(t);
@@ -588,6 +607,10 @@ void Engine::batch(fpx_job* jobs, size_t count) {
       }
     } side_join{*this};
     if (!fused.empty()) {
+      // one launch for the one-CTA jobs, one for the cluster jobs
+      bool any_nat = false, any_crt = false;
+      for (const NewtonJob& x : fused) (x.aux ? any_crt : any_nat) = true;
+      const int newton_kernels = (int)any_nat + (int)any_crt;
       Stage& st = stage(batch_newton_bytes(fused.size()));
       fdesc = Buf(&pool_, batch_newton_bytes(fused.size()) / 4 + 1);
       if (side) {
@@ -595,11 +618,12 @@ void Engine::batch(fpx_job* jobs, size_t count) {
         check(cudaStreamWaitEvent(side_, side_fork_, 0), "cudaStreamWaitEvent");
         side_join.active = true;
         check(launch_newton_batch(fused, st.host, fdesc.get(), side_, st.ev), "newton");
-        ++launches_;
+        launches_ += newton_kernels;
       } else {
         prof_begin();
         check(launch_newton_batch(fused, st.host, fdesc.get(), stream_, st.ev), "newton");
         prof_end("newton");
+        launches_ += newton_kernels - 1;  // prof_end counted one
       }
     }
     if (!seeds1.empty()) {

@@ -957,7 +957,7 @@ static size_t fused_newton_csize(size_t K) {
 
 // The fused CRT Newton kernels for the small sizes (k_newton_*_crt);
 // FPX_CRT_NEWTON=0 keeps the 32-term seeds and per-step CRT products.
-static bool crt_newton_on() {
+bool crt_newton_on() {
   static const bool on = [] {
     const char* e = std::getenv("FPX_CRT_NEWTON");
     return !(e && e[0] == '0');

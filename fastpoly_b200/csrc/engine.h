@@ -97,6 +97,10 @@ struct BigPlan {
   Buf lo_fwd, mid_fwd, hi_fwd, lo_inv, lo_inv_r, mid_inv, hi_inv, cf_fwd, cf_inv;
 };
 
+// The cluster CRT Newton kernels for small series modulo primes without
+// 2^13-th roots of unity (FPX_CRT_NEWTON=0 turns them off).
+bool crt_newton_on();
+
 // Host-side number theory.
 uint32_t powm(uint32_t a, uint64_t e, uint32_t p);
 uint32_t invm(uint32_t a, uint32_t p);

@@ -957,8 +957,7 @@ __device__ __forceinline__ void crt_cl_inv_step(const CrtCl& cc, const uint32_t*
   crt_cl_window(cc, H, hl, Cs, k, 0, hl, logN, X, Y, R2, par, Cs + k, 0, nullptr, tid, nt);  // (h c) mod x^hl
 }
 
-__global__ void __launch_bounds__(kNewtonThreads) k_newton_inv_crt(NewtonCrtD d) {
-  pdl_enter();
+__device__ __forceinline__ void newton_inv_crt_body(const NewtonCrtD& d) {
   namespace cg = cooperative_groups;
   cg::cluster_group cl = cg::this_cluster();
   extern __shared__ uint32_t smn[];
@@ -990,8 +989,7 @@ __global__ void __launch_bounds__(kNewtonThreads) k_newton_inv_crt(NewtonCrtD d)
   cl.sync();  // no CTA leaves while another may still read its residues
 }
 
-__global__ void __launch_bounds__(kNewtonThreads) k_newton_exp_crt(NewtonExpCrtD d) {
-  pdl_enter();
+__device__ __forceinline__ void newton_exp_crt_body(const NewtonExpCrtD& d) {
   namespace cg = cooperative_groups;
   cg::cluster_group cl = cg::this_cluster();
   extern __shared__ uint32_t smn[];
@@ -1030,6 +1028,30 @@ __global__ void __launch_bounds__(kNewtonThreads) k_newton_exp_crt(NewtonExpCrtD
   if (lead)
     for (uint32_t i = tid; i < cs; i += nt) d.c[i] = Cs[i];
   cl.sync();
+}
+
+__global__ void __launch_bounds__(kNewtonThreads) k_newton_inv_crt(NewtonCrtD d) {
+  pdl_enter();
+  newton_inv_crt_body(d);
+}
+
+__global__ void __launch_bounds__(kNewtonThreads) k_newton_exp_crt(NewtonExpCrtD d) {
+  pdl_enter();
+  newton_exp_crt_body(d);
+}
+
+// Many small CRT Newton inverses and exponentials (batches): one cluster of
+// three CTAs per job, the job's descriptor read from global memory.
+struct NewtonCrtJobB {
+  int kind;  // 0 inverse, 1 exponential
+  NewtonCrtD inv;
+  NewtonExpCrtD exp;
+};
+__global__ void __launch_bounds__(kNewtonThreads) k_newton_crt_b(const NewtonCrtJobB* __restrict__ jobs) {
+  pdl_enter();
+  const NewtonCrtJobB& j = jobs[blockIdx.x / 3];
+  if (j.kind == 0) newton_inv_crt_body(j.inv);
+  else newton_exp_crt_body(j.exp);
 }
 
 __global__ void __launch_bounds__(kNewtonThreads) k_newton_sqrt_crt(NewtonSqrtCrtD d) {
@@ -1112,6 +1134,7 @@ cudaError_t kernels_init() {
   set((const void*)k_newton_inv_crt, kNewtonCrtSmemWords * 4);
   set((const void*)k_newton_exp_crt, kNewtonCrtSmemWords * 4);
   set((const void*)k_newton_sqrt_crt, kNewtonCrtSmemWords * 4);
+  set((const void*)k_newton_crt_b, kNewtonCrtSmemWords * 4);
   const cudaError_t r = kernels_fast_init();
   const cudaError_t r2 = kernels_batch_init();
   const cudaError_t r3 = kernels_cyc_init();
@@ -1494,32 +1517,51 @@ void fill_newton_exp(NewtonExpD& d, const PrimeTables& pt, const uint32_t* ap, s
 }
 }  // namespace
 
-size_t batch_newton_bytes(size_t jobs) { return jobs * sizeof(NewtonJobB) + 256; }
+size_t batch_newton_bytes(size_t jobs) {
+  return jobs * std::max(sizeof(NewtonJobB), sizeof(NewtonCrtJobB)) + 512;
+}
+
+// The CRT jobs of a batch (defined with the cluster launchers below).
+cudaError_t fill_newton_crt_batch(const std::vector<const NewtonJob*>& jobs, void* host);
+cudaError_t launch_newton_crt_b(const void* dev, size_t count, cudaStream_t s);
 
 cudaError_t launch_newton_batch(const std::vector<NewtonJob>& jobs, void* host_staging, void* dev_desc,
                                 cudaStream_t s, cudaEvent_t staged) {
   if (jobs.empty()) return cudaSuccess;
-  std::vector<NewtonJobB> v(jobs.size());
-  for (size_t i = 0; i < jobs.size(); ++i) {
+  std::vector<const NewtonJob*> crt;
+  for (const NewtonJob& x : jobs)
+    if (x.aux) crt.push_back(&x);
+  std::vector<NewtonJobB> v(jobs.size() - crt.size());
+  for (size_t i = 0, vi = 0; i < jobs.size(); ++i) {
     const NewtonJob& x = jobs[i];
+    if (x.aux) continue;
     const PrimeTables& pt = *x.pt;
     if (x.K < 1 || x.K > (size_t(1) << kNewtonMaxLog) || (size_t(1) << pt.small_log) < x.K || !(pt.p & 1u) ||
         pt.p >= (1u << 30) || (x.kind == 1 && x.K < 2))
       return cudaErrorInvalidValue;
-    NewtonJobB& j = v[i];
+    NewtonJobB& j = v[vi++];
     std::memset(&j, 0, sizeof j);
     j.kind = x.kind;
     j.pt = dev_tab(pt);
     if (x.kind == 0) fill_newton_inv(j.inv, pt, x.a, x.la, x.out, x.K);
     else fill_newton_exp(j.exp, pt, x.a, x.la, x.tab, x.out, x.c, x.K);
   }
+  // descriptors: the one-CTA jobs, then (256-byte aligned) the cluster jobs
+  const size_t off = (v.size() * sizeof(NewtonJobB) + 255) & ~size_t(255);
   std::memcpy(host_staging, v.data(), v.size() * sizeof(NewtonJobB));
-  cudaError_t e = cudaMemcpyAsync(dev_desc, host_staging, v.size() * sizeof(NewtonJobB), cudaMemcpyHostToDevice, s);
+  cudaError_t e = cudaSuccess;
+  if (!crt.empty() && (e = fill_newton_crt_batch(crt, static_cast<char*>(host_staging) + off)) != cudaSuccess)
+    return e;
+  const size_t bytes = crt.empty() ? v.size() * sizeof(NewtonJobB) : off + crt.size() * sizeof(NewtonCrtJobB);
+  e = cudaMemcpyAsync(dev_desc, host_staging, bytes, cudaMemcpyHostToDevice, s);
   if (e != cudaSuccess) return e;
   if (staged && (e = cudaEventRecord(staged, s)) != cudaSuccess) return e;
-  (void)pdl_launch(k_newton_b, (unsigned)v.size(), kNewtonThreads, (size_t)kNewtonExpSmemWords * 4, s,
-                   static_cast<const NewtonJobB*>(dev_desc));
-  return cudaGetLastError();
+  if (!v.empty())
+    (void)pdl_launch(k_newton_b, (unsigned)v.size(), kNewtonThreads, (size_t)kNewtonExpSmemWords * 4, s,
+                     static_cast<const NewtonJobB*>(dev_desc));
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  if (!crt.empty()) return launch_newton_crt_b(static_cast<const char*>(dev_desc) + off, crt.size(), s);
+  return cudaSuccess;
 }
 
 cudaError_t launch_newton_sqrt(const PrimeTables& pt, const uint32_t* u, size_t ulen, uint32_t root, uint32_t root_inv,
@@ -3064,9 +3106,9 @@ bool crt_cl_fill(const PrimeTables* aux, uint32_t P, CrtCl& cc) {
 
 // One cluster of three CTAs, one per transform prime.
 template <typename D>
-cudaError_t crt_cl_launch(void (*k)(D), const D& d, cudaStream_t s) {
+cudaError_t crt_cl_launch(void (*k)(D), const D& d, cudaStream_t s, unsigned clusters = 1) {
   cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = dim3(3);
+  cfg.gridDim = dim3(3 * clusters);
   cfg.blockDim = dim3(kNewtonThreads);
   cfg.dynamicSmemBytes = (size_t)kNewtonCrtSmemWords * 4;
   cfg.stream = s;
@@ -3105,6 +3147,41 @@ cudaError_t launch_newton_exp_crt(const PrimeTables* aux, uint32_t P, const uint
   d.c = c;
   d.K = (uint32_t)K;
   return crt_cl_launch(k_newton_exp_crt, d, s);
+}
+
+cudaError_t fill_newton_crt_batch(const std::vector<const NewtonJob*>& jobs, void* host) {
+  auto* out = static_cast<NewtonCrtJobB*>(host);
+  for (size_t i = 0; i < jobs.size(); ++i) {
+    const NewtonJob& x = *jobs[i];
+    if (x.K < 1 || x.K > (size_t(1) << kNewtonMaxLog) || (x.kind == 1 && (x.K < 2 || !(x.P & 1u))))
+      return cudaErrorInvalidValue;
+    NewtonCrtJobB j;
+    std::memset(&j, 0, sizeof j);
+    j.kind = x.kind;
+    CrtCl& cc = x.kind == 0 ? j.inv.cc : j.exp.cc;
+    if (!crt_cl_fill(x.aux, x.P, cc)) return cudaErrorInvalidValue;
+    if (x.kind == 0) {
+      j.inv.a = x.a;
+      j.inv.la = (uint32_t)std::min<size_t>(x.la, x.K);
+      j.inv.c = x.out;
+      j.inv.K = (uint32_t)x.K;
+    } else {
+      j.exp.ap = x.a;
+      j.exp.lap = (uint32_t)std::min<size_t>(x.la, x.K);
+      j.exp.tab = x.tab;
+      j.exp.b = x.out;
+      j.exp.c = x.c;
+      j.exp.K = (uint32_t)x.K;
+    }
+    std::memcpy(out + i, &j, sizeof j);
+  }
+  return cudaSuccess;
+}
+
+cudaError_t launch_newton_crt_b(const void* dev, size_t count, cudaStream_t s) {
+  if (count == 0) return cudaSuccess;
+  if (count > 65535) return cudaErrorInvalidValue;
+  return crt_cl_launch(k_newton_crt_b, static_cast<const NewtonCrtJobB*>(dev), s, (unsigned)count);
 }
 
 cudaError_t launch_newton_sqrt_crt(const PrimeTables* aux, uint32_t P, const uint32_t* u, size_t ulen, uint32_t root,

@@ -187,6 +187,11 @@ struct NewtonJob {
   uint32_t* out;
   uint32_t* c;
   size_t K;
+  // a prime P without 2^13-th roots of unity: the three CRT primes' plans
+  // (167772161, 469762049, 754974721 in that order; pt unused), one cluster
+  // of three CTAs per job
+  const PrimeTables* aux = nullptr;
+  uint32_t P = 0;
 };
 size_t batch_newton_bytes(size_t jobs);
 cudaError_t launch_newton_batch(const std::vector<NewtonJob>& jobs, void* host_staging, void* dev_desc,
