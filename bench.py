@@ -433,6 +433,23 @@ def serve_mix(count: int, seed: int = 5, max_log: int = 22):
     return specs
 
 
+def mix_digest(specs) -> str:
+    """SHA-256 over every job's operation, modulus, scalars and operand words:
+    identifies a generated mix (the parity fixtures record it)."""
+    import hashlib
+    h = hashlib.sha256()
+    for s in specs:
+        h.update(s[0].encode())
+        h.update(int(s[1]).to_bytes(4, "little"))
+        for x in s[2:]:
+            if isinstance(x, np.ndarray):
+                h.update(len(x).to_bytes(8, "little"))
+                h.update(np.ascontiguousarray(x, dtype=np.uint32).tobytes())
+            else:
+                h.update(int(x).to_bytes(8, "little"))
+    return h.hexdigest()
+
+
 def _native(p: int, log_n: int) -> bool:
     return p % 2 == 1 and p < (1 << 30) and 1 <= log_n <= ((p - 1) & -(p - 1)).bit_length() - 1
 

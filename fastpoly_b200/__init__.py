@@ -71,6 +71,7 @@ def load_library(path: str = LIB_PATH):
     L.fpx_last_error_message.restype = C.c_char_p
     L.fpx_pool_stats.argtypes = [vp, vp]
     L.fpx_release_pool.argtypes = [vp]
+    L.fpx_ctx_set_crt_block.argtypes = [vp, sz]
     L.fpx_ntt_max_log.argtypes = [u32]
     L.fpx_profile.argtypes = [vp, i32]
     L.fpx_profile_report.argtypes = [vp, C.c_char_p, sz, _szp]
@@ -328,6 +329,10 @@ class Context:
 
     def release_pool(self):
         self._check(self._L.fpx_release_pool(self._h), "release_pool")
+
+    def set_crt_block(self, terms: int = 0):
+        """Terms per block of the block-pair CRT product (0: the default 2^23)."""
+        self._check(self._L.fpx_ctx_set_crt_block(self._h, terms), "set_crt_block")
 
     # -- column-pass tile shapes (the tuner's choice per transform size) ----------
     def col_shape_candidates(self, log_n: int, kind: int) -> list:

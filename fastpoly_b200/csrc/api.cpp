@@ -155,6 +155,10 @@ int fpx_release_pool(fpx_ctx* ctx) {
   });
 }
 
+int fpx_ctx_set_crt_block(fpx_ctx* ctx, size_t block_terms) {
+  return guarded(ctx, [&](fpx::Engine& e) { e.set_crt_block(block_terms); });
+}
+
 int fpx_col_shape_candidates(fpx_ctx* ctx, int log_n, int kind, fpx_col_shape* out, int max, int* count) {
   if (!out || !count || max < 0) return FPX_EINVAL;
   return guarded(ctx, [&](fpx::Engine& e) {

@@ -179,10 +179,22 @@ uint32_t* Pool::get(size_t words, size_t* cls_out) {
       if (capturing_) cap_owned_[static_cast<uint32_t*>(p)] = cls;
       return static_cast<uint32_t*>(p);
     }
+    // The limit is checked and the block's bytes reserved under the lock, so
+    // concurrent callers of one pool cannot together pass the limit.
+    if (limit_ && in_use_bytes + cls > limit_)
+      throw Error{FPX_ENOMEM, "device pool limit reached (" + std::to_string(limit_) + " bytes)"};
+    in_use_bytes += cls;
   }
-  if (limit_ && in_use_bytes + cls > limit_)
-    throw Error{FPX_ENOMEM, "device pool limit reached (" + std::to_string(limit_) + " bytes)"};
-  if (limit_ && in_use_bytes + cached_bytes + cls > limit_) release();
+  auto unreserve = [&] {
+    std::lock_guard<std::mutex> g(mu_);
+    in_use_bytes -= cls;
+  };
+  bool trim;
+  {
+    std::lock_guard<std::mutex> g(mu_);
+    trim = limit_ && in_use_bytes + cached_bytes > limit_;
+  }
+  if (trim) release();
   void* p = nullptr;
   cudaError_t e = cudaMalloc(&p, cls);
   if (e != cudaSuccess) {
@@ -191,12 +203,12 @@ uint32_t* Pool::get(size_t words, size_t* cls_out) {
     e = cudaMalloc(&p, cls);
     if (e != cudaSuccess) {
       cudaGetLastError();
+      unreserve();
       throw Error{FPX_ENOMEM, "cudaMalloc of " + std::to_string(cls) + " bytes failed"};
     }
   }
   std::lock_guard<std::mutex> g(mu_);
   ++system_allocations;
-  in_use_bytes += cls;
   *cls_out = cls;
   if (capturing_) cap_owned_[static_cast<uint32_t*>(p)] = cls;
   return static_cast<uint32_t*>(p);
@@ -251,7 +263,7 @@ void Pool::release() {
 
 // ------------------------------------------------------------------- engine
 
-Engine::Engine(int device, size_t pool_limit) : device_(device), pool_(pool_limit) {
+Engine::Engine(int device, size_t pool_limit) : device_(device), pool_(pool_limit), crt_block_(kCrtBlock) {
   int n = 0;
   if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
     cudaGetLastError();
@@ -736,7 +748,7 @@ void Engine::product(uint32_t p, const uint32_t* a, size_t la, const uint32_t* b
     cyc_product(p, logN, op);
     return;
   }
-  if (!accumulate && logN <= 20) {
+  if (!accumulate && logN <= 20 && std::max(la, lb) <= crt_block_) {
     // one block pair of at most 2^20 points: the auxiliary primes' transforms
     // share one launch set and the Garner epilogue applies post_mont (larger
     // products measured 4 % faster on separate per-prime launches)
@@ -760,9 +772,16 @@ void Engine::product(uint32_t p, const uint32_t* a, size_t la, const uint32_t* b
 // instead of 3 nA nB.  The whole coefficient is reconstructed at once, so this
 // needs (p-1)^2 min(la, lb) below the auxiliary primes' product (false: not
 // taken; crt_product's per-pair path reconstructs each pair separately).
+void Engine::set_crt_block(size_t terms) {
+  if (terms == 0) terms = kCrtBlock;
+  if ((terms & (terms - 1)) || terms < (size_t(1) << 13) || terms > kCrtBlock)
+    throw Error{FPX_EINVAL, "CRT block size must be a power of two in [2^13, 2^23]"};
+  crt_block_ = terms;
+}
+
 bool Engine::crt_blocked(uint32_t p, const uint32_t* a, size_t la, const uint32_t* b, size_t lb, size_t outn,
                          uint32_t* out, bool accumulate) {
-  const size_t B = kCrtBlock;
+  const size_t B = crt_block_;
   const size_t nA = (la + B - 1) / B, nB = (lb + B - 1) / B;
   if (nA * nB < 2 || std::min(la, lb) <= kNaive) return false;
   if (const char* e = std::getenv("FPX_CRT_BLOCKED"); e && e[0] == '0') return false;  // the per-pair path
@@ -832,9 +851,9 @@ void Engine::crt_product(uint32_t p, const uint32_t* a, size_t la, const uint32_
   if (crt_blocked(p, a, la, b, lb, outn, out, accumulate)) return;
   if (!accumulate) check(cudaMemsetAsync(out, 0, outn * 4, stream_), "memset");
   for (size_t ai = 0; ai < la;) {
-    const size_t na = std::min(kCrtBlock, la - ai);
+    const size_t na = std::min(crt_block_, la - ai);
     for (size_t bi = 0; bi < lb && bi < outn - ai;) {
-      const size_t nb = std::min(kCrtBlock, lb - bi);
+      const size_t nb = std::min(crt_block_, lb - bi);
       const size_t cnt = std::min(na + nb - 1, outn - ai - bi);
       const uint32_t* pa = a + ai;
       const uint32_t* pb = b + bi;

@@ -159,6 +159,13 @@ class Engine {
   // replay it.  FPX_GRAPHS=0 turns this off.  drop_graphs frees them all.
   void drop_graphs();
 
+  // Terms per block of the block-pair CRT product (the reference's
+  // crt_convolution<M, Block> parameter, crt_convolution.hpp:188; default
+  // 2^23).  A power of two in [2^13, 2^23]; smaller blocks run the same block
+  // loops on small inputs.  Every block size gives the same exact product.
+  void set_crt_block(size_t terms);
+  size_t crt_block() const { return crt_block_; }
+
   // Per-kernel timing (CUDA events on the launching stream) and launch count.
   void profile(bool on);
   std::string profile_report();  // {"kernel": [launches, total_ms], ...}
@@ -302,6 +309,7 @@ class Engine {
   std::map<uint32_t, std::unique_ptr<PrimePlan>> primes_;
   std::map<std::pair<uint32_t, int>, std::unique_ptr<BigPlan>> bigs_;
   std::map<uint32_t, std::pair<size_t, Buf>> inv_tabs_;
+  size_t crt_block_;
   unsigned long long* scratch_ull_ = nullptr;  // device word for scans
   unsigned long long* host_ull_ = nullptr;     // pinned
 };

@@ -66,6 +66,12 @@ const char* fpx_last_error_message(fpx_ctx* ctx);
 /* scratch_memory_stats() / release_scratch_memory() (memory.hpp:21-26, 252-258) */
 int fpx_pool_stats(fpx_ctx* ctx, fpx_pool_stats_t* out);
 int fpx_release_pool(fpx_ctx* ctx);
+/* Terms per block of products that go through the block-pair three-prime CRT
+ * path (the reference's crt_convolution<M, Block> template parameter,
+ * crt_convolution.hpp:188, default 2^23 = 0 here): a power of two in
+ * [2^13, 2^23], else FPX_EINVAL.  Every block size gives the same exact
+ * product; small blocks run the multi-block loops on small inputs (tests). */
+int fpx_ctx_set_crt_block(fpx_ctx* ctx, size_t block_terms);
 
 /* ---- instrumentation (the reference's bench harness timing, bench/bench.cpp:161-203,
  *      moved onto the device) ---------------------------------------------------
@@ -244,7 +250,11 @@ size_t fpx_serve_plan_bytes(const fpx_job* job);
  * product length next_pow2(min(la,n) + min(lb,n) - 1) at most 2^20 and
  * 2^v2(p-1), unless the shorter operand has <= 40 terms (FPX_ESIZE otherwise).
  * The first call on a device looks the array up (cudaGetSymbolAddress) and
- * should come before any stream capture.  All calls share the array and keep
+ * should come before any stream capture.  The device is the current one: the
+ * stream must belong to it, and the looked-up address is kept for the life of
+ * the process, so no cudaDeviceReset may come between calls.  A CUDA error
+ * already pending when the call starts is left pending and the call returns
+ * FPX_ECUDA without launching anything.  All calls share the array and keep
  * its last contents; calls that overlap on the GPU race and must be serialised
  * by the caller. */
 int fpx_conv_noalloc(uint32_t p, const uint32_t* d_a, size_t la, const uint32_t* d_b, size_t lb, size_t n,
