@@ -245,6 +245,13 @@ uint32_t* limbs(std::vector<M>& v) {
 
 /// The reference's scratch statistics (memory.hpp:21-26), here of the GPU
 /// context's device pool (one per process rather than per thread).
+#ifndef FASTPOLY_SCRATCH_CACHE_BYTES
+// The reference's per-thread idle scratch limit (memory.hpp:15-17).  The device
+// pool keeps every idle block until release_scratch_memory(), so a warm call of
+// any size is served from the cache.
+#define FASTPOLY_SCRATCH_CACHE_BYTES (64u * 1024u * 1024u)
+#endif
+
 struct ScratchMemoryStats {
   size_t cached_bytes = 0;
   size_t cached_blocks = 0;
@@ -450,7 +457,60 @@ vec<M> integral(const vec<M>& a) {
   return r;
 }
 
+// The reference's three-prime CRT helpers (crt_convolution.hpp:78-227), which its
+// own tests call directly.  Products are exact, so every block size gives the same
+// values; the GPU picks its own schedule for each product.
+namespace detail {
+
+inline constexpr size_t crt_block_size = size_t(1) << 23;
+inline constexpr uint64_t crt_aux_primes[3] = {167772161u, 469762049u, 754974721u};
+
+/// Auxiliary primes that make an exact product of `terms`-term operands mod
+/// M::mod unique: the first k whose product exceeds terms * (p - 1)^2.
+template <class M>
+constexpr size_t crt_prime_count(size_t terms) {
+  const unsigned __int128 worst = (unsigned __int128)(M::mod - 1) * (M::mod - 1) * terms;
+  unsigned __int128 range = 1;
+  for (size_t k = 0; k < 2; ++k) {
+    range *= crt_aux_primes[k];
+    if (worst < range) return k + 1;
+  }
+  return 3;
+}
+
+/// a * b truncated to `out` terms, zero-padded to exactly `out`.
+template <class M, size_t BlockSize = crt_block_size>
+vec<M> crt_convolution(const vec<M>& a, const vec<M>& b, size_t out) {
+  static_assert(BlockSize > 0 && BlockSize <= crt_block_size);
+  vec<M> r = conv(a, b, out);
+  r.resize(out);
+  return r;
+}
+
+/// Coefficients [offset, offset + count) of a * b, a read up to offset + count
+/// terms and b up to m (offset defaults to m): the Newton middle product.  As in
+/// the reference, the window must lie above every coefficient a cyclic product
+/// of next_pow2(2m) points would wrap; there it equals the exact product.
+template <class M>
+vec<M> crt_middle_product(const vec<M>& a, const vec<M>& b, size_t m, size_t count, size_t offset = SIZE_MAX) {
+  if (offset == SIZE_MAX) offset = m;
+  vec<M> r(count);
+  const size_t la = std::min(a.size(), offset + count), lb = std::min(b.size(), m);
+  if (la == 0 || lb == 0) return r;
+  const vec<M> full = conv(vec<M>(a.begin(), a.begin() + la), vec<M>(b.begin(), b.begin() + lb), offset + count);
+  for (size_t i = 0; i < count && offset + i < full.size(); ++i) r[i] = full[offset + i];
+  return r;
+}
+
+}  // namespace detail
+
 }  // namespace poly
+
+// The SIMD width the reference's kernels are written for (fastpoly/simd.hpp);
+// here the 32 lanes of a warp, the unit the GPU kernels are laid out in.
+namespace simd {
+inline constexpr unsigned lane = 32;
+}  // namespace simd
 
 // ----------------------------------------------------------------- batches
 
@@ -586,10 +646,15 @@ class Poly : public std::vector<M> {
   Poly operator*(const base& b) const { return poly::conv<M>(*this, b); }
   Poly operator*(M c) const { return poly::mul_scalar<M>(*this, c); }
   Poly operator<<(size_t k) const { return poly::shift<M>(*this, k); }
-  Poly& operator+=(const base& b) { return *this = *this + b; }
-  Poly& operator-=(const base& b) { return *this = *this - b; }
+  // In place, in the existing storage (poly.hpp:47-50): b may be *this itself,
+  // and a longer b grows *this to its length.
+  Poly& operator+=(const base& b) { return accumulate<false>(b); }
+  Poly& operator-=(const base& b) { return accumulate<true>(b); }
   Poly& operator*=(const base& b) { return *this = poly::conv<M>(*this, b); }
-  Poly& operator*=(M c) { return *this = *this * c; }
+  Poly& operator*=(M c) {
+    for (auto& x : *this) x *= c;
+    return *this;
+  }
   Poly mul(const base& b, size_t n) const { return poly::conv<M>(*this, b, n); }
   Poly derivative() const { return poly::derivative<M>(*this); }
   Poly integral() const { return poly::integral<M>(*this); }
@@ -614,6 +679,16 @@ class Poly : public std::vector<M> {
     Poly r(v.size());
     for (size_t i = 0; i < v.size(); ++i) r[i] = M::from_int(v[i]);
     return r;
+  }
+ private:
+  template <bool SUB>
+  Poly& accumulate(const base& b) {
+    const size_t nb = b.size();
+    if (nb > this->size()) this->resize(nb);  // never taken when b is *this
+    M* x = this->data();
+    const M* y = b.data();
+    for (size_t i = 0; i < nb; ++i) x[i] = SUB ? x[i] - y[i] : x[i] + y[i];
+    return *this;
   }
 };
 
