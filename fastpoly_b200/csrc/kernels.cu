@@ -3178,10 +3178,19 @@ cudaError_t fill_newton_crt_batch(const std::vector<const NewtonJob*>& jobs, voi
   return cudaSuccess;
 }
 
+// Any number of cluster jobs: launches of at most kCrtClustersPerLaunch clusters
+// each, the descriptor pointer advanced by the jobs already launched.
+constexpr size_t kCrtClustersPerLaunch = 65535;
+
 cudaError_t launch_newton_crt_b(const void* dev, size_t count, cudaStream_t s) {
-  if (count == 0) return cudaSuccess;
-  if (count > 65535) return cudaErrorInvalidValue;
-  return crt_cl_launch(k_newton_crt_b, static_cast<const NewtonCrtJobB*>(dev), s, (unsigned)count);
+  const auto* jobs = static_cast<const NewtonCrtJobB*>(dev);
+  for (size_t done = 0; done < count;) {
+    const size_t n = std::min(count - done, kCrtClustersPerLaunch);
+    const cudaError_t e = crt_cl_launch(k_newton_crt_b, jobs + done, s, (unsigned)n);
+    if (e != cudaSuccess) return e;
+    done += n;
+  }
+  return cudaSuccess;
 }
 
 cudaError_t launch_newton_sqrt_crt(const PrimeTables* aux, uint32_t P, const uint32_t* u, size_t ulen, uint32_t root,

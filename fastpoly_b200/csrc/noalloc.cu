@@ -13,9 +13,12 @@
 // the call allocates nothing (no cudaMalloc, no cudaFree, no context, no pool).
 // The first call on each device looks up the array's device address with
 // cudaGetSymbolAddress (and sets the kernels' shared-memory limits); make that
-// first call before any stream capture.  All calls share the array and it keeps
-// the last call's contents: the tables are rebuilt by every call and the
-// transform buffers are fully written before they are read.  Calls whose work
+// first call before any stream capture.  The device is the current one: the
+// stream must belong to it, and the address is cached per device for the life
+// of the process, so no cudaDeviceReset may come between calls.  All calls
+// share the array and it keeps the last call's contents: each call rebuilds the
+// table entries its transform size reads, and the transform buffers are fully
+// written before they are read.  Calls whose work
 // overlaps on the GPU (different streams, or different host threads) race on
 // the array and must be serialised by the caller.
 #include <cstdint>
@@ -24,6 +27,7 @@
 #include <cuda_runtime.h>
 
 #include "engine.h"
+#include "field.cuh"
 #include "fpx_b200.h"
 #include "kernels.h"
 
@@ -52,32 +56,40 @@ constexpr size_t kWords = kOffHiI + kHiWords;
 static __device__ __align__(256) uint32_t g_noalloc_scratch[kWords];
 
 struct Roots {
-  uint32_t p;
-  uint32_t w[14], wi[14];  // w[lg] = primitive 2^lg-th root of unity and its inverse (lg <= 13)
-  uint32_t wN, wNi;        // primitive N-th root and inverse (two-pass sizes)
-  uint32_t inv_scale;      // 2^32 / N mod p
-  uint32_t nhi;            // max(1, N / 65536) (0 for one-CTA sizes)
+  uint32_t p, pinv;        // modulus and p^-1 mod 2^32 (Montgomery products)
+  uint32_t r1;             // 2^32 mod p: Montgomery form of 1
+  uint32_t w[14], wi[14];  // Montgomery forms of the primitive 2^lg-th root and its inverse (lg <= 13)
+  uint32_t wN, wNi;        // Montgomery forms of the primitive N-th root and its inverse (two-pass sizes)
+  uint32_t inv_scale;      // Montgomery form of 2^32 / N mod p
+  uint32_t small;          // one-CTA table entries used: min(N, 2^13)
+  uint32_t nhi;            // max(1, N / 65536) for two-pass sizes, 0 for one-CTA sizes (no Bailey tables)
 };
 
-__device__ uint32_t mulm(uint32_t a, uint32_t b, uint32_t p) { return (uint32_t)((uint64_t)a * b % p); }
-__device__ uint32_t powm_dev(uint32_t a, uint32_t e, uint32_t p) {
-  uint32_t r = 1 % p;
-  for (; e; e >>= 1, a = mulm(a, a, p))
-    if (e & 1) r = mulm(r, a, p);
-  return r;
+// Montgomery arithmetic for the table build: every factor is kept in [0, p).
+__device__ uint32_t mmul(uint32_t a, uint32_t b, const Roots& r) {
+  return fpx_dev::red(fpx_dev::mont(a, b, fpx_dev::Fp{r.p, 2u * r.p, r.pinv}), r.p);
+}
+// x^e from the Montgomery form of x; returns the canonical residue.
+__device__ uint32_t powm_dev(uint32_t xm, uint32_t e, const Roots& r) {
+  uint32_t acc = r.r1;
+  for (; e; e >>= 1, xm = mmul(xm, xm, r))
+    if (e & 1) acc = mmul(acc, xm, r);
+  return mmul(acc, 1u, r);
 }
 __device__ void put(uint32_t* t, size_t i, uint32_t w, uint32_t p) {
   t[2 * i] = w;
   t[2 * i + 1] = (uint32_t)(((uint64_t)w << 32) / p);
 }
 
-// Rebuilds every twiddle table in the static array for (p, N).
+// Rebuilds the twiddle tables the transform of N points reads: the first
+// min(N, 2^13) entries of the per-prime tables and, for two-pass sizes only,
+// the Bailey tables.
 __global__ void k_noalloc_tables(Roots r) {
   uint32_t* s = g_noalloc_scratch;
   const uint32_t p = r.p;
-  const size_t total = (size_t(1) << 13) + 512 + r.nhi;
+  const size_t total = r.small + (r.nhi ? 512 + r.nhi : 0);
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
-    if (i < (size_t(1) << 13)) {
+    if (i < r.small) {
       if (i == 0) {
         put(s + kOffFwd, 0, 1 % p, p);
         put(s + kOffInv, 0, 1 % p, p);
@@ -86,22 +98,21 @@ __global__ void k_noalloc_tables(Roots r) {
       const uint32_t h = 1u << (31 - __clz((unsigned)i));  // entry h + k is w_{2h}^k
       const int lg = 32 - __clz(h);
       const uint32_t k = (uint32_t)i - h;
-      put(s + kOffFwd, i, powm_dev(r.w[lg], k, p), p);
-      put(s + kOffInv, i, powm_dev(r.wi[lg], k, p), p);
-    } else if (i < (size_t(1) << 13) + 512) {
-      if (!r.nhi) continue;
-      const uint32_t y = (uint32_t)(i - (size_t(1) << 13));
+      put(s + kOffFwd, i, powm_dev(r.w[lg], k, r), p);
+      put(s + kOffInv, i, powm_dev(r.wi[lg], k, r), p);
+    } else if (i < r.small + 512) {
+      const uint32_t y = (uint32_t)(i - r.small);
       if (y < 256) {  // w_N^y, inverse scaled by 2^32 / N
-        put(s + kOffLoF, y, powm_dev(r.wN, y, p), p);
-        put(s + kOffLoI, y, mulm(powm_dev(r.wNi, y, p), r.inv_scale, p), p);
+        put(s + kOffLoF, y, powm_dev(r.wN, y, r), p);
+        put(s + kOffLoI, y, mmul(powm_dev(r.wNi, y, r), r.inv_scale, r), p);
       } else {        // w_N^(256 y)
-        put(s + kOffMidF, y - 256, powm_dev(r.wN, 256u * (y - 256), p), p);
-        put(s + kOffMidI, y - 256, powm_dev(r.wNi, 256u * (y - 256), p), p);
+        put(s + kOffMidF, y - 256, powm_dev(r.wN, 256u * (y - 256), r), p);
+        put(s + kOffMidI, y - 256, powm_dev(r.wNi, 256u * (y - 256), r), p);
       }
     } else {  // w_N^(65536 x)
-      const uint32_t x = (uint32_t)(i - (size_t(1) << 13) - 512);
-      put(s + kOffHiF, x, powm_dev(r.wN, 65536u * x, p), p);
-      put(s + kOffHiI, x, powm_dev(r.wNi, 65536u * x, p), p);
+      const uint32_t x = (uint32_t)(i - r.small - 512);
+      put(s + kOffHiF, x, powm_dev(r.wN, 65536u * x, r), p);
+      put(s + kOffHiI, x, powm_dev(r.wNi, 65536u * x, r), p);
     }
   }
 }
@@ -136,6 +147,9 @@ extern "C" int fpx_conv_noalloc(uint32_t p, const uint32_t* d_a, size_t la, cons
   if (!out_len) return FPX_EINVAL;
   *out_len = 0;
   if (la == 0 || lb == 0 || n == 0) return FPX_OK;
+  // An error already pending from the caller's own work is left pending for the
+  // caller and nothing is launched: every error seen below is this call's.
+  if (cudaPeekAtLastError() != cudaSuccess) return FPX_ECUDA;
   if (!d_a || !d_b || !d_out) return FPX_EINVAL;
   if (!(p & 1u) || p >= (1u << 30) || !fpx::is_prime(p)) return FPX_EINVAL;
   la = la < n ? la : n;
@@ -161,21 +175,28 @@ extern "C" int fpx_conv_noalloc(uint32_t p, const uint32_t* d_a, size_t la, cons
 
   Roots r{};
   r.p = p;
+  r.pinv = fpx_dev::inv_mod_2_32(p);
+  const uint32_t R = (uint32_t)((uint64_t(1) << 32) % p);
+  r.r1 = R;
+  auto to_mont = [&](uint32_t x) { return (uint32_t)((uint64_t)x * R % p); };
   const uint32_t g = fpx::primitive_root(p);
   for (int lg = 1; lg <= 13 && lg <= fpx::v2_of(p); ++lg) {
-    r.w[lg] = fpx::powm(g, (p - 1) >> lg, p);
-    r.wi[lg] = fpx::invm(r.w[lg], p);
+    const uint32_t w = fpx::powm(g, (p - 1) >> lg, p);
+    r.w[lg] = to_mont(w);
+    r.wi[lg] = to_mont(fpx::invm(w, p));
   }
   const uint32_t N = 1u << logN;
-  const uint32_t R = (uint32_t)((uint64_t(1) << 32) % p);
   const uint32_t scale = (uint32_t)((uint64_t)fpx::invm(N % p, p) * R % p);  // undoes the Montgomery pointwise
+  r.small = N < (1u << 13) ? N : (1u << 13);
   if (logN > 13) {
-    r.wN = fpx::powm(g, (p - 1) >> logN, p);
-    r.wNi = fpx::invm(r.wN, p);
-    r.inv_scale = scale;
+    const uint32_t wN = fpx::powm(g, (p - 1) >> logN, p);
+    r.wN = to_mont(wN);
+    r.wNi = to_mont(fpx::invm(wN, p));
+    r.inv_scale = to_mont(scale);
     r.nhi = (N >> 16) > 0 ? (N >> 16) : 1;
   }
-  k_noalloc_tables<<<64, 256, 0, s>>>(r);
+  const unsigned blocks = (r.small + (r.nhi ? 512 + r.nhi : 0) + 255) / 256;
+  k_noalloc_tables<<<blocks < 64 ? blocks : 64, 256, 0, s>>>(r);
   if (cudaGetLastError() != cudaSuccess) return FPX_ECUDA;
 
   fpx::PrimeTables pt;
