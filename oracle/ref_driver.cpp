@@ -4,7 +4,9 @@
 // header-only C++20), compiled from the reference's own headers by
 // oracle/Makefile into oracle/_ref/.  It serves two purposes:
 //   * pinning the C restatement (oracle/fpx_oracle.c) against the reference
-//     itself on the same inputs (tests/test_oracle_vs_reference.py);
+//     itself on the same inputs (tests/golden/make_golden.py writes the
+//     reference's outputs that tests/test_oracle_golden.py checks the oracle
+//     against) and the GPU tests that call the reference directly;
 //   * the timed CPU baseline (bench.py --impl reference / cpu_baseline).
 // Nothing here is part of the product library.
 //

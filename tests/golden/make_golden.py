@@ -15,7 +15,8 @@ reference_vectors.json
     its tests cover: empty operands, truncation, short operands at the 40-term
     cut-over, valuations, non-residues, degree-dropping divisions.
 
-Usage:  python tests/golden/make_golden.py [--reference /root/reference]
+Usage:  python tests/golden/make_golden.py [--reference <checkout>]
+        (default: the FPX_REFERENCE environment variable)
 """
 from __future__ import annotations
 
@@ -139,8 +140,10 @@ def reference_vectors():
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", default=os.environ.get("FPX_REFERENCE"))
     args = ap.parse_args()
+    if not args.reference:
+        raise SystemExit("name the reference checkout: --reference <dir> or FPX_REFERENCE")
     pub = published(args.reference)
     with open(os.path.join(HERE, "published_checksums.json"), "w") as f:
         json.dump(pub, f, indent=0)
