@@ -21,6 +21,14 @@ seeded uniform residues.  Metric: output Mcoeff/s.
          measured HBM copy bandwidth.
 `cpu_baseline` the reference library (compiled from its own headers,
          oracle/_ref) on this host's cores, bounded sample, rank 0 at N = 1.
+`batch`  (N = 1) the config-4 mix in one fpx_batch_submit (polys/s, device
+         buffers, CUDA events), the plain per-call path on the same buffers
+         (`plain_per_call`, `batch_speedup`) and fpx_batch_run from host buffers
+         (`e2e`); as --workload batch.
+`serve`  (N = 1) the config-5 request loop: closed-loop saturation req/s, then
+         Poisson arrivals at 50 / 80 / 100 % of it with p50 / p99 latency,
+         overall and per request-size class, --requests (3000) per level; as
+         --workload serve.  --headline-only leaves both out.
 Multi-GPU: one process per GPU (torchrun), independent replicas ("weak").
 
 Other workloads, one JSON line each (not the default):
@@ -368,6 +376,11 @@ def run_fpx(args):
                 "gpu_launches": int(launches), "roofline": roof, "clocks": clk}
         if world == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_reference_sample(reps=3)
+        if world == 1 and not args.headline_only:
+            # configs 4 and 5 beside the headline (own contexts, after its timing)
+            cpu_s = None if args.no_cpu_baseline else 8.0
+            line["batch"] = batch_summary(local, 3, 20, cpu_s)
+            line["serve"] = serve_summary(local, args.requests, args.workers, args.clients, args.serve_max_log, cpu_s)
         print(json.dumps(line))
     if dist:
         dist.barrier()
@@ -535,15 +548,18 @@ def _device_jobs(F, torch, specs):
     return jobs, din, dout
 
 
-def run_batch_fpx(args):
+def batch_summary(local: int, warmup: int, steps: int, cpu_budget_s: float | None):
+    """The config-4 mix (4096 conv + 512 inv/exp) through fpx_batch_submit on
+    device buffers (CUDA events, L2 flushed between steps), the plain per-call
+    device path on the same buffers, fpx_batch_run end to end from host buffers,
+    and optionally the reference on the host cores.  Returns one dict."""
     import torch
     import fastpoly_b200 as F
 
-    rank, local, world = env_rank()
-    torch.cuda.set_device(local)
     ctx = F.Context(local)
     stream = torch.cuda.Stream()
     ctx.set_stream(stream.cuda_stream)
+    prev = torch.cuda.current_stream()
     torch.cuda.set_stream(stream)
     specs = batch_mix()
     jobs, din, dout = _device_jobs(F, torch, specs)
@@ -554,14 +570,11 @@ def run_batch_fpx(args):
         rc = ctx.batch_submit(jobs)
         assert rc == F.OK, rc
 
-    for _ in range(args.warmup):
+    for _ in range(warmup):
         flush.zero_()
         step()
     torch.cuda.synchronize()
-    clocks = ClockSampler(local)
-    clocks.start()
-    time.sleep(0.3)
-    steps = max(3, min(args.steps, 50))
+    steps = max(3, min(steps, 50))
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
     launches0 = ctx.launch_count()
     torch.cuda.synchronize()
@@ -599,33 +612,46 @@ def run_batch_fpx(args):
     for _ in range(e2e_steps):
         res = ctx.batch(specs)
     e2e_s = (time.perf_counter() - t0) / e2e_steps
-    clk = clocks.stop()
     bad = sum(isinstance(r, Exception) for r in res)
     assert bad == 0, f"{bad} failed jobs"
     h2d = 4 * sum(len(s[2]) + (len(s[3]) if s[0] == "conv" else 0) for s in specs)
     d2h = 4 * sum(r.size for r in res)
     peak, peak_kind = measured_peak_hbm()
     achieved = step_bytes / (ms * 1e-3) / 1e9
-    line = {"metric": "polys/s, mixed batch (4096 conv + 512 inv/exp)", "value": round(value, 1), "unit": "polys/s",
-            "n_gpus": 1, "steps": steps, "warmup": args.warmup, "ms_per_step": round(ms, 4), "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
-            "config": {"workload": "4096 conv (lengths 2^U, U~U[6,16]) + 512 inv/exp (n log-uniform 2^8..2^14), "
-                                   "moduli 50/50 998244353 / 1000000007, fixed seed", "jobs": len(specs),
-                       "l2": "flushed between steps (512 MiB write)"},
-            "plain_per_call": {"value": round(len(specs) / plain_s, 1), "unit": "polys/s",
-                               "api": "fpx_conv_device / fpx_inv_device / fpx_exp_device, one call per job"},
-            "batch_speedup": round(value / (len(specs) / plain_s), 2),
-            "e2e": {"value": round(len(specs) / e2e_s, 1), "unit": "polys/s", "h2d_bytes_per_step": h2d,
-                    "d2h_bytes_per_step": d2h, "api": "fpx_batch_run (host buffers)"},
-            "gpu_launches": int(launches),
-            "roofline": {"bound": "hbm", "kernel": "whole batch step", "achieved": round(achieved, 1), "peak": peak,
-                         "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": None,
-                         "alg_bytes_per_step": step_bytes, "peak_source": peak_kind},
-            "clocks": clk}
-    if not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_mix_sample(specs, budget_s=20.0)
-    print(json.dumps(line))
+    out = {"metric": "polys/s, mixed batch (4096 conv + 512 inv/exp)", "value": round(value, 1), "unit": "polys/s",
+           "steps": steps, "ms_per_step": round(ms, 4),
+           "config": {"workload": "4096 conv (lengths 2^U, U~U[6,16]) + 512 inv/exp (n log-uniform 2^8..2^14), "
+                                  "moduli 50/50 998244353 / 1000000007, fixed seed", "jobs": len(specs),
+                      "l2": "flushed between steps (512 MiB write)"},
+           "plain_per_call": {"value": round(len(specs) / plain_s, 1), "unit": "polys/s",
+                              "api": "fpx_conv_device / fpx_inv_device / fpx_exp_device, one call per job"},
+           "batch_speedup": round(value / (len(specs) / plain_s), 2),
+           "e2e": {"value": round(len(specs) / e2e_s, 1), "unit": "polys/s", "h2d_bytes_per_step": h2d,
+                   "d2h_bytes_per_step": d2h, "api": "fpx_batch_run (host buffers)"},
+           "gpu_launches": int(launches),
+           "roofline": {"bound": "hbm", "kernel": "whole batch step", "achieved": round(achieved, 1), "peak": peak,
+                        "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": None,
+                        "alg_bytes_per_step": step_bytes, "peak_source": peak_kind}}
+    torch.cuda.set_stream(prev)
     ctx.close()
+    del din, dout, flush
+    if cpu_budget_s:
+        out["cpu_baseline"] = cpu_mix_sample(specs, budget_s=cpu_budget_s)
+    return out
+
+
+def run_batch_fpx(args):
+    import torch
+
+    rank, local, world = env_rank()
+    torch.cuda.set_device(local)
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(0.3)
+    b = batch_summary(local, args.warmup, args.steps, None if args.no_cpu_baseline else 20.0)
+    line = dict(b, n_gpus=1, warmup=args.warmup, higher_is_better=True, scaling="weak", vs_baseline=None,
+                dtype="u32", data="synthetic", clocks=clocks.stop())
+    print(json.dumps(line))
     return 0
 
 
@@ -694,16 +720,27 @@ def run_batch_reference(args):
     return 0
 
 
-def run_serve_fpx(args):
+SIZE_CLASSES = [(8, 12), (12, 16), (16, 19), (19, 23)]  # log2 of the request size, [lo, hi)
+
+
+def _size_log(spec) -> int:
+    n = len(spec[2]) if spec[0] in ("conv", "divmod") else spec[-1]
+    if spec[0] == "conv":
+        n = max(n, len(spec[3]))
+    return max(0, int(n).bit_length() - 1)
+
+
+def serve_summary(local: int, count: int, workers: int, clients: int, max_log: int, cpu_budget_s: float | None):
+    """The config-5 request loop: burst rate, closed-loop saturation, then Poisson
+    arrivals at 50 / 80 / 100 % of saturation with p50 / p99 latency (overall and
+    per request-size class), `count` requests per level.  Returns one dict."""
     import threading
-    import torch
     import fastpoly_b200 as F
 
-    rank, local, world = env_rank()
-    torch.cuda.set_device(local)
-    count = args.requests
-    specs = serve_mix(count, max_log=args.serve_max_log)
-    srv = F.Server(local, workers=args.workers)
+    specs = serve_mix(count, max_log=max_log)
+    cls_of = [next(k for k, (lo, hi) in enumerate(SIZE_CLASSES) if lo <= min(_size_log(sp), 22) < hi)
+              for sp in specs]
+    srv = F.Server(local, workers=workers)
     try:
         # warm-up: plans, pools and pinned buffers of every worker, on the same mix
         for t in [srv.submit(s) for s in specs]:
@@ -716,27 +753,28 @@ def run_serve_fpx(args):
             r, _ = srv.poll(t)
             fails += isinstance(r, Exception)
         burst_rate = count / (time.perf_counter() - t0)
+
         # saturation: a closed loop of `clients` callers, each submitting its next
         # request when the previous one completes (the steady state the open-loop
         # loads below are fractions of)
-        def closed_loop(clients):
+        def closed_loop(n_clients):
             def client(k):
-                for i in range(k, count, clients):
+                for i in range(k, count, n_clients):
                     srv.poll(srv.submit(specs[i]))
-            th = [threading.Thread(target=client, args=(k,)) for k in range(clients)]
+            th = [threading.Thread(target=client, args=(k,)) for k in range(n_clients)]
             t0 = time.perf_counter()
             for t in th:
                 t.start()
             for t in th:
                 t.join()
             return count / (time.perf_counter() - t0)
-        sat_rate = closed_loop(args.clients)
+
+        sat_rate = closed_loop(clients)
         loads = {}
         for frac in (0.5, 0.8, 1.0):
             rate = frac * sat_rate
             rng = np.random.default_rng(int(frac * 100))
-            gaps = rng.exponential(1.0 / rate, count)
-            arrivals = np.cumsum(gaps)
+            arrivals = np.cumsum(rng.exponential(1.0 / rate, count))
             tickets = [None] * count
 
             def submitter():
@@ -754,33 +792,55 @@ def run_serve_fpx(args):
             for i in range(count):
                 while tickets[i] is None:
                     time.sleep(0.0002)
-                r, l = srv.poll(tickets[i])
-                lats.append(l)
+                r, lat = srv.poll(tickets[i])
+                lats.append(lat)
             th.join()
             el = time.perf_counter() - t0
+            lats = np.asarray(lats)
+            per_cls = {}
+            for k, (lo, hi) in enumerate(SIZE_CLASSES):
+                sel = lats[[c == k for c in cls_of]]
+                if sel.size:
+                    per_cls[f"2^{lo}..2^{hi - 1}"] = {"n": int(sel.size),
+                                                      "p50_ms": round(1e3 * float(np.percentile(sel, 50)), 3),
+                                                      "p99_ms": round(1e3 * float(np.percentile(sel, 99)), 3)}
             loads[f"{int(frac * 100)}%"] = {"offered_req_s": round(rate, 2), "achieved_req_s": round(count / el, 2),
                                             "p50_ms": round(1e3 * float(np.percentile(lats, 50)), 3),
-                                            "p99_ms": round(1e3 * float(np.percentile(lats, 99)), 3)}
+                                            "p99_ms": round(1e3 * float(np.percentile(lats, 99)), 3),
+                                            "by_size": per_cls}
         st = srv.stats()
     finally:
         srv.stop()
     in_bytes = 4 * sum(len(s[2]) + (len(s[3]) if s[0] in ("conv", "divmod") else 0) for s in specs)
     out_bytes = 4 * sum(len(s[2]) + len(s[3]) - 1 if s[0] == "conv" else
                         (len(s[2]) + len(s[3]) if s[0] == "divmod" else s[-1]) for s in specs)
-    line = {"metric": "served requests/s at saturation (mixed ops, sizes 2^8..2^%d)" % args.serve_max_log,
-            "value": round(sat_rate, 2), "unit": "req/s", "n_gpus": 1, "steps": count, "warmup": count,
-            "ms_per_step": round(1e3 / sat_rate, 3), "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "u32", "data": "synthetic",
-            "config": {"workload": "conv 40 / inv 20 / exp 15 / sqrt 10 / divmod 10 / pow 5 %, sizes log-uniform "
-                                   f"2^8..2^{args.serve_max_log}, moduli 998244353 / 167772161 / 1e9+7 / 2^31-1",
-                       "requests": count, "workers": args.workers, "failed": int(fails),
-                       "saturation": f"closed loop of {args.clients} callers"},
-            "latency": loads, "server": st,
-            "burst_req_s": round(burst_rate, 2),
-            "e2e": {"value": round(sat_rate, 2), "unit": "req/s", "h2d_bytes_per_step": in_bytes // count,
-                    "d2h_bytes_per_step": out_bytes // count, "api": "fpx_serve_submit / fpx_serve_poll (host buffers)"}}
-    if not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_mix_sample(specs, budget_s=30.0, unit="req/s")
+    out = {"metric": "served requests/s at saturation (mixed ops, sizes 2^8..2^%d)" % max_log,
+           "value": round(sat_rate, 2), "unit": "req/s", "ms_per_step": round(1e3 / sat_rate, 3),
+           "config": {"workload": "conv 40 / inv 20 / exp 15 / sqrt 10 / divmod 10 / pow 5 %, sizes log-uniform "
+                                  f"2^8..2^{max_log}, moduli 998244353 / 167772161 / 1e9+7 / 2^31-1",
+                      "requests_per_level": count, "workers": workers, "failed": int(fails),
+                      "saturation": f"closed loop of {clients} callers"},
+           "latency": loads, "server": st, "burst_req_s": round(burst_rate, 2),
+           "e2e": {"value": round(sat_rate, 2), "unit": "req/s", "h2d_bytes_per_step": in_bytes // count,
+                   "d2h_bytes_per_step": out_bytes // count,
+                   "api": "fpx_serve_submit / fpx_serve_poll (host buffers)"}}
+    if cpu_budget_s:
+        out["cpu_baseline"] = cpu_mix_sample(specs, budget_s=cpu_budget_s, unit="req/s")
+    return out
+
+
+def run_serve_fpx(args):
+    import torch
+
+    rank, local, world = env_rank()
+    torch.cuda.set_device(local)
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(0.3)
+    sv = serve_summary(local, args.requests, args.workers, args.clients, args.serve_max_log,
+                       None if args.no_cpu_baseline else 30.0)
+    line = dict(sv, n_gpus=1, steps=args.requests, warmup=args.requests, higher_is_better=True, scaling="weak",
+                vs_baseline=None, dtype="u32", data="synthetic", clocks=clocks.stop())
     print(json.dumps(line))
     return 0
 
@@ -898,11 +958,13 @@ def main():
     ap.add_argument("--workload", default="conv", choices=["conv", "batch", "serve", "ops"],
                     help="conv: the headline 2^23 conv (default); batch: mixed batch; serve: request loop; "
                          "ops: single operations of configs 1-3")
-    ap.add_argument("--requests", type=int, default=600, help="serve: requests per load level")
+    ap.add_argument("--requests", type=int, default=3000, help="serve: requests per load level")
     ap.add_argument("--serve-max-log", type=int, default=22, help="serve: largest size 2^k")
     ap.add_argument("--workers", type=int, default=2, help="serve: micro-batches in flight")
     ap.add_argument("--clients", type=int, default=32, help="serve: callers of the closed-loop saturation run")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--headline-only", action="store_true",
+                    help="conv: leave out the batch (config 4) and serve (config 5) objects of the default line")
     ap.add_argument("--e2e-callers", type=int, default=4,
                     help="conv: concurrent host threads (one context each) of the end-to-end measurement")
     args = ap.parse_args()

@@ -50,22 +50,39 @@ def _run(cmd, verbose):
         raise RuntimeError(f"build step failed with status {r.returncode}: {cmd[0]} {cmd[-1]}")
 
 
+def _object_stale(src: str, obj: str, headers: list) -> bool:
+    """An object is rebuilt when it is missing or older than its source or any
+    header of the library (headers are shared, so any change rebuilds all)."""
+    if not os.path.exists(obj):
+        return True
+    t = os.path.getmtime(obj)
+    return os.path.getmtime(src) > t or any(os.path.getmtime(h) > t for h in headers if os.path.exists(h))
+
+
 def build(force: bool = False, verbose: bool = False) -> str:
     if not force and not _stale():
         return LIB
     os.makedirs(BUILD, exist_ok=True)
-    objs = []
-    for s in CU_SOURCES:
-        o = os.path.join(BUILD, s + ".o")
-        _run([NVCC, "-std=c++17", "-O3", *ARCH, "-lineinfo", "-Xcompiler", "-fPIC", "-I" + CSRC, "-I" + INCLUDE,
-              "-c", os.path.join(CSRC, s), "-o", o], verbose)
-        objs.append(o)
+    headers = [os.path.join(CSRC, h) for h in HEADERS] + [os.path.join(INCLUDE, "fpx_b200.h")]
     cxx = os.environ.get("CXX", shutil.which("g++") or "g++")
-    for s in CPP_SOURCES:
-        o = os.path.join(BUILD, s + ".o")
-        _run([cxx, "-std=c++20", "-O2", "-fPIC", "-Wall", "-I" + CSRC, "-I" + INCLUDE,
-              "-I" + os.path.join(CUDA_HOME, "include"), "-c", os.path.join(CSRC, s), "-o", o], verbose)
+    jobs, objs = [], []
+    for s in CU_SOURCES:
+        src, o = os.path.join(CSRC, s), os.path.join(BUILD, s + ".o")
         objs.append(o)
+        if force or _object_stale(src, o, headers):
+            jobs.append([NVCC, "-std=c++17", "-O3", *ARCH, "-lineinfo", "-Xcompiler", "-fPIC", "-I" + CSRC,
+                         "-I" + INCLUDE, "-c", src, "-o", o])
+    for s in CPP_SOURCES:
+        src, o = os.path.join(CSRC, s), os.path.join(BUILD, s + ".o")
+        objs.append(o)
+        if force or _object_stale(src, o, headers):
+            jobs.append([cxx, "-std=c++20", "-O2", "-fPIC", "-Wall", "-I" + CSRC, "-I" + INCLUDE,
+                         "-I" + os.path.join(CUDA_HOME, "include"), "-c", src, "-o", o])
+    # the translation units compile in parallel (the kernels dominate)
+    from concurrent.futures import ThreadPoolExecutor
+    with ThreadPoolExecutor(max_workers=max(1, min(len(jobs), os.cpu_count() or 1))) as ex:
+        for f in [ex.submit(_run, j, verbose) for j in jobs]:
+            f.result()
     tmp = LIB + ".tmp"
     # --exclude-libs: symbols of static archives (the CUDA runtime, and the C++
     # runtime where the toolchain links it statically) stay private, so a host

@@ -233,3 +233,19 @@ def test_batch_launch_sharing(fpx):
     fpx.batch(jobs)
     used = fpx.launch_count() - before
     assert used < 200, used
+
+
+def test_batch_more_cluster_jobs_than_one_launch(fpx, oracle):
+    """Inverse jobs of at most 2^13 terms modulo a prime without the roots run
+    as one three-CTA cluster each; more of them than one launch takes (65535
+    clusters) go out in several launches."""
+    p = 1000000007
+    rng = np.random.default_rng(65)
+    polys = [rnd(rng, p, 6, nonzero0=True) for _ in range(16)]
+    want = [oracle.inv(p, a, 5) for a in polys]
+    count = 65535 + 37
+    got = fpx.batch([("inv", p, polys[i % 16], 5) for i in range(count)])
+    for i in range(count):
+        assert not isinstance(got[i], Exception), (i, got[i])
+        if not np.array_equal(got[i], want[i % 16]):
+            raise AssertionError(f"job {i} differs")
