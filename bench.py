@@ -18,7 +18,9 @@ seeded uniform residues.  Metric: output Mcoeff/s.
          CUDA-event duration (events the library records on its stream around
          each launch, in a pass of the same steps right after the timed ones:
          inside the timed steps they would serialise the launches), against the
-         measured HBM copy bandwidth.
+         measured HBM copy bandwidth; `roofline.compute` sets the step's and each
+         kernel's algorithmic butterflies against the measured butterfly rate
+         (fpx_measure_butterfly_rate), the ceiling that binds this path.
 `cpu_baseline` the reference library (compiled from its own headers,
          oracle/_ref) on this host's cores, bounded sample, rank 0 at N = 1.
 `batch`  (N = 1) the config-4 mix in one fpx_batch_submit (polys/s, device
@@ -77,6 +79,13 @@ ALG_MULS = {"colfwd": 2 * (N_FFT // 2) * LOG_R * 3,
             "rows": 3 * (N_FFT // 2) * LOG_C * 3 + N_FFT * 4,
             "colinv": (N_FFT // 2) * LOG_R * 3}
 STEP_ALG_MULS = sum(ALG_MULS.values())
+# Algorithmic butterflies per launch ((N/2) log2(points) per transform; the
+# pointwise Montgomery product counted as 1.5, its multiply-pipe cycles over a
+# Shoup butterfly's): the work the measured butterfly rate bounds.
+ALG_BF = {"colfwd": 2 * (N_FFT // 2) * LOG_R,
+          "rows": 3 * (N_FFT // 2) * LOG_C + 1.5 * N_FFT,
+          "colinv": (N_FFT // 2) * LOG_R}
+STEP_ALG_BF = sum(ALG_BF.values())
 
 
 def env_rank():
@@ -338,6 +347,7 @@ def run_fpx(args):
     # multiply instructions over the measured 32-bit multiply rate
     peak, peak_kind = measured_peak_hbm()
     imad = F.measure_imad_rate(local)
+    bfr = F.measure_butterfly_rate(local)
     dom = max((k for k in prof if k in ALG_BYTES), key=lambda k: prof[k][1], default=None)
     roof = None
     if dom:
@@ -361,7 +371,19 @@ def run_fpx(args):
                             "frac": round(ALG_MULS[dom] / avg_s / imad, 4),
                             "peak_source": "measured in this run (fpx_measure_imad_rate)"},
                 "frac_of_roofline": round(max(ALG_BYTES[dom] / (peak * 1e9), ALG_MULS[dom] / imad) / avg_s, 4),
-                "kernels_us": {k: round(v[1] / v[0] * 1e3, 2) for k, v in prof.items()}}
+                "kernels_us": {k: round(v[1] / v[0] * 1e3, 2) for k, v in prof.items()},
+                # the binding roofline of this path: transform butterflies over the
+                # measured butterfly rate (mul.hi at a quarter of the warp rate)
+                "compute": {"bound": "int multiply pipe (Shoup butterflies)",
+                            "peak_butterflies_per_s": round(bfr, 1),
+                            "peak_source": "measured in this run (fpx_measure_butterfly_rate)",
+                            "step": {"alg_butterflies": STEP_ALG_BF,
+                                     "t_roof_us": round(1e6 * STEP_ALG_BF / bfr, 2),
+                                     "frac": round(STEP_ALG_BF / bfr / (ms_per_step * 1e-3), 4)},
+                            "kernels": {k: {"alg_butterflies": ALG_BF[k],
+                                            "t_roof_us": round(1e6 * ALG_BF[k] / bfr, 2),
+                                            "frac": round(ALG_BF[k] / bfr / (prof[k][1] / prof[k][0] * 1e-3), 4)}
+                                        for k in ALG_BF if k in prof}}}
 
     line = None
     if rank == 0:

@@ -93,6 +93,7 @@ def load_library(path: str = LIB_PATH):
     L.fpx_div.argtypes = [vp, u32, _u32p, sz, _u32p, sz, _u32p, _szp, i32]
     L.fpx_mod.argtypes = [vp, u32, _u32p, sz, _u32p, sz, _u32p, _szp, i32]
     L.fpx_measure_imad_rate.argtypes = [i32, C.POINTER(C.c_double)]
+    L.fpx_measure_butterfly_rate.argtypes = [i32, C.POINTER(C.c_double)]
     L.fpx_batch_submit.argtypes = [vp, vp, sz]
     L.fpx_batch_wait.argtypes = [vp]
     L.fpx_batch_run.argtypes = [vp, vp, sz, i32]
@@ -495,6 +496,15 @@ def measure_imad_rate(device: int = 0) -> float:
     rc = load_library().fpx_measure_imad_rate(device, C.byref(r))
     if rc != OK:
         raise FpxError(rc, "fpx_measure_imad_rate failed")
+    return r.value
+
+
+def measure_butterfly_rate(device: int = 0) -> float:
+    """Measured lazy DIF butterflies per second (all SMs), the transforms' compute ceiling."""
+    r = C.c_double(0)
+    rc = load_library().fpx_measure_butterfly_rate(device, C.byref(r))
+    if rc != OK:
+        raise FpxError(rc, "fpx_measure_butterfly_rate failed")
     return r.value
 
 

@@ -86,6 +86,10 @@ uint64_t fpx_launch_count(fpx_ctx* ctx);
  * mad.lo.u32 instructions per second, all SMs busy, CUDA-event timed): the
  * compute denominator of the transform roofline.  No context needed. */
 int fpx_measure_imad_rate(int device, double* per_second);
+/* The GPU's measured rate of the transforms' lazy DIF butterfly (one add with
+ * conditional subtract, one Shoup product: mul.hi plus two mul.lo), all SMs
+ * busy, butterflies per second: the compute ceiling of a transform pass. */
+int fpx_measure_butterfly_rate(int device, double* per_second);
 
 /* ---- column-pass tile shapes (no counterpart in the reference, whose NTT plan
  *      has one fixed schedule per size) ------------------------------------------
