@@ -324,18 +324,30 @@ def run_fpx(args):
         for _ in range(e2e_steps // callers):
             c.conv(P, pa, pb, out=po)
 
-    threads = [threading.Thread(target=caller, args=t) for t in pinned]
-    for t in threads:
-        t.start()
+    def run_callers(bufs):
+        th = [threading.Thread(target=caller, args=t) for t in bufs]
+        for t in th:
+            t.start()
+        t0 = time.perf_counter()
+        go.wait()
+        for t in th:
+            t.join()
+        return time.perf_counter() - t0
+
     if dist:
         dist.barrier()
-    t0 = time.perf_counter()
-    go.wait()
-    for t in threads:
-        t.join()
-    e2e_s = time.perf_counter() - t0
+    e2e_s = run_callers(pinned)
+    # the same calls from ordinary (pageable) host memory, as a drop-in user's
+    # std::vector storage would be: the library stages them through its pinned
+    # slots
+    pageable = []
+    for c in ctxs:
+        pa, pb, po = a.copy(), b.copy(), np.empty(N_OUT, dtype=np.uint32)
+        c.conv(P, pa, pb, out=po)
+        pageable.append((c, pa, pb, po))
+    e2e_pageable_s = run_callers(pageable)
     clk = clocks.stop()
-    for _, _, _, po in pinned:
+    for _, _, _, po in pinned + pageable:
         assert int(po[0]) == want0
     for c in ctxs[1:]:
         c.close()
@@ -387,6 +399,7 @@ def run_fpx(args):
 
     line = None
     if rank == 0:
+        e2e_pageable = world * N_OUT * e2e_steps / e2e_pageable_s / 1e6
         line = {"metric": METRIC, "value": round(value, 1), "unit": "Mcoeff/s", "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": round(ms_per_step, 5), "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
@@ -394,7 +407,9 @@ def run_fpx(args):
                            "parallelism": f"replicas x{world}", "l2": "flushed between steps (512 MiB write)"},
                 "e2e": {"value": round(e2e_value, 1), "unit": "Mcoeff/s", "h2d_bytes_per_step": 2 * N_IN * 4,
                         "d2h_bytes_per_step": N_OUT * 4, "steps": e2e_steps, "callers": callers,
-                        "api": f"fpx_conv (host buffers, pinned), {callers} concurrent callers, one context each"},
+                        "api": f"fpx_conv (host buffers, pinned), {callers} concurrent callers, one context each",
+                        "pageable": {"value": round(e2e_pageable, 1), "unit": "Mcoeff/s",
+                                     "api": f"fpx_conv from pageable host memory, {callers} concurrent callers"}},
                 "gpu_launches": int(launches), "roofline": roof, "clocks": clk}
         if world == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_reference_sample(reps=3)
@@ -982,7 +997,8 @@ def main():
                          "ops: single operations of configs 1-3")
     ap.add_argument("--requests", type=int, default=3000, help="serve: requests per load level")
     ap.add_argument("--serve-max-log", type=int, default=22, help="serve: largest size 2^k")
-    ap.add_argument("--workers", type=int, default=2, help="serve: micro-batches in flight")
+    ap.add_argument("--workers", type=int, default=0,
+                    help="serve: worker threads (half large-lane, the rest small-lane; 0 = the library's 4)")
     ap.add_argument("--clients", type=int, default=32, help="serve: callers of the closed-loop saturation run")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--headline-only", action="store_true",

@@ -144,7 +144,7 @@ class ServeStats(C.Structure):
     """struct fpx_serve_stats."""
     _fields_ = [("submitted", C.c_uint64), ("completed", C.c_uint64), ("batches", C.c_uint64),
                 ("max_batch_jobs_seen", C.c_uint64), ("max_batch_bytes_seen", C.c_uint64),
-                ("oversize_requests", C.c_uint64)]
+                ("oversize_requests", C.c_uint64), ("max_in_flight_bytes", C.c_uint64)]
 
 
 def make_job(spec, keep: list) -> tuple:

@@ -53,18 +53,15 @@ void check_ptr(const void* ptr, size_t n, const char* what) {
 Buf upload(fpx::Engine& e, uint32_t p, const uint32_t* h, size_t n, int repr) {
   Buf d(&e.pool(), n);
   if (n) {
-    e.check(cudaMemcpyAsync(d.get(), h, n * 4, cudaMemcpyHostToDevice, e.stream()), "H2D");
+    e.to_device(d.get(), h, n);
     if (repr == FPX_REPR_MONTGOMERY) e.check(fpx::launch_from_mont(p, d.get(), d.get(), n, e.stream()), "repr");
   }
   return d;
 }
 
 void download(fpx::Engine& e, uint32_t p, uint32_t* h, uint32_t* d, size_t n, int repr) {
-  if (n) {
-    if (repr == FPX_REPR_MONTGOMERY) e.check(fpx::launch_to_mont(p, d, d, n, e.stream()), "repr");
-    e.check(cudaMemcpyAsync(h, d, n * 4, cudaMemcpyDeviceToHost, e.stream()), "D2H");
-  }
-  e.sync();
+  if (n && repr == FPX_REPR_MONTGOMERY) e.check(fpx::launch_to_mont(p, d, d, n, e.stream()), "repr");
+  e.to_host(h, d, n);
 }
 
 void check_repr(int repr) {
@@ -372,12 +369,12 @@ static int divmod_host(fpx_ctx* ctx, uint32_t p, const uint32_t* a, size_t la, c
     if (want_q) {
       check_ptr(q, lq, "q");
       if (repr == FPX_REPR_MONTGOMERY && lq) e.check(fpx::launch_to_mont(p, dq.get(), dq.get(), lq, e.stream()), "repr");
-      if (lq) e.check(cudaMemcpyAsync(q, dq.get(), lq * 4, cudaMemcpyDeviceToHost, e.stream()), "D2H");
+      e.to_host(q, dq.get(), lq);
     }
     if (want_r) {
       check_ptr(r, lr, "r");
       if (repr == FPX_REPR_MONTGOMERY && lr) e.check(fpx::launch_to_mont(p, dr.get(), dr.get(), lr, e.stream()), "repr");
-      if (lr) e.check(cudaMemcpyAsync(r, dr.get(), lr * 4, cudaMemcpyDeviceToHost, e.stream()), "D2H");
+      e.to_host(r, dr.get(), lr);
     }
     e.sync();
     if (want_q) *q_len = lq;

@@ -10,7 +10,10 @@
 // inverse together) plus three for exp, however many jobs there are.
 #include <algorithm>
 #include <bit>
+#include <condition_variable>
 #include <cstring>
+#include <mutex>
+#include <thread>
 
 #include "engine.h"
 
@@ -881,6 +884,104 @@ void Engine::batch_host(fpx_job* jobs, size_t count, int repr) {
 
 namespace {
 constexpr size_t kPinWords = size_t(8) << 20;  // 32 MiB per slot
+
+// Host copies between the caller's buffers and the pinned staging slots, split
+// across a small process-wide pool of threads: one thread moves about 10 GB/s
+// of host memory, the PCIe link 50 GB/s each way, so a single-threaded packing
+// loop would set the pace of every host-buffer batch.
+struct CopyPiece {
+  void* dst;
+  const void* src;
+  size_t bytes;
+};
+
+class CopyPool {
+ public:
+  static CopyPool& instance() {
+    static CopyPool pool;
+    return pool;
+  }
+  // Copies every piece; returns when all bytes are in place.  Small totals stay
+  // on the calling thread.
+  void run(const std::vector<CopyPiece>& pieces) {
+    size_t total = 0;
+    for (const CopyPiece& c : pieces) total += c.bytes;
+    if (total < kParallelBytes || threads_.empty()) {
+      part(pieces, 0, total);
+      return;
+    }
+    std::lock_guard<std::mutex> call(call_mu_);  // one parallel copy at a time
+    const int n = (int)threads_.size() + 1;
+    {
+      std::lock_guard<std::mutex> g(mu_);
+      pieces_ = &pieces;
+      total_ = total;
+      parts_ = n;
+      remaining_ = n - 1;
+      ++gen_;
+    }
+    cv_.notify_all();
+    part(pieces, 0, total / n);  // the caller's share: part 0
+    std::unique_lock<std::mutex> g(mu_);
+    done_.wait(g, [&] { return remaining_ == 0; });
+  }
+  ~CopyPool() {
+    {
+      std::lock_guard<std::mutex> g(mu_);
+      stop_ = true;
+    }
+    cv_.notify_all();
+    for (auto& t : threads_) t.join();
+  }
+
+ private:
+  static constexpr size_t kParallelBytes = size_t(2) << 20;
+  CopyPool() {
+    const unsigned hw = std::thread::hardware_concurrency();
+    const int extra = (int)std::min(7u, hw > 2 ? hw / 2 - 1 : 0u);
+    for (int i = 1; i <= extra; ++i) threads_.emplace_back([this, i] { loop(i); });
+  }
+  // Bytes [lo, hi) of the concatenated pieces.
+  static void part(const std::vector<CopyPiece>& pieces, size_t lo, size_t hi) {
+    size_t at = 0;
+    for (const CopyPiece& c : pieces) {
+      const size_t a = std::max(lo, at), b = std::min(hi, at + c.bytes);
+      if (a < b) std::memcpy(static_cast<char*>(c.dst) + (a - at), static_cast<const char*>(c.src) + (a - at), b - a);
+      at += c.bytes;
+      if (at >= hi) break;
+    }
+  }
+  void loop(int id) {
+    uint64_t seen = 0;
+    for (;;) {
+      const std::vector<CopyPiece>* pieces;
+      size_t lo, hi;
+      {
+        std::unique_lock<std::mutex> g(mu_);
+        cv_.wait(g, [&] { return stop_ || gen_ != seen; });
+        if (stop_) return;
+        seen = gen_;
+        pieces = pieces_;
+        lo = total_ * id / parts_;
+        hi = total_ * (id + 1) / parts_;
+      }
+      part(*pieces, lo, hi);
+      {
+        std::lock_guard<std::mutex> g(mu_);
+        --remaining_;
+      }
+      done_.notify_one();
+    }
+  }
+  std::vector<std::thread> threads_;
+  std::mutex call_mu_, mu_;
+  std::condition_variable cv_, done_;
+  const std::vector<CopyPiece>* pieces_ = nullptr;
+  size_t total_ = 0;
+  int parts_ = 1, remaining_ = 0;
+  uint64_t gen_ = 0;
+  bool stop_ = false;
+};
 }
 
 uint32_t* Engine::pin_slot(int k) {
@@ -894,15 +995,48 @@ uint32_t* Engine::pin_slot(int k) {
   return q.host;
 }
 
+namespace {
+// Pageable host memory of at least this size goes through the pinned slots.
+constexpr size_t kStagedBytes = size_t(1) << 20;
+bool pinned(const void* p) {
+  cudaPointerAttributes a{};
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeHost || a.type == cudaMemoryTypeManaged;
+}
+}  // namespace
+
+void Engine::to_device(uint32_t* d_dst, const uint32_t* h_src, size_t words) {
+  if (!words) return;
+  if (words * 4 < kStagedBytes || pinned(h_src)) {
+    check(cudaMemcpyAsync(d_dst, h_src, words * 4, cudaMemcpyHostToDevice, stream_), "H2D");
+    return;
+  }
+  copy_in({HostSpan{h_src, nullptr, words}}, d_dst);
+}
+
+void Engine::to_host(uint32_t* h_dst, const uint32_t* d_src, size_t words) {
+  if (words && (words * 4 < kStagedBytes || pinned(h_dst))) {
+    check(cudaMemcpyAsync(h_dst, d_src, words * 4, cudaMemcpyDeviceToHost, stream_), "D2H");
+  } else if (words) {
+    copy_out(d_src, {HostSpan{nullptr, h_dst, words}});
+  }
+  sync();
+}
+
 void Engine::copy_in(const std::vector<HostSpan>& spans, uint32_t* dst) {
   size_t si = 0, so = 0;
   int k = 0;
+  std::vector<CopyPiece> pieces;
   while (si < spans.size()) {
     uint32_t* h = pin_slot(k);
     size_t filled = 0;
+    pieces.clear();
     while (si < spans.size() && filled < kPinWords) {
       const size_t take = std::min(spans[si].words - so, kPinWords - filled);
-      std::memcpy(h + filled, spans[si].src + so, take * 4);
+      pieces.push_back(CopyPiece{h + filled, spans[si].src + so, take * 4});
       filled += take;
       so += take;
       if (so == spans[si].words) {
@@ -910,6 +1044,7 @@ void Engine::copy_in(const std::vector<HostSpan>& spans, uint32_t* dst) {
         so = 0;
       }
     }
+    CopyPool::instance().run(pieces);
     check(cudaMemcpyAsync(dst, h, filled * 4, cudaMemcpyHostToDevice, stream_), "H2D");
     check(cudaEventRecord(pins_[k].ev, stream_), "event");
     dst += filled;
@@ -922,6 +1057,7 @@ void Engine::copy_out(const uint32_t* src, const std::vector<HostSpan>& spans) {
   for (const HostSpan& s : spans) total += s.words;
   const size_t chunks = (total + kPinWords - 1) / kPinWords;
   size_t si = 0, so = 0;
+  std::vector<CopyPiece> pieces;
   auto issue = [&](size_t c) {  // D2H of chunk c into slot c % 2
     const int k = (int)(c & 1);
     uint32_t* h = pin_slot(k);
@@ -937,9 +1073,10 @@ void Engine::copy_out(const uint32_t* src, const std::vector<HostSpan>& spans) {
     const uint32_t* h = pins_[k].host;
     const size_t w = std::min(kPinWords, total - c * kPinWords);
     size_t used = 0;
+    pieces.clear();
     while (used < w) {
       const size_t take = std::min(spans[si].words - so, w - used);
-      if (spans[si].dst) std::memcpy(spans[si].dst + so, h + used, take * 4);
+      if (spans[si].dst) pieces.push_back(CopyPiece{spans[si].dst + so, h + used, take * 4});
       used += take;
       so += take;
       if (so == spans[si].words) {
@@ -947,6 +1084,7 @@ void Engine::copy_out(const uint32_t* src, const std::vector<HostSpan>& spans) {
         so = 0;
       }
     }
+    CopyPool::instance().run(pieces);
     if (c + 2 < chunks) issue(c + 2);
   }
   sync();

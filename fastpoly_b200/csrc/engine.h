@@ -145,6 +145,13 @@ class Engine {
   void check(cudaError_t e, const char* what);
   void sync();
 
+  // Host <-> device copies of the host-buffer entry points.  Pinned (or small)
+  // host buffers go straight to cudaMemcpyAsync on the stream; pageable ones
+  // through the engine's pinned slots, packed by several host threads while
+  // the previous slot's DMA runs.  to_host returns with the words in place.
+  void to_device(uint32_t* d_dst, const uint32_t* h_src, size_t words);
+  void to_host(uint32_t* h_dst, const uint32_t* d_src, size_t words);
+
   // Column-pass tile shapes of N = 2^logN transforms on this device (kind 0:
   // forward pass of one operand, 1: of two or three, 2: inverse pass), chosen
   // by timing the compiled candidates once per process, device and size

@@ -1,5 +1,5 @@
-// serve.cpp - request loop with HBM-budget admission and continuous batching
-// (the C ABI's fpx_serve_*).  The reference has no server; this serves its
+// serve.cpp - request loop with device-wide HBM-budget admission, size lanes
+// and continuous batching (the C ABI's fpx_serve_*).  The reference has no server; this serves its
 // batch/serve workload (mixed operations, sizes and moduli arriving over time)
 // with the same per-request results as the single-operation functions.
 #include <algorithm>
@@ -91,46 +91,94 @@ extern "C" size_t fpx_serve_plan_bytes(const fpx_job* j) {
   return 4 * (in + out + scratch) + 1024;
 }
 
+// Size lanes: requests of at most 2^kSmallLaneLog terms (the longest operand,
+// or the series length) go to the small lane, the rest to the large lane.  Each
+// lane has its own queue and workers, so a short request is never batched with
+// (and held behind) a 2^22-term one.
+constexpr int kSmallLaneLog = 17;
+
+int lane_of(const fpx_job* j) {
+  size_t n = 0;
+  switch (j->op) {
+    case FPX_OP_CONV: n = std::max(std::min(j->la, j->n), std::min(j->lb, j->n)); break;
+    case FPX_OP_DIVMOD: n = std::max(j->la, j->lb); break;
+    default: n = j->n;
+  }
+  return n <= (size_t(1) << kSmallLaneLog) ? 0 : 1;
+}
+
 struct fpx_server {
   int device = 0;
   fpx_serve_config cfg{};
   std::mutex mu;
   std::condition_variable cv_work, cv_done;
-  std::deque<Request*> queue;
+  std::deque<Request*> queue[2];  // per lane, arrival order
   std::unordered_map<uint64_t, std::unique_ptr<Request>> all;
   uint64_t next_ticket = 1;
   bool stopping = false;
   std::vector<std::thread> workers;
   std::vector<std::unique_ptr<fpx::Engine>> engines;
   fpx_serve_stats stats{};
-  int start_error = FPX_OK;
+  int small_workers = 1;
+  // Device-wide admission: planned bytes of every micro-batch on the GPU,
+  // charged when it is formed and refunded when it completes.
+  size_t in_flight = 0;
+  // The large lane's oldest request does not fit the bytes left: no lane admits
+  // new work until it does, so large requests cannot be starved by small ones.
+  bool large_waiting = false;
+
+  bool drained() const { return queue[0].empty() && queue[1].empty(); }
+
+  // Forms one micro-batch for a worker of `lane` (mu held): from the lane's own
+  // queue, or, for the large lane with nothing of its own, from the small lane.
+  // Returns the planned bytes taken (mine empty: nothing admissible now).
+  size_t admit(int lane, std::vector<Request*>& mine) {
+    const bool own = !queue[lane].empty();
+    if (!own && lane == 0) return 0;
+    std::deque<Request*>& q = own ? queue[lane] : queue[0];
+    if (large_waiting && !(own && lane == 1)) return 0;
+    size_t bytes = 0;
+    while (!q.empty() && mine.size() < cfg.max_batch_jobs) {
+      Request* r = q.front();
+      const size_t total = in_flight + bytes + r->bytes;
+      const bool alone = in_flight == 0 && mine.empty();  // a request larger than the budget runs alone
+      if (total > cfg.hbm_budget_bytes && !alone) {
+        if (own && lane == 1 && mine.empty()) large_waiting = true;
+        break;
+      }
+      if (r->bytes > cfg.hbm_budget_bytes) ++stats.oversize_requests;
+      bytes += r->bytes;
+      mine.push_back(r);
+      q.pop_front();
+    }
+    if (!mine.empty() && own && lane == 1) large_waiting = false;
+    return bytes;
+  }
 
   void worker(int w) {
     fpx::Engine& eng = *engines[w];
+    const int lane = w < small_workers ? 0 : 1;
     cudaSetDevice(device);
     std::vector<Request*> mine;
     std::vector<fpx_job> jobs;
     for (;;) {
       mine.clear();
+      size_t bytes = 0;
       {
         std::unique_lock<std::mutex> g(mu);
-        cv_work.wait(g, [&] { return stopping || !queue.empty(); });
-        if (queue.empty()) return;  // stopping and drained
-        // admission: arrival order, while the planned bytes fit the budget
-        size_t bytes = 0;
-        while (!queue.empty() && mine.size() < cfg.max_batch_jobs) {
-          Request* r = queue.front();
-          if (!mine.empty() && bytes + r->bytes > cfg.hbm_budget_bytes) break;
-          if (r->bytes > cfg.hbm_budget_bytes) ++stats.oversize_requests;
-          bytes += r->bytes;
-          mine.push_back(r);
-          queue.pop_front();
+        for (;;) {
+          bytes = admit(lane, mine);
+          if (!mine.empty()) break;
+          if (stopping && drained()) return;
+          cv_work.wait(g);
         }
+        in_flight += bytes;
         ++stats.batches;
         stats.max_batch_jobs_seen = std::max<uint64_t>(stats.max_batch_jobs_seen, mine.size());
         stats.max_batch_bytes_seen = std::max<uint64_t>(stats.max_batch_bytes_seen, bytes);
-        if (!queue.empty()) cv_work.notify_one();  // more work for another worker
+        stats.max_in_flight_bytes = std::max<uint64_t>(stats.max_in_flight_bytes, in_flight);
       }
+      cv_work.notify_all();  // another worker may admit from what is left
       jobs.resize(mine.size());
       for (size_t i = 0; i < mine.size(); ++i) jobs[i] = *mine[i]->job;
       int whole = FPX_OK;
@@ -154,8 +202,10 @@ struct fpx_server {
           mine[i]->done = true;
           ++stats.completed;
         }
+        in_flight -= bytes;
       }
       cv_done.notify_all();
+      cv_work.notify_all();  // bytes were refunded
     }
   }
 };
@@ -168,9 +218,20 @@ int fpx_serve_start(int device, const fpx_serve_config* cfg, fpx_server** out) {
   auto s = std::make_unique<fpx_server>();
   s->device = device;
   if (cfg) s->cfg = *cfg;
-  if (s->cfg.hbm_budget_bytes == 0) s->cfg.hbm_budget_bytes = size_t(8) << 30;
+  if (s->cfg.hbm_budget_bytes == 0) {
+    // a quarter of the device memory free at start, at most 32 GiB
+    size_t free_b = 0, total_b = 0;
+    if (cudaSetDevice(device) != cudaSuccess || cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) {
+      cudaGetLastError();
+      free_b = size_t(32) << 30;
+    }
+    s->cfg.hbm_budget_bytes = std::min(free_b / 4, size_t(32) << 30);
+  }
   if (s->cfg.max_batch_jobs == 0) s->cfg.max_batch_jobs = 4096;
-  if (s->cfg.workers <= 0) s->cfg.workers = 2;
+  if (s->cfg.workers <= 0) s->cfg.workers = 4;
+  if (s->cfg.workers < 2) s->cfg.workers = 2;
+  // half the workers (at least one) for the large lane, the rest for the small lane
+  s->small_workers = s->cfg.workers - std::max(1, s->cfg.workers / 2);
   if (s->cfg.repr != FPX_REPR_CANONICAL && s->cfg.repr != FPX_REPR_MONTGOMERY) return FPX_EINVAL;
   try {
     for (int w = 0; w < s->cfg.workers; ++w) s->engines.push_back(std::make_unique<fpx::Engine>(device, 0));
@@ -196,11 +257,11 @@ int fpx_serve_submit(fpx_server* srv, fpx_job* job, uint64_t* ticket) {
     if (srv->stopping) return FPX_EINVAL;
     r->ticket = srv->next_ticket++;
     *ticket = r->ticket;
-    srv->queue.push_back(r.get());
+    srv->queue[lane_of(job)].push_back(r.get());
     srv->all.emplace(r->ticket, std::move(r));
     ++srv->stats.submitted;
   }
-  srv->cv_work.notify_one();
+  srv->cv_work.notify_all();
   return FPX_OK;
 }
 

@@ -202,17 +202,26 @@ int fpx_batch_run(fpx_ctx* ctx, fpx_job* jobs, size_t count, int repr);
 /* ---- serving (no counterpart in the reference) --------------------------------
  * A request loop on one GPU.  Requests are fpx_job records with HOST buffers;
  * the job record and its buffers must stay valid until fpx_serve_poll reports
- * completion.  Worker threads, each with its own stream and device pool, form
- * micro-batches from whatever is queued when they become free (continuous
- * batching): requests are admitted in arrival order while the sum of their
- * planned device bytes (operands, results and transform scratch) fits the HBM
- * budget (a request larger than the budget runs alone), and each micro-batch
- * runs as fpx_batch_run.  Every request's result is the one the single-job
- * function gives it, whatever it was batched with. */
+ * completion.  Requests go to one of two size lanes: at most 2^17 terms (the
+ * longest operand, or the series length) to the small lane, the rest to the
+ * large lane; each lane has its own queue and worker threads (each with its own
+ * stream and device pool), so a short request is never batched with, and held
+ * behind, a long one.  A free worker forms a micro-batch from its lane's queue
+ * in arrival order (continuous batching: what arrives while others run joins
+ * the next micro-batch; the large lane's workers also take small requests when
+ * their own queue is empty).  Admission is device-wide: a micro-batch is formed
+ * only while the planned device bytes of everything on the GPU (operands,
+ * results and transform scratch, fpx_serve_plan_bytes) stay within the budget,
+ * charged when it is formed and refunded when it completes; a request larger
+ * than the whole budget runs alone, and when the large lane's oldest request
+ * does not fit, no lane admits new work until it does.  Every request's result
+ * is the one the single-job function gives it, whatever it was batched with. */
 typedef struct fpx_serve_config {
-  size_t hbm_budget_bytes; /* planned device bytes per micro-batch; 0 = 8 GiB */
+  size_t hbm_budget_bytes; /* planned device bytes of all requests on the GPU at once;
+                              0 = a quarter of the device memory free at start, at most 32 GiB */
   size_t max_batch_jobs;   /* 0 = 4096 */
-  int workers;             /* micro-batches in flight; 0 = 2 */
+  int workers;             /* worker threads (at least 2): half for the large lane, the rest for the small
+                              lane; 0 = 4 */
   int repr;                /* FPX_REPR_CANONICAL or FPX_REPR_MONTGOMERY for every request */
 } fpx_serve_config;
 
@@ -221,6 +230,7 @@ typedef struct fpx_serve_stats {
   uint64_t max_batch_jobs_seen;     /* largest micro-batch formed */
   uint64_t max_batch_bytes_seen;    /* largest planned device bytes admitted in one micro-batch */
   uint64_t oversize_requests;       /* requests that alone exceeded the budget (ran alone) */
+  uint64_t max_in_flight_bytes;     /* largest planned device bytes of all micro-batches on the GPU at once */
 } fpx_serve_stats;
 
 typedef struct fpx_server fpx_server;

@@ -1,6 +1,8 @@
 """The request loop (fpx_serve_*): every request gets the result the single call
-gives it, whatever it was batched with; admission keeps micro-batches within
-the HBM budget; stopping drains the queue."""
+and the oracle give it, whatever it was batched with; admission keeps all
+micro-batches on the GPU within one device-wide HBM budget; short requests are
+not held behind long ones; stopping drains the queue."""
+import time
 import threading
 
 import numpy as np
@@ -8,7 +10,7 @@ import pytest
 
 import fastpoly_b200 as F
 from test_gpu_parity import eq, rnd
-from test_gpu_batch import _check
+from test_gpu_batch import _check, _oracle_job
 
 pytestmark = pytest.mark.gpu
 
@@ -58,7 +60,7 @@ def _alone(fpx, spec):
         return e
 
 
-def test_served_results_equal_single_calls(fpx):
+def test_served_results_equal_single_calls(fpx, oracle):
     rng = np.random.default_rng(2025)
     specs = _mix(rng, 300)
     srv = F.Server(0)
@@ -73,6 +75,7 @@ def test_served_results_equal_single_calls(fpx):
         res, lat = got[i]
         assert lat > 0
         _check(res, _alone(fpx, s), f"request {i} {s[0]} p={s[1]}")
+        _check(res, _oracle_job(oracle, s), f"request {i} {s[0]} p={s[1]} vs oracle")
 
 
 def test_admission_respects_budget(fpx):
@@ -143,3 +146,54 @@ def test_stop_drains_queue():
     for t in tickets:
         j = live[t][0]
         assert j.status in (F.OK, F.EDOMAIN)
+
+
+def test_small_requests_not_held_behind_a_large_one(oracle):
+    """A 2^22-term inverse modulo 1e9+7 (three-prime CRT Newton steps, a few ms)
+    submitted first, then 40 short products: every short one completes before
+    the long one, and all results are exact."""
+    rng = np.random.default_rng(17)
+    q = 1000000007
+    big = rnd(rng, q, 1 << 22, nonzero0=True)
+    smalls = [("conv", 998244353, rnd(rng, 998244353, 700), rnd(rng, 998244353, 900)) for _ in range(40)]
+    srv = F.Server(0)
+    try:
+        t_big = time.perf_counter()
+        tb = srv.submit(("inv", q, big, 1 << 22))
+        subs = []
+        for s in smalls:
+            subs.append((time.perf_counter(), srv.submit(s)))
+        done_small = []
+        for t0, t in subs:
+            r, lat = srv.poll(t)
+            done_small.append(t0 + lat)
+        rb, lat_b = srv.poll(tb)
+    finally:
+        srv.stop()
+    done_big = t_big + lat_b
+    assert max(done_small) < done_big, (max(done_small) - t_big, lat_b)
+    want = oracle.inv(q, big[:4096], 4096)
+    eq(rb[:4096], want, "served big inverse (first 4096 terms)")
+
+
+def test_device_wide_budget(oracle):
+    """Three workers share one 48 MiB budget: the planned bytes of everything on
+    the GPU at once never exceed it, and every result is exact."""
+    rng = np.random.default_rng(23)
+    p = 998244353
+    specs = [("conv", p, rnd(rng, p, 1 << 17), rnd(rng, p, 1 << 17)) for _ in range(12)]
+    specs += [("conv", p, rnd(rng, p, 3000), rnd(rng, p, 2000)) for _ in range(30)]
+    specs += [("inv", p, rnd(rng, p, 1 << 18, nonzero0=True), 1 << 18) for _ in range(4)]
+    budget = 48 << 20
+    srv = F.Server(0, hbm_budget_bytes=budget, workers=3)
+    try:
+        assert all(srv.plan_bytes(s) <= budget for s in specs)
+        tickets = [srv.submit(s) for s in specs]
+        got = [srv.poll(t)[0] for t in tickets]
+        st = srv.stats()
+    finally:
+        srv.stop()
+    assert st["oversize_requests"] == 0
+    assert 0 < st["max_in_flight_bytes"] <= budget, st
+    for i, s in enumerate(specs):
+        _check(got[i], _oracle_job(oracle, s), f"request {i} {s[0]}")
