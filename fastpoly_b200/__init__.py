@@ -134,6 +134,23 @@ class Job(C.Structure):
                 ("out2", C.c_void_p), ("out_len", C.c_size_t), ("out2_len", C.c_size_t), ("status", C.c_int)]
 
 
+# The same layout as a numpy record: a batch's job array is filled column-wise.
+_JOB_DTYPE = np.dtype({"names": [n for n, _ in Job._fields_],
+                       "formats": [np.int32, np.uint32, np.uint64, np.uint64, np.uint64, np.uint64, np.uint64,
+                                   np.uint64, np.uint64, np.uint64, np.uint64, np.uint64, np.int32],
+                       "offsets": [getattr(Job, n).offset for n, _ in Job._fields_],
+                       "itemsize": C.sizeof(Job)})
+
+
+def _host_u32(x, keep: list):
+    """x as a C-contiguous uint32 array (converted only when it is not one)."""
+    if isinstance(x, np.ndarray) and x.dtype == np.uint32 and x.flags.c_contiguous:
+        return x
+    a = _arr(x)
+    keep.append(a)
+    return a
+
+
 class ServeConfig(C.Structure):
     """struct fpx_serve_config."""
     _fields_ = [("hbm_budget_bytes", C.c_size_t), ("max_batch_jobs", C.c_size_t), ("workers", C.c_int),
@@ -466,20 +483,98 @@ class Context:
 
         Each job is a tuple: ("conv", p, a, b[, n]), ("inv" | "log" | "exp" | "sqrt", p, a, n),
         ("pow", p, a, k, n) or ("divmod", p, a, b).  Returns one entry per job: the
-        result array ((q, r) for divmod), or the exception the single-job call would
-        raise for that job (not raised).
+        result array ((q, r) for divmod; views into one output buffer), or the
+        exception the single-job call would raise for that job (not raised).
         """
-        arr = (Job * max(len(jobs), 1))()
-        keep, outs = [], []
-        for i, jb in enumerate(jobs):
-            j, o1, o2 = make_job(jb, keep)
-            arr[i] = j
-            outs.append((o1, o2))
-        rc = self._L.fpx_batch_run(self._h, C.cast(arr, C.c_void_p), len(jobs), repr)
+        m = len(jobs)
+        keep = []
+        op, pp, ca, cla, cb, clb, ck, cn, cap1, cap2 = ([] for _ in range(10))
+        u32 = np.uint32
+        conv_op, pow_op, div_op = OP_CONV, OP_POW, OP_DIVMOD
+        cfb, addr = C.c_char.from_buffer, C.addressof
+
+        def ptr(x):  # a third of the cost of __array_interface__ (read-only arrays fall back)
+            try:
+                return addr(cfb(x))
+            except TypeError:
+                return x.__array_interface__["data"][0]
+
+        for jb in jobs:
+            o = _OPS[jb[0]]
+            op.append(o)
+            pp.append(jb[1])
+            a = jb[2]
+            if not (type(a) is np.ndarray and a.dtype == u32 and a.flags.c_contiguous):
+                a = _arr(a)
+                keep.append(a)
+            na = a.size
+            cla.append(na)
+            ca.append(ptr(a) if na else 0)
+            nb = 0
+            if o == conv_op or o == div_op:
+                bb = jb[3]
+                if not (type(bb) is np.ndarray and bb.dtype == u32 and bb.flags.c_contiguous):
+                    bb = _arr(bb)
+                    keep.append(bb)
+                nb = bb.size
+                clb.append(nb)
+                cb.append(ptr(bb) if nb else 0)
+            else:
+                clb.append(0)
+                cb.append(0)
+            if o == conv_op:
+                n = SIZE_MAX if len(jb) < 5 or jb[4] is None else int(jb[4])
+                cn.append(n)
+                ck.append(0)
+                cap = min(na, n) + min(nb, n) - 1 if na and nb and n else 0
+                cap1.append(max(min(cap, n), 1))
+                cap2.append(0)
+            elif o == pow_op:
+                ck.append(int(jb[3]))
+                cn.append(int(jb[4]))
+                cap1.append(max(int(jb[4]), 1))
+                cap2.append(0)
+            elif o == div_op:
+                ck.append(0)
+                cn.append(0)
+                cap1.append(max(na, 1))
+                cap2.append(max(nb, 1))
+            else:
+                ck.append(0)
+                cn.append(int(jb[3]))
+                cap1.append(max(int(jb[3]), 1))
+                cap2.append(0)
+        cols = {"a": ca, "la": cla, "b": cb, "lb": clb, "k": ck, "n": cn}
+        op = np.asarray(op, np.int32)
+        cap1 = np.asarray(cap1, np.int64)
+        cap2 = np.asarray(cap2, np.int64)
+        off1 = np.zeros(m, np.int64)
+        if m:
+            np.cumsum((cap1 + cap2)[:-1], out=off1[1:])
+        off2 = off1 + cap1
+        out = np.empty(max(int((cap1 + cap2).sum()), 1), np.uint32)
+        base = np.uint64(out.__array_interface__["data"][0])
+        arr = np.zeros(max(m, 1), dtype=_JOB_DTYPE)
+        v = arr[:m]
+        v["op"], v["p"] = op, np.asarray(pp, np.uint32)
+        for f in ("a", "la", "b", "lb", "k", "n"):
+            v[f] = np.asarray(cols[f], np.uint64)
+        v["out"] = base + np.uint64(4) * off1.astype(np.uint64)
+        v["out2"] = np.where(cap2 > 0, base + np.uint64(4) * off2.astype(np.uint64), np.uint64(0))
+        rc = self._L.fpx_batch_run(self._h, arr.ctypes.data, m, repr)
         if rc not in (OK, EDOMAIN, ESIZE, ELENGTH, EINVAL):
             self._check(rc, "batch")
-        return [job_result(arr[i], outs[i][0], outs[i][1], f"batch job {i} ({jobs[i][0]})")
-                for i in range(len(jobs))]
+        st, ol, ol2 = v["status"].tolist(), v["out_len"].tolist(), v["out2_len"].tolist()
+        o1s, o2s, ops = off1.tolist(), off2.tolist(), op.tolist()
+        res = []
+        for i in range(m):
+            if st[i] != OK:
+                res.append(_ERRORS.get(st[i], FpxError)(st[i], f"batch job {i} ({jobs[i][0]})"))
+            elif ops[i] == OP_DIVMOD:
+                res.append((out[o1s[i]: o1s[i] + ol[i]], out[o2s[i]: o2s[i] + ol2[i]]))
+            else:
+                res.append(out[o1s[i]: o1s[i] + ol[i]])
+        return res
 
     def batch_submit(self, jobs) -> int:
         """fpx_batch_submit on a ctypes array of Job with device pointers; returns the call's status

@@ -10,6 +10,7 @@
 // inverse together) plus three for exp, however many jobs there are.
 #include <algorithm>
 #include <bit>
+#include <chrono>
 #include <condition_variable>
 #include <cstring>
 #include <mutex>
@@ -173,10 +174,14 @@ class BatchRec {
       if (!g.c2) g.c2 = g.c1;
       if (!g.c3) g.c3 = g.c1;
     }
+    const auto ts = std::chrono::steady_clock::now();
     Engine::Stage& st = e_.stage(batch_descriptor_bytes(plan_));
+    const auto tl = std::chrono::steady_clock::now();
     e_.prof_begin();
     e_.check(launch_batch(plan_, st.host, st.dev.get(), e_.stream(), st.ev), "batch");
     e_.prof_end("batch");
+    e_.host_phase("stage_wait", std::chrono::duration<double, std::milli>(tl - ts).count());
+    e_.host_phase("launch_batch", std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - tl).count());
     e_.count_batch(plan_);
     plan_ = BatchPlan();
     need_.clear();
@@ -436,15 +441,20 @@ void Engine::batch(fpx_job* jobs, size_t count) {
       if (route[i] == kConv) order.push_back(i);
     auto cls = [&](size_t i) { return std::bit_width(conv_len[i]); };
     std::stable_sort(order.begin(), order.end(), [&](size_t x, size_t y) { return cls(x) > cls(y); });
+    using HClock = std::chrono::steady_clock;
     for (size_t k = 0; k < order.size();) {
       BatchRec rec(*this);
       const int c = cls(order[k]);
+      auto t0 = HClock::now();
       for (; k < order.size() && cls(order[k]) == c; ++k) {
         const fpx_job& j = jobs[order[k]];
         rec.product(j.p, j.a, std::min(j.la, j.n), j.b, std::min(j.lb, j.n), 0, conv_len[order[k]], j.out, 0,
                     nullptr, false);
       }
+      auto t1 = HClock::now();
       rec.flush();
+      host_phase("conv_record", std::chrono::duration<double, std::milli>(t1 - t0).count());
+      host_phase("conv_flush", std::chrono::duration<double, std::milli>(HClock::now() - t1).count());
     }
   }
 
@@ -826,19 +836,35 @@ void Engine::batch_host(fpx_job* jobs, size_t count, int repr) {
   uint32_t* din = dbuf.get();
   uint32_t* dout = din + in_words;
   std::vector<fpx_job> dj(jobs, jobs + count);
-  std::vector<ReprSeg> segs;
-  std::vector<HostSpan> ins;
+  // Two chunks of about equal input words when the batch moves at least
+  // 64 MiB: the host packs the second while the GPU runs the first, and unpacks
+  // the first (copied back on the copy stream) while the GPU runs the second.
+  size_t cut = count;
+  if (count >= 2 && in_words * 4 >= (size_t(64) << 20)) {
+    size_t acc = 0;
+    for (cut = 0; cut + 1 < count && acc < in_words / 2; ++cut) acc += wa[cut] + wb[cut];
+  }
+  const size_t bounds[3] = {0, cut, count};
+  const int nchunks = cut < count && cut > 0 ? 2 : 1;
+  std::vector<ReprSeg> segs[2];
+  std::vector<HostSpan> ins[2];
+  size_t in_off[3] = {0, 0, in_words}, out_off[3] = {0, 0, out_words};
   size_t qi = 0, qo = 0;
   for (size_t i = 0; i < count; ++i) {
+    const int c = nchunks == 2 && i >= cut ? 1 : 0;
+    if (nchunks == 2 && i == cut) {
+      in_off[1] = qi;
+      out_off[1] = qo;
+    }
     const fpx_job& j = jobs[i];
     fpx_job& d = dj[i];
-    if (wa[i]) ins.push_back(HostSpan{j.a, nullptr, wa[i]});
+    if (wa[i]) ins[c].push_back(HostSpan{j.a, nullptr, wa[i]});
     d.a = j.a ? din + qi : nullptr;
-    if (wa[i]) segs.push_back(ReprSeg{j.p, din + qi, wa[i], 0});
+    if (wa[i]) segs[c].push_back(ReprSeg{j.p, din + qi, wa[i], 0});
     qi += wa[i];
-    if (wb[i]) ins.push_back(HostSpan{j.b, nullptr, wb[i]});
+    if (wb[i]) ins[c].push_back(HostSpan{j.b, nullptr, wb[i]});
     d.b = j.b ? din + qi : nullptr;
-    if (wb[i]) segs.push_back(ReprSeg{j.p, din + qi, wb[i], 0});
+    if (wb[i]) segs[c].push_back(ReprSeg{j.p, din + qi, wb[i], 0});
     qi += wb[i];
     d.la = j.a ? wa[i] : j.la;  // a null pointer keeps its length: the batch reports it
     d.lb = j.b ? wb[i] : j.lb;
@@ -847,37 +873,64 @@ void Engine::batch_host(fpx_job* jobs, size_t count, int repr) {
     d.out2 = j.out2 ? dout + qo : nullptr;
     qo += wo2[i];
   }
-  copy_in(ins, din);
-  if (repr == FPX_REPR_MONTGOMERY) convert_repr(segs);
-  batch(dj.data(), count);
-  if (repr == FPX_REPR_MONTGOMERY) {
-    segs.clear();
-    for (size_t i = 0; i < count; ++i) {
+  if (nchunks == 1) {
+    in_off[1] = in_words;
+    out_off[1] = out_words;
+  }
+  if (!copy_stream_) {
+    check(cudaStreamCreateWithFlags(&copy_stream_, cudaStreamNonBlocking), "cudaStreamCreate");
+    for (auto& e : chunk_ev_) check(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "cudaEventCreate");
+  }
+  using HClock = std::chrono::steady_clock;
+  auto ms_since = [](HClock::time_point t) { return std::chrono::duration<double, std::milli>(HClock::now() - t).count(); };
+
+  // Results of chunk c: statuses and lengths to the caller's records, then
+  // every output region in device order (result words to the caller's buffer,
+  // the rest skipped), copied on the copy stream once the chunk's work is done.
+  auto drain = [&](int c) {
+    std::vector<HostSpan> outs;
+    for (size_t i = bounds[c]; i < bounds[c + 1]; ++i) {
+      fpx_job& j = jobs[i];
       const fpx_job& d = dj[i];
-      if (d.status != FPX_OK) continue;
-      if (d.out && d.out_len) segs.push_back(ReprSeg{d.p, d.out, d.out_len, 1});
-      if (d.out2 && d.out2_len) segs.push_back(ReprSeg{d.p, d.out2, d.out2_len, 1});
+      j.status = d.status;
+      j.out_len = d.out_len;
+      j.out2_len = d.out2_len;
+      const bool ok = d.status == FPX_OK;
+      const size_t n1 = ok && j.out ? std::min(d.out_len, wo[i]) : 0;
+      const size_t n2 = ok && j.out2 ? std::min(d.out2_len, wo2[i]) : 0;
+      if (n1) outs.push_back(HostSpan{nullptr, j.out, n1});
+      if (wo[i] > n1) outs.push_back(HostSpan{nullptr, nullptr, wo[i] - n1});
+      if (n2) outs.push_back(HostSpan{nullptr, j.out2, n2});
+      if (wo2[i] > n2) outs.push_back(HostSpan{nullptr, nullptr, wo2[i] - n2});
     }
-    convert_repr(segs);
+    check(cudaStreamWaitEvent(copy_stream_, chunk_ev_[c], 0), "cudaStreamWaitEvent");
+    const auto t0 = HClock::now();
+    copy_out(dout + out_off[c], outs, copy_stream_);
+    host_phase("copy_out", ms_since(t0));
+  };
+
+  for (int c = 0; c < nchunks; ++c) {
+    auto t0 = HClock::now();
+    copy_in(ins[c], din + in_off[c]);
+    host_phase("copy_in", ms_since(t0));
+    t0 = HClock::now();
+    if (repr == FPX_REPR_MONTGOMERY) convert_repr(segs[c]);
+    batch(dj.data() + bounds[c], bounds[c + 1] - bounds[c]);
+    if (repr == FPX_REPR_MONTGOMERY) {
+      std::vector<ReprSeg> outs;
+      for (size_t i = bounds[c]; i < bounds[c + 1]; ++i) {
+        const fpx_job& d = dj[i];
+        if (d.status != FPX_OK) continue;
+        if (d.out && d.out_len) outs.push_back(ReprSeg{d.p, d.out, d.out_len, 1});
+        if (d.out2 && d.out2_len) outs.push_back(ReprSeg{d.p, d.out2, d.out2_len, 1});
+      }
+      convert_repr(outs);
+    }
+    check(cudaEventRecord(chunk_ev_[c], stream_), "cudaEventRecord");
+    host_phase("batch", ms_since(t0));
+    if (c > 0) drain(c - 1);
   }
-  // every job's output region, in device order: its result words go to the
-  // caller's buffer, the rest of the region is skipped
-  std::vector<HostSpan> outs;
-  for (size_t i = 0; i < count; ++i) {
-    fpx_job& j = jobs[i];
-    const fpx_job& d = dj[i];
-    j.status = d.status;
-    j.out_len = d.out_len;
-    j.out2_len = d.out2_len;
-    const bool ok = d.status == FPX_OK;
-    const size_t n1 = ok && j.out ? std::min(d.out_len, wo[i]) : 0;
-    const size_t n2 = ok && j.out2 ? std::min(d.out2_len, wo2[i]) : 0;
-    if (n1) outs.push_back(HostSpan{nullptr, j.out, n1});
-    if (wo[i] > n1) outs.push_back(HostSpan{nullptr, nullptr, wo[i] - n1});
-    if (n2) outs.push_back(HostSpan{nullptr, j.out2, n2});
-    if (wo2[i] > n2) outs.push_back(HostSpan{nullptr, nullptr, wo2[i] - n2});
-  }
-  copy_out(dout, outs);
+  drain(nchunks - 1);
 }
 
 // --------------------------------------------------------- pinned staging
@@ -1044,7 +1097,9 @@ void Engine::copy_in(const std::vector<HostSpan>& spans, uint32_t* dst) {
         so = 0;
       }
     }
+    const auto tp = std::chrono::steady_clock::now();
     CopyPool::instance().run(pieces);
+    host_phase("pack", std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - tp).count());
     check(cudaMemcpyAsync(dst, h, filled * 4, cudaMemcpyHostToDevice, stream_), "H2D");
     check(cudaEventRecord(pins_[k].ev, stream_), "event");
     dst += filled;
@@ -1052,7 +1107,8 @@ void Engine::copy_in(const std::vector<HostSpan>& spans, uint32_t* dst) {
   }
 }
 
-void Engine::copy_out(const uint32_t* src, const std::vector<HostSpan>& spans) {
+void Engine::copy_out(const uint32_t* src, const std::vector<HostSpan>& spans, cudaStream_t s) {
+  if (!s) s = stream_;
   size_t total = 0;
   for (const HostSpan& s : spans) total += s.words;
   const size_t chunks = (total + kPinWords - 1) / kPinWords;
@@ -1062,8 +1118,8 @@ void Engine::copy_out(const uint32_t* src, const std::vector<HostSpan>& spans) {
     const int k = (int)(c & 1);
     uint32_t* h = pin_slot(k);
     const size_t off = c * kPinWords, w = std::min(kPinWords, total - off);
-    check(cudaMemcpyAsync(h, src + off, w * 4, cudaMemcpyDeviceToHost, stream_), "D2H");
-    check(cudaEventRecord(pins_[k].ev, stream_), "event");
+    check(cudaMemcpyAsync(h, src + off, w * 4, cudaMemcpyDeviceToHost, s), "D2H");
+    check(cudaEventRecord(pins_[k].ev, s), "event");
   };
   if (chunks > 0) issue(0);
   if (chunks > 1) issue(1);
@@ -1084,10 +1140,12 @@ void Engine::copy_out(const uint32_t* src, const std::vector<HostSpan>& spans) {
         so = 0;
       }
     }
+    const auto tp = std::chrono::steady_clock::now();
     CopyPool::instance().run(pieces);
+    host_phase("unpack", std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - tp).count());
     if (c + 2 < chunks) issue(c + 2);
   }
-  sync();
+  // every chunk's copy was waited for before its words were unpacked
 }
 
 }  // namespace fpx

@@ -296,6 +296,12 @@ Engine::~Engine() {
   }
   if (side_fork_) cudaEventDestroy(side_fork_);
   if (side_join_) cudaEventDestroy(side_join_);
+  if (copy_stream_) {
+    cudaStreamSynchronize(copy_stream_);
+    cudaStreamDestroy(copy_stream_);
+  }
+  for (cudaEvent_t e : chunk_ev_)
+    if (e) cudaEventDestroy(e);
   primes_.clear();
   bigs_.clear();
   inv_tabs_.clear();
@@ -348,12 +354,13 @@ void Engine::profile(bool on) {
     ev_free_.push_back(r.e);
   }
   prof_recs_.clear();
+  host_prof_.clear();
   prof_on_ = on;
 }
 
 std::string Engine::profile_report() {
   sync();
-  std::map<std::string, std::pair<long, double>> agg;
+  std::map<std::string, std::pair<long, double>> agg = host_prof_;
   for (auto& r : prof_recs_) {
     float ms = 0;
     check(cudaEventElapsedTime(&ms, r.b, r.e), "cudaEventElapsedTime");

@@ -282,8 +282,14 @@ class Engine {
   };
   // Host spans, concatenated, -> dst (device), through the pinned slots.
   void copy_in(const std::vector<HostSpan>& spans, uint32_t* dst);
-  // Device region [src, src + sum(words)) -> host spans (null ones skipped).
-  void copy_out(const uint32_t* src, const std::vector<HostSpan>& spans);
+  // Device region [src, src + sum(words)) -> host spans (null ones skipped),
+  // the copies on stream s (nullptr: the engine's stream); returns with every
+  // word in place.
+  void copy_out(const uint32_t* src, const std::vector<HostSpan>& spans, cudaStream_t s = nullptr);
+  // Stream of batch_host's copies back, so that a chunk's results come back
+  // while the next chunk's kernels run, and the events that order them.
+  cudaStream_t copy_stream_ = nullptr;
+  cudaEvent_t chunk_ev_[2] = {nullptr, nullptr};
   // Next ring slot, holding >= bytes, whose previous copy has completed.
   Stage& stage(size_t bytes);
   void free_stages();
@@ -304,6 +310,18 @@ class Engine {
     cudaEvent_t b, e;
   };
   bool prof_on_ = false;
+  // Wall time of named host phases while profiling (reported beside the
+  // kernels as "host:<name>").
+  std::map<std::string, std::pair<long, double>> host_prof_;
+ public:
+  void host_phase(const char* name, double ms) {
+    if (!prof_on_) return;
+    auto& a = host_prof_[std::string("host:") + name];
+    a.first += 1;
+    a.second += ms;
+  }
+  bool profiling() const { return prof_on_; }
+ private:
   cudaEvent_t prof_open_ = nullptr;
   std::vector<ProfRec> prof_recs_;
   std::vector<cudaEvent_t> ev_free_;
