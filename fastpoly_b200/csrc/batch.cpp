@@ -12,6 +12,7 @@
 #include <bit>
 #include <chrono>
 #include <condition_variable>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <thread>
@@ -25,6 +26,9 @@ constexpr size_t kNaiveB = 40;                                        // base.hp
 const uint32_t kCrtPrimesB[3] = {167772161u, 469762049u, 754974721u};  // crt_convolution.hpp:14-18
 // Batched transforms use rows of 2^12 points: at most 2^24 points.
 constexpr int kBatchMaxLog = 24;
+// Terms the fused Newton kernels (one CTA, or a cluster of three for CRT
+// moduli) compute: longer inverses and exponentials start the lockstep loop there.
+size_t fused_terms() { return size_t(1) << newton_inv_max_log(); }
 
 Tw2 shoup_pair_b(uint32_t w, uint32_t p) { return Tw2{w, (uint32_t)(((uint64_t)w << 32) / p)}; }
 size_t round64(size_t w) { return (w + 63) & ~size_t(63); }
@@ -347,6 +351,7 @@ void Engine::batch(fpx_job* jobs, size_t count) {
   std::vector<uint8_t> route(count, kNone);
   std::vector<const uint32_t*> firsts(count, nullptr);
   std::vector<size_t> conv_len(count, 0);
+  std::vector<uint8_t> cont(count, 0);  // inv / exp continued from a fused 2^13-term start
   bool need_first = false;
   const size_t max_series = size_t(1) << kBatchMaxLog;
   for (size_t i = 0; i < count; ++i) {
@@ -428,6 +433,10 @@ void Engine::batch(fpx_job* jobs, size_t count) {
                           (crt_newton_on() && (route[i] != kExp || (p & 1u))));
       if (small && route[i] == kInv) route[i] = kInvF;
       if (small && route[i] == kExp && std::min(j.la, j.n) > 1 && j.n > 1) route[i] = kExpF;
+      // longer inverses and exponentials on the same moduli: their first 2^13
+      // terms come from the same fused kernels, the lockstep loop continues
+      const bool fusable = native(p, newton_inv_max_log()) || (crt_newton_on() && (route[i] != kExp || (p & 1u)));
+      if (fusable && !small && (route[i] == kInv || (route[i] == kExp && std::min(j.la, j.n) > 1))) cont[i] = 1;
     }
   }
 
@@ -442,6 +451,11 @@ void Engine::batch(fpx_job* jobs, size_t count) {
     auto cls = [&](size_t i) { return std::bit_width(conv_len[i]); };
     std::stable_sort(order.begin(), order.end(), [&](size_t x, size_t y) { return cls(x) > cls(y); });
     using HClock = std::chrono::steady_clock;
+    // One flush per output-size class, largest first.  Merging classes into
+    // fewer, larger flushes measured slower (config-4 mix: 6.02 ms per batch
+    // with one flush per class, 6.16 with at least 512 products per flush, 6.97
+    // with one flush): the GPU starts later and the small-transform launches gain
+    // little from being larger.
     for (size_t k = 0; k < order.size();) {
       BatchRec rec(*this);
       const int c = cls(order[k]);
@@ -465,12 +479,14 @@ void Engine::batch(fpx_job* jobs, size_t count) {
     size_t la, n;
     uint32_t* out;
     uint32_t *cs, *h;
+    size_t start = 32;  // terms present when the lockstep loop takes the job over
   };
   struct ExpT {
     size_t i;
     size_t lap, csize;
     uint32_t *ap, *c, *bs, *cs, *h, *t1, *t2;
     const uint32_t* tab;
+    size_t start;  // terms of b present when the lockstep loop takes the job over
   };
   struct LogT {
     size_t i, ld;
@@ -547,8 +563,14 @@ void Engine::batch(fpx_job* jobs, size_t count) {
                                     crt_aux(), j.p});
       } else if (route[i] == kInv) {
         InvT t{j.p, j.a, cnt, n, j.out, take(2 * n), take(n)};
+        if (cont[i]) {  // c[0, 2^13) by the fused kernel, the lockstep loop from there
+          t.start = fused_terms();
+          if (nat) fused.push_back(NewtonJob{0, &prime_plan(j.p).t, j.a, cnt, nullptr, j.out, nullptr, fused_terms()});
+          else fused.push_back(NewtonJob{0, nullptr, j.a, cnt, nullptr, j.out, nullptr, fused_terms(), crt_aux(), j.p});
+        } else {
+          seeds1.push_back(SeedJob{0, j.p, j.a, cnt, j.out, (int)std::min<size_t>(n, 32), 0});
+        }
         invs.push_back(t);
-        seeds1.push_back(SeedJob{0, j.p, j.a, cnt, j.out, (int)std::min<size_t>(n, 32), 0});
       } else if (route[i] == kLog) {
         if (cnt <= 1 || n == 1) {  // log = 0
           ExpPrep e{j.p, j.a, 0, nullptr, j.out, n};
@@ -578,8 +600,16 @@ void Engine::batch(fpx_job* jobs, size_t count) {
         e.h = take(n);
         e.t1 = take(n);
         e.t2 = take(n);
+        e.start = 32;
         preps.push_back(ExpPrep{j.p, j.a, cnt, e.ap, j.out, n});
-        if (e.lap && n > 1) {
+        if (e.lap && n > 1 && cont[i]) {
+          // b[0, 2^13) and c = 1/b to 2^12 terms by the fused kernel
+          e.tab = inv_table(j.p, n - 1);
+          e.start = fused_terms();
+          e.csize = fused_terms() / 2;
+          if (nat) fused.push_back(NewtonJob{1, &prime_plan(j.p).t, e.ap, e.lap, e.tab, j.out, e.c, fused_terms()});
+          else fused.push_back(NewtonJob{1, nullptr, e.ap, e.lap, e.tab, j.out, e.c, fused_terms(), crt_aux(), j.p});
+        } else if (e.lap && n > 1) {
           e.tab = inv_table(j.p, n - 1);
           seeds1.push_back(SeedJob{1, j.p, e.ap, e.lap, j.out, (int)std::min<size_t>(n, 32), 0});
           if (n > 32) seeds2.push_back(SeedJob{0, j.p, j.out, 32, e.c, 16, 0});
@@ -653,14 +683,23 @@ void Engine::batch(fpx_job* jobs, size_t count) {
     }
 
     // ---- lockstep doubling
-    for (size_t m = 32;; m <<= 1) {
+    // jobs continued from the fused kernels need their first 2^13 terms
+    bool any_cont = false;
+    for (const InvT& t : invs) any_cont |= t.start > 32;
+    for (const ExpT& e : exps) any_cont |= e.start > 32;
+    if (any_cont) side_join.join();
+    size_t m_end = 0;  // the loop runs until the longest job is complete
+    for (const InvT& t : invs) m_end = std::max(m_end, t.n);
+    for (const ExpT& e : exps)
+      if (e.lap) m_end = std::max(m_end, jobs[e.i].n);
+    for (size_t m = 32; m < m_end; m <<= 1) {
       std::vector<ExtJob> ext;
       for (const InvT& t : invs)
-        if (m < t.n) ext.push_back(ExtJob{t.p, t.a, t.la, t.out, m, std::min(2 * m, t.n), t.cs, t.h});
+        if (m < t.n && m >= t.start) ext.push_back(ExtJob{t.p, t.a, t.la, t.out, m, std::min(2 * m, t.n), t.cs, t.h});
       std::vector<ExpT*> act;
       for (ExpT& e : exps) {
         const fpx_job& j = jobs[e.i];
-        if (!e.lap || m >= j.n) continue;
+        if (!e.lap || m >= j.n || m < e.start) continue;
         act.push_back(&e);
         const size_t hlen = std::min(2 * m, j.n) - m;
         if (e.csize < hlen) {  // exponential.hpp:158-163: extend the inverse of b
@@ -668,7 +707,7 @@ void Engine::batch(fpx_job* jobs, size_t count) {
           e.csize = hlen;
         }
       }
-      if (ext.empty() && act.empty()) break;
+      if (ext.empty() && act.empty()) continue;
       if (!ext.empty()) {
         BatchRec r1(*this);
         for (const ExtJob& x : ext) ext_phase1(r1, x);
