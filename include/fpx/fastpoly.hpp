@@ -42,33 +42,45 @@ namespace fpx {
 
 // ------------------------------------------------------------------ field
 
+namespace detail {
+// x^e mod m for 64-bit intermediates (compile-time friendly).
+constexpr uint64_t pow_mod(uint64_t x, uint64_t e, uint64_t m) {
+  uint64_t r = 1 % m;
+  x %= m;
+  while (e) {
+    if (e & 1) r = r * x % m;
+    x = x * x % m;
+    e >>= 1;
+  }
+  return r;
+}
+}  // namespace detail
+
+/// a^-1 mod 2^32 for odd a: a is its own inverse to 3 bits, and each Newton
+/// step x <- x (2 - a x) doubles the correct bits (3, 6, 12, 24, 48).
 constexpr uint32_t inv_mod_2_32(uint32_t a) {
-  uint32_t x = 1;
-  for (int i = 0; i < 5; ++i) x *= 2u - a * x;
+  uint32_t x = a;
+  for (int bits = 3; bits < 32; bits *= 2) x *= 2u - a * x;
   return x;
 }
 
+/// The smallest primitive root of the prime p: the first g whose powers
+/// g^((p-1)/q) avoid 1 for every prime q dividing p - 1.
 constexpr uint32_t primitive_root(uint32_t p) {
   if (p == 2) return 1;
-  std::array<uint32_t, 10> f{};
-  size_t nf = 0;
-  uint32_t rem = p - 1;
-  for (uint32_t d = 2; uint64_t(d) * d <= rem; ++d) {
-    if (rem % d) continue;
-    f[nf++] = d;
-    while (rem % d == 0) rem /= d;
+  std::array<uint32_t, 10> q{};  // distinct prime factors of p - 1 (at most 9 below 2^31)
+  size_t nq = 0;
+  uint32_t r = p - 1;
+  for (uint32_t d = 2; uint64_t(d) * d <= r; d += (d == 2 ? 1 : 2)) {
+    if (r % d) continue;
+    q[nq++] = d;
+    while (r % d == 0) r /= d;
   }
-  if (rem > 1) f[nf++] = rem;
-  auto pw = [p](uint64_t a, uint32_t e) {
-    uint64_t r = 1;
-    for (; e; e >>= 1, a = a * a % p)
-      if (e & 1) r = r * a % p;
-    return r;
-  };
+  if (r > 1) q[nq++] = r;
   for (uint32_t g = 2; g < p; ++g) {
-    bool ok = true;
-    for (size_t i = 0; i < nf && ok; ++i) ok = pw(g, (p - 1) / f[i]) != 1;
-    if (ok) return g;
+    size_t k = 0;
+    while (k < nq && detail::pow_mod(g, (p - 1) / q[k], p) != 1) ++k;
+    if (k == nq) return g;
   }
   return 0;
 }
@@ -81,33 +93,36 @@ class Mont {
   static_assert(Mod < (1u << 31) && Mod >= 2, "modulus must be a prime in [2, 2^31)");
   static constexpr uint32_t mod = Mod;
   static constexpr uint32_t primitive_root = Root != 0 ? Root : fpx::primitive_root(Mod);
-  static constexpr uint32_t ninv = static_cast<uint32_t>(0u - inv_mod_2_32(Mod | 1u));
+  // -Mod^-1 mod 2^32 (0 for Mod = 2, whose limbs are the bits themselves)
+  static constexpr uint32_t ninv = Mod == 2 ? 0u : static_cast<uint32_t>(0u - inv_mod_2_32(Mod));
   static constexpr uint32_t one = Mod == 2 ? 1u : static_cast<uint32_t>((uint64_t(1) << 32) % Mod);
   static constexpr uint32_t r2 = static_cast<uint32_t>(uint64_t(one) * one % Mod);
   static constexpr uint32_t inv2 = (Mod + 1) / 2;
 
   constexpr Mont() : v_(0) {}
   template <class I, class = std::enable_if_t<std::is_integral_v<I> && !std::is_same_v<I, bool>>>
-  constexpr Mont(I x) : v_(enter(static_cast<uint64_t>(x))) {}
+  constexpr Mont(I x) : v_(to_limb(static_cast<uint64_t>(x))) {}
 
-  static constexpr Mont from_int(uint64_t x) { return wrap(enter(x)); }
-  static constexpr Mont raw(uint32_t x) { return wrap(x); }
+  static constexpr Mont from_int(uint64_t x) { return of_limb(to_limb(x)); }
+  static constexpr Mont raw(uint32_t x) { return of_limb(x); }
+  /// t * 2^-32 mod Mod for t < Mod * 2^32 (Montgomery reduction), canonical.
   static constexpr uint32_t reduce(uint64_t t) {
-    if constexpr (Mod == 2) return static_cast<uint32_t>(t & 1u);
-    const uint32_t m = static_cast<uint32_t>(t) * ninv;
-    const uint64_t u = (t + uint64_t(m) * Mod) >> 32;
-    return static_cast<uint32_t>(u >= Mod ? u - Mod : u);
+    if constexpr (Mod == 2) {
+      return static_cast<uint32_t>(t & 1u);
+    } else {
+      // t + m Mod is divisible by 2^32 for m = (t mod 2^32) (-Mod^-1)
+      const uint64_t m = static_cast<uint32_t>(static_cast<uint32_t>(t) * ninv);
+      const uint64_t u = (t >> 32) + ((static_cast<uint64_t>(static_cast<uint32_t>(t)) + m * Mod) >> 32);
+      return canon(u);
+    }
   }
   constexpr uint32_t val() const { return reduce(v_); }
   constexpr uint32_t raw_val() const { return v_; }
 
-  friend constexpr Mont operator+(Mont a, Mont b) {
-    const uint32_t s = a.v_ + b.v_;
-    return wrap(s >= Mod ? s - Mod : s);
-  }
-  friend constexpr Mont operator-(Mont a, Mont b) { return wrap(a.v_ >= b.v_ ? a.v_ - b.v_ : a.v_ - b.v_ + Mod); }
-  friend constexpr Mont operator-(Mont a) { return wrap(a.v_ == 0 ? 0 : Mod - a.v_); }
-  friend constexpr Mont operator*(Mont a, Mont b) { return wrap(reduce(uint64_t(a.v_) * b.v_)); }
+  friend constexpr Mont operator+(Mont a, Mont b) { return of_limb(canon(uint64_t(a.v_) + b.v_)); }
+  friend constexpr Mont operator-(Mont a, Mont b) { return of_limb(canon(uint64_t(a.v_) + Mod - b.v_)); }
+  friend constexpr Mont operator-(Mont a) { return Mont() - a; }
+  friend constexpr Mont operator*(Mont a, Mont b) { return of_limb(reduce(uint64_t(a.v_) * b.v_)); }
   friend constexpr Mont operator/(Mont a, Mont b) { return a * b.inv(); }
   constexpr Mont& operator+=(Mont b) { return *this = *this + b; }
   constexpr Mont& operator-=(Mont b) { return *this = *this - b; }
@@ -119,49 +134,60 @@ class Mont {
   constexpr bool operator!() const { return v_ == 0; }
   constexpr explicit operator bool() const { return v_ != 0; }
 
+  /// this^e, scanning the exponent from its top bit down.
   constexpr Mont pow(uint64_t e) const {
-    Mont r = from_int(1), b = *this;
-    for (; e; e >>= 1) {
-      if (e & 1) r *= b;
-      b *= b;
+    Mont r = from_int(1);
+    for (int bit = 63; bit >= 0; --bit) {
+      r *= r;
+      if ((e >> bit) & 1) r *= *this;
     }
     return r;
   }
+  /// Multiplicative inverse by Fermat (0 maps to 0).
   constexpr Mont inv() const {
     if constexpr (Mod == 2) return *this;
     else return pow(Mod - 2);
   }
-  /// Tonelli-Shanks with the reference's root choice (z searched upward from 2).
+  /// A square root, the one Tonelli-Shanks gives with the non-residue z found
+  /// by counting up from 2 (the reference's choice, which fixes poly::sqrt's
+  /// result); false for a non-residue.  For Mod = 3 mod 4 this is
+  /// this^((Mod+1)/4), the case s = 1 below.
   bool sqrt(Mont& out) const {
-    if constexpr (Mod == 2) { out = *this; return true; }
-    const Mont o = from_int(1);
-    if (v_ == 0) { out = *this; return true; }
-    if (pow((Mod - 1) / 2) != o) return false;
-    if (Mod % 4 == 3) { out = pow((uint64_t(Mod) + 1) / 4); return true; }
-    uint64_t q = Mod - 1;
-    int s = 0;
-    while (q % 2 == 0) { q /= 2; ++s; }
-    Mont z = from_int(2);
-    while (z.pow((Mod - 1) / 2) != -o) z += o;
-    Mont c = z.pow(q), x = pow((q + 1) / 2), t = pow(q);
-    int m = s;
-    while (t != o) {
-      int i = 0;
-      for (Mont t2 = t; t2 != o; t2 *= t2) ++i;
-      const Mont b = c.pow(uint64_t(1) << (m - i - 1));
-      x *= b;
-      c = b * b;
-      t *= c;
-      m = i;
+    if constexpr (Mod == 2) {
+      out = *this;
+      return true;
+    } else {
+      const Mont unit = from_int(1);
+      if (is_zero()) {
+        out = *this;
+        return true;
+      }
+      if (pow((Mod - 1) / 2) != unit) return false;  // Euler's criterion
+      int s = std::countr_zero(Mod - 1);             // Mod - 1 = q 2^s, q odd
+      const uint64_t q = (Mod - 1) >> s;
+      Mont z = from_int(2);
+      while (z.pow((Mod - 1) / 2) == unit) z += unit;  // the first non-residue
+      Mont c = z.pow(q), t = pow(q), root = pow((q + 1) / 2);
+      while (t != unit) {
+        int i = 1;  // least i with t^(2^i) = 1
+        for (Mont sq = t * t; sq != unit; sq *= sq) ++i;
+        Mont b = c;
+        for (int k = 0; k < s - i - 1; ++k) b *= b;
+        root *= b;
+        c = b * b;
+        t *= c;
+        s = i;
+      }
+      out = root;
+      return true;
     }
-    out = x;
-    return true;
   }
   std::string str() const { return std::to_string(val()); }
 
  private:
-  static constexpr uint32_t enter(uint64_t x) { return static_cast<uint32_t>(x % Mod) * uint64_t(one) % Mod; }
-  static constexpr Mont wrap(uint32_t v) {
+  static constexpr uint32_t canon(uint64_t x) { return static_cast<uint32_t>(x >= Mod ? x - Mod : x); }
+  static constexpr uint32_t to_limb(uint64_t x) { return static_cast<uint32_t>(x % Mod * uint64_t(one) % Mod); }
+  static constexpr Mont of_limb(uint32_t v) {
     Mont m;
     m.v_ = v;
     return m;
