@@ -161,7 +161,11 @@ class ServeStats(C.Structure):
     """struct fpx_serve_stats."""
     _fields_ = [("submitted", C.c_uint64), ("completed", C.c_uint64), ("batches", C.c_uint64),
                 ("max_batch_jobs_seen", C.c_uint64), ("max_batch_bytes_seen", C.c_uint64),
-                ("oversize_requests", C.c_uint64), ("max_in_flight_bytes", C.c_uint64)]
+                ("oversize_requests", C.c_uint64), ("max_in_flight_bytes", C.c_uint64),
+                ("device_pool_bytes", C.c_uint64), ("device_allocations", C.c_uint64),
+                ("pool_flushes", C.c_uint64), ("device_alloc_ns", C.c_uint64),
+                ("device_alloc_ns_max", C.c_uint64), ("host_allocs", C.c_uint64),
+                ("host_alloc_ns", C.c_uint64), ("host_alloc_ns_max", C.c_uint64)]
 
 
 def make_job(spec, keep: list) -> tuple:

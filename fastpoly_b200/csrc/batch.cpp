@@ -236,6 +236,7 @@ Engine::Stage& Engine::stage(size_t bytes) {
   if (!s.ev) check(cudaEventCreateWithFlags(&s.ev, cudaEventDisableTiming), "cudaEventCreate");
   else check(cudaEventSynchronize(s.ev), "staging wait");  // the slot's previous copy has left
   if (bytes > s.cap) {
+    const auto t0 = std::chrono::steady_clock::now();
     const size_t cap = std::max<size_t>(bytes + bytes / 2, size_t(1) << 16);
     if (s.host) cudaFreeHost(s.host);
     s.host = nullptr;
@@ -243,6 +244,7 @@ Engine::Stage& Engine::stage(size_t bytes) {
     check(cudaMallocHost(&s.host, cap), "cudaMallocHost");
     s.dev = Buf(&pool_, cap / 4 + 1);
     s.cap = cap;
+    count_host_alloc(t0);
   }
   return s;
 }
@@ -1079,7 +1081,9 @@ class CopyPool {
 uint32_t* Engine::pin_slot(int k) {
   Pin& q = pins_[k];
   if (!q.host) {
+    const auto t0 = std::chrono::steady_clock::now();
     check(cudaMallocHost(&q.host, kPinWords * 4), "cudaMallocHost");
+    count_host_alloc(t0);
     check(cudaEventCreateWithFlags(&q.ev, cudaEventDisableTiming), "cudaEventCreate");
   } else {
     check(cudaEventSynchronize(q.ev), "staging wait");

@@ -9,6 +9,7 @@
 #include "engine.h"
 
 #include <algorithm>
+#include <chrono>
 #include <bit>
 #include <cstdlib>
 #include <cstring>
@@ -179,6 +180,25 @@ uint32_t* Pool::get(size_t words, size_t* cls_out) {
       if (capturing_) cap_owned_[static_cast<uint32_t*>(p)] = cls;
       return static_cast<uint32_t*>(p);
     }
+    // A large class with nothing cached takes the smallest cached block of up
+    // to four times its size: a batch's arena is sized by the sum of its jobs'
+    // scratch, so batches of new shapes keep asking for classes not seen yet,
+    // and a cudaMalloc of several GB holds the caller (and the driver's
+    // allocation lock) for up to ~100 ms.
+    if (cls >= kFitBytes) {
+      for (auto ft = free_.upper_bound(cls); ft != free_.end() && ft->first <= 4 * cls; ++ft) {
+        if (ft->second.empty() || (limit_ && in_use_bytes + ft->first > limit_)) continue;
+        void* p = ft->second.back();
+        ft->second.pop_back();
+        cached_bytes -= ft->first;
+        --cached_blocks;
+        ++cache_hits;
+        in_use_bytes += ft->first;
+        *cls_out = ft->first;
+        if (capturing_) cap_owned_[static_cast<uint32_t*>(p)] = ft->first;
+        return static_cast<uint32_t*>(p);
+      }
+    }
     // The limit is checked and the block's bytes reserved under the lock, so
     // concurrent callers of one pool cannot together pass the limit.
     if (limit_ && in_use_bytes + cls > limit_)
@@ -196,6 +216,7 @@ uint32_t* Pool::get(size_t words, size_t* cls_out) {
   }
   if (trim) release();
   void* p = nullptr;
+  const auto t0 = std::chrono::steady_clock::now();
   cudaError_t e = cudaMalloc(&p, cls);
   if (e != cudaSuccess) {
     cudaGetLastError();
@@ -207,8 +228,12 @@ uint32_t* Pool::get(size_t words, size_t* cls_out) {
       throw Error{FPX_ENOMEM, "cudaMalloc of " + std::to_string(cls) + " bytes failed"};
     }
   }
+  const uint64_t ns = static_cast<uint64_t>(
+      std::chrono::duration_cast<std::chrono::nanoseconds>(std::chrono::steady_clock::now() - t0).count());
   std::lock_guard<std::mutex> g(mu_);
   ++system_allocations;
+  alloc_ns += ns;
+  alloc_ns_max = std::max(alloc_ns_max, ns);
   *cls_out = cls;
   if (capturing_) cap_owned_[static_cast<uint32_t*>(p)] = cls;
   return static_cast<uint32_t*>(p);
@@ -252,8 +277,14 @@ void Pool::give_back(const std::vector<std::pair<uint32_t*, size_t>>& blocks) {
   }
 }
 
+Pool::Snapshot Pool::snapshot() {
+  std::lock_guard<std::mutex> g(mu_);
+  return {cached_bytes, in_use_bytes, system_allocations, flushes, alloc_ns, alloc_ns_max};
+}
+
 void Pool::release() {
   std::lock_guard<std::mutex> g(mu_);
+  if (cached_blocks) ++flushes;
   for (auto& [cls, v] : free_)
     for (void* p : v) cudaFree(p);
   free_.clear();

@@ -6,6 +6,8 @@
 // (include/fastpoly/detail/poly/*.hpp) with its transforms replaced by the
 // fused GPU passes of kernels.cu.
 #pragma once
+#include <atomic>
+#include <chrono>
 #include <cstdint>
 #include <functional>
 #include <map>
@@ -37,6 +39,12 @@ class Pool {
   uint32_t* get(size_t words, size_t* cls_out);
   void put(uint32_t* p, size_t cls);
   void release();
+  // Cached, in-use and lifetime counters read together under the pool's lock.
+  struct Snapshot {
+    size_t cached_bytes, in_use_bytes, system_allocations, flushes;
+    uint64_t alloc_ns, alloc_ns_max;
+  };
+  Snapshot snapshot();
   // Graph capture: between begin_capture and end_capture every block handed
   // out is owned by the graph being captured; released ones are recycled only
   // within the capture (stream order inside the graph), and end_capture hands
@@ -46,7 +54,11 @@ class Pool {
   std::vector<std::pair<uint32_t*, size_t>> end_capture();
   void give_back(const std::vector<std::pair<uint32_t*, size_t>>& blocks);
   size_t cached_bytes = 0, cached_blocks = 0, in_use_bytes = 0, system_allocations = 0, cache_hits = 0;
+  size_t flushes = 0;  // release() calls that returned cached blocks to the device
+  uint64_t alloc_ns = 0, alloc_ns_max = 0;  // host time in cudaMalloc: total and longest call
   size_t limit_ = 0;
+  // Classes from this size up may be served by a cached block of a larger class.
+  static constexpr size_t kFitBytes = size_t(64) << 20;
 
  private:
   std::map<size_t, std::vector<void*>> free_;
@@ -321,6 +333,16 @@ class Engine {
     a.second += ms;
   }
   bool profiling() const { return prof_on_; }
+  // Pinned host allocations of the staging buffers (count, host time: total
+  // and longest); written by the thread that drives the engine.
+  std::atomic<uint64_t> host_allocs{0}, host_alloc_ns{0}, host_alloc_ns_max{0};
+  void count_host_alloc(std::chrono::steady_clock::time_point t0) {
+    const uint64_t ns = static_cast<uint64_t>(
+        std::chrono::duration_cast<std::chrono::nanoseconds>(std::chrono::steady_clock::now() - t0).count());
+    host_allocs.fetch_add(1, std::memory_order_relaxed);
+    host_alloc_ns.fetch_add(ns, std::memory_order_relaxed);
+    if (ns > host_alloc_ns_max.load(std::memory_order_relaxed)) host_alloc_ns_max.store(ns, std::memory_order_relaxed);
+  }
  private:
   cudaEvent_t prof_open_ = nullptr;
   std::vector<ProfRec> prof_recs_;

@@ -284,8 +284,24 @@ int fpx_serve_poll(fpx_server* srv, uint64_t ticket, int wait, uint64_t* latency
 
 int fpx_serve_stats_get(fpx_server* srv, fpx_serve_stats* out) {
   if (!srv || !out) return FPX_EINVAL;
-  std::lock_guard<std::mutex> g(srv->mu);
-  *out = srv->stats;
+  {
+    std::lock_guard<std::mutex> g(srv->mu);
+    *out = srv->stats;
+  }
+  out->device_pool_bytes = out->device_allocations = out->pool_flushes = 0;
+  out->device_alloc_ns = out->device_alloc_ns_max = 0;
+  out->host_allocs = out->host_alloc_ns = out->host_alloc_ns_max = 0;
+  for (auto& e : srv->engines) {
+    const fpx::Pool::Snapshot p = e->pool().snapshot();
+    out->device_pool_bytes += p.cached_bytes + p.in_use_bytes;
+    out->device_allocations += p.system_allocations;
+    out->pool_flushes += p.flushes;
+    out->device_alloc_ns += p.alloc_ns;
+    out->device_alloc_ns_max = std::max<uint64_t>(out->device_alloc_ns_max, p.alloc_ns_max);
+    out->host_allocs += e->host_allocs.load();
+    out->host_alloc_ns += e->host_alloc_ns.load();
+    out->host_alloc_ns_max = std::max<uint64_t>(out->host_alloc_ns_max, e->host_alloc_ns_max.load());
+  }
   return FPX_OK;
 }
 

@@ -231,6 +231,14 @@ typedef struct fpx_serve_stats {
   uint64_t max_batch_bytes_seen;    /* largest planned device bytes admitted in one micro-batch */
   uint64_t oversize_requests;       /* requests that alone exceeded the budget (ran alone) */
   uint64_t max_in_flight_bytes;     /* largest planned device bytes of all micro-batches on the GPU at once */
+  uint64_t device_pool_bytes;       /* device bytes the workers' scratch pools hold now (cached + in use) */
+  uint64_t device_allocations;      /* cudaMalloc calls made by the workers' pools so far */
+  uint64_t pool_flushes;            /* times a worker's pool returned its cache to the device (a failed cudaMalloc) */
+  uint64_t device_alloc_ns;         /* host time the workers spent in those cudaMalloc calls */
+  uint64_t device_alloc_ns_max;     /* the longest of them */
+  uint64_t host_allocs;             /* pinned host allocations of the workers' staging buffers */
+  uint64_t host_alloc_ns;           /* host time spent in them (frees of the buffers they replace included) */
+  uint64_t host_alloc_ns_max;       /* the longest of them */
 } fpx_serve_stats;
 
 typedef struct fpx_server fpx_server;

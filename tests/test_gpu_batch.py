@@ -249,3 +249,46 @@ def test_batch_more_cluster_jobs_than_one_launch(fpx, oracle):
         assert not isinstance(got[i], Exception), (i, got[i])
         if not np.array_equal(got[i], want[i % 16]):
             raise AssertionError(f"job {i} differs")
+
+
+def test_batch_smaller_arena_takes_cached_block(oracle):
+    """A batch whose scratch arena falls in a smaller size class than any cached
+    block takes a cached block of up to four times its size instead of a new
+    device allocation, with the same results."""
+    import torch
+    ctx = F.Context(0)
+    try:
+        p, n = 998244353, 1 << 19
+        rng = np.random.default_rng(66)
+        count = 64
+
+        def jobs_of(bufs):
+            jobs = (F.Job * len(bufs))()
+            for j, (da, db, do) in zip(jobs, bufs):
+                j.op, j.p, j.a, j.la, j.b, j.lb = F.OP_CONV, p, da.data_ptr(), da.numel(), db.data_ptr(), db.numel()
+                j.n, j.out = F.SIZE_MAX, do.data_ptr()
+            return jobs
+
+        def run(jobs):
+            assert ctx.batch_submit(jobs) == F.OK
+            ctx.batch_wait()
+
+        host = [(rnd(rng, p, n), rnd(rng, p, n)) for _ in range(count)]
+        big = [(torch.from_numpy(a.view(np.int32)).cuda(), torch.from_numpy(b.view(np.int32)).cuda(),
+                torch.empty(2 * n - 1, dtype=torch.int32, device="cuda")) for a, b in host]
+        tiny = [(x[:100], y[:100], o[:199]) for x, y, o in big]
+        for _ in range(6):  # descriptor ring slots sized for `count` jobs
+            run(jobs_of(tiny))
+        run(jobs_of(big))
+        first = [o.clone() for _, _, o in big]
+        for _, _, o in big:
+            o.zero_()
+        before = ctx.pool_stats()["system_allocations"]
+        run(jobs_of(big[: count // 3]))
+        assert ctx.pool_stats()["system_allocations"] == before
+        for i in range(count // 3):
+            assert torch.equal(big[i][2], first[i]), i
+        for i in (0, count // 3 - 1):
+            eq(first[i].cpu().numpy().view(np.uint32), oracle.conv(p, *host[i]), f"job {i}")
+    finally:
+        ctx.close()
