@@ -15,7 +15,9 @@ exceptions: ``DomainError`` (fpx::poly::domain_error), ``NttSizeError``
 from __future__ import annotations
 
 import ctypes as C
+import mmap
 import os
+import sys
 
 import numpy as np
 
@@ -283,6 +285,10 @@ def _dptr(t) -> int:
     return t if isinstance(t, int) else t.data_ptr()
 
 
+# Batch output buffers of at least this many words are reused across calls.
+_OUT_KEEP_WORDS = 1 << 20
+
+
 class Context:
     """One device, one stream, one device-memory pool and plan cache (fpx_ctx)."""
 
@@ -294,6 +300,7 @@ class Context:
             raise FpxError(rc, f"fpx_ctx_create(device={device}) failed")
         self._h = h
         self.device = device
+        self._outbufs = []  # batch output buffers kept for reuse (at most two)
 
     # -- plumbing --------------------------------------------------------------
     def close(self):
@@ -556,7 +563,7 @@ class Context:
         if m:
             np.cumsum((cap1 + cap2)[:-1], out=off1[1:])
         off2 = off1 + cap1
-        out = np.empty(max(int((cap1 + cap2).sum()), 1), np.uint32)
+        out = self._out_buffer(max(int((cap1 + cap2).sum()), 1))
         base = np.uint64(out.__array_interface__["data"][0])
         arr = np.zeros(max(m, 1), dtype=_JOB_DTYPE)
         v = arr[:m]
@@ -579,6 +586,32 @@ class Context:
             else:
                 res.append(out[o1s[i]: o1s[i] + ol[i]])
         return res
+
+    def _out_buffer(self, words: int) -> np.ndarray:
+        """Output buffer of a batch.  Large ones are kept and handed out again once
+        no result of the call that had them is referenced any more: a fresh buffer
+        costs a page fault per 4 KiB page on first write (several ms for the
+        hundreds of MB a large batch returns), and is mapped with transparent huge
+        pages requested."""
+        if words < _OUT_KEEP_WORDS:
+            return np.empty(words, np.uint32)
+        for b in self._outbufs:
+            # references: the list, the loop variable, the argument (a result view adds one)
+            if b.size >= words and sys.getrefcount(b) == 3:
+                return b[:words]
+        m = mmap.mmap(-1, words * 4)
+        if hasattr(m, "madvise") and hasattr(mmap, "MADV_HUGEPAGE"):
+            try:
+                m.madvise(mmap.MADV_HUGEPAGE)
+            except OSError:
+                pass
+        buf = np.frombuffer(m, np.uint32)
+        free = [i for i, b in enumerate(self._outbufs) if sys.getrefcount(b) == 3]
+        if len(self._outbufs) < 2:
+            self._outbufs.append(buf)
+        elif free:
+            self._outbufs[free[0]] = buf
+        return buf
 
     def batch_submit(self, jobs) -> int:
         """fpx_batch_submit on a ctypes array of Job with device pointers; returns the call's status

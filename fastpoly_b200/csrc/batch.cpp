@@ -1030,9 +1030,15 @@ class CopyPool {
 
  private:
   static constexpr size_t kParallelBytes = size_t(2) << 20;
+  // Threads per copy (the caller and the pool's): FPX_COPY_THREADS, else half
+  // the hardware threads, at most 8.
   CopyPool() {
     const unsigned hw = std::thread::hardware_concurrency();
-    const int extra = (int)std::min(7u, hw > 2 ? hw / 2 - 1 : 0u);
+    int extra = (int)std::min(7u, hw > 2 ? hw / 2 - 1 : 0u);
+    if (const char* e = std::getenv("FPX_COPY_THREADS")) {
+      const int n = std::atoi(e);
+      if (n >= 1) extra = std::min(n, 64) - 1;
+    }
     for (int i = 1; i <= extra; ++i) threads_.emplace_back([this, i] { loop(i); });
   }
   // Bytes [lo, hi) of the concatenated pieces.

@@ -54,24 +54,54 @@ def test_null_context_rejected():
     assert lib.fpx_conv(None, 998244353, None, 0, None, 0, 0, None, None, 0) == F.EINVAL
 
 
-def test_job_struct_layout_matches_header(tmp_path):
-    """fastpoly_b200.Job (ctypes) has the layout of struct fpx_job in include/fpx_b200.h."""
+@pytest.mark.parametrize("cls,ctype", [("Job", "fpx_job"), ("ServeConfig", "fpx_serve_config"),
+                                       ("ServeStats", "fpx_serve_stats"), ("PoolStats", "fpx_pool_stats_t"),
+                                       ("ColShape", "fpx_col_shape")])
+def test_struct_layout_matches_header(tmp_path, cls, ctype):
+    """Each ctypes structure of fastpoly_b200 has the layout of its struct in include/fpx_b200.h."""
     import shutil
     import subprocess
     cc = shutil.which("gcc") or shutil.which("cc")
     if cc is None:
         pytest.skip("no C compiler")
-    fields = [f for f, _ in F.Job._fields_]
+    S = getattr(F, cls)
+    fields = [f for f, _ in S._fields_]
     src = tmp_path / "layout.c"
     src.write_text("#include <stdio.h>\n#include <stddef.h>\n#include \"fpx_b200.h\"\nint main(void) {\n"
-                   "  printf(\"%zu\\n\", sizeof(fpx_job));\n"
-                   + "".join(f"  printf(\"%zu\\n\", offsetof(fpx_job, {f}));\n" for f in fields)
+                   f"  printf(\"%zu\\n\", sizeof({ctype}));\n"
+                   + "".join(f"  printf(\"%zu\\n\", offsetof({ctype}, {f}));\n" for f in fields)
                    + "  return 0;\n}\n")
     exe = tmp_path / "layout"
     subprocess.run([cc, "-I" + os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
     got = [int(x) for x in subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split()]
-    assert got[0] == ctypes.sizeof(F.Job)
-    assert got[1:] == [getattr(F.Job, f).offset for f in fields]
+    assert got[0] == ctypes.sizeof(S)
+    assert got[1:] == [getattr(S, f).offset for f in fields]
+
+
+def test_batch_output_buffer_reuse():
+    """Context.batch hands a large output buffer out again only once no result
+    view of the call that had it is alive."""
+    import numpy as np
+    ctx = F.Context.__new__(F.Context)  # the buffer logic needs no device
+    ctx._outbufs = []
+    words = 3 << 20
+    first = ctx._out_buffer(words)
+    result = first[5:10]
+    result[:] = 7
+    del first
+    second = ctx._out_buffer(words)
+    assert not np.shares_memory(second, result), "a buffer with a live result was handed out again"
+    assert (result == 7).all()
+    addr = second.__array_interface__["data"][0]
+    del second
+    third = ctx._out_buffer(words - 100)
+    assert third.__array_interface__["data"][0] == addr
+    del third
+    larger = ctx._out_buffer(2 * words)  # fits no kept buffer: a new one
+    assert larger.size == 2 * words and not np.shares_memory(larger, result)
+    assert len(ctx._outbufs) <= 2
+    small = ctx._out_buffer(100)
+    assert small.size == 100 and all(b.size >= F._OUT_KEEP_WORDS for b in ctx._outbufs)
 
 
 def test_batch_rejects_null_context():
