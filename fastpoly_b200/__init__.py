@@ -276,6 +276,22 @@ def _arr(a) -> np.ndarray:
     return np.ascontiguousarray(np.asarray(a, dtype=np.uint32))
 
 
+_JOBS_EXT = None
+
+
+def _jobs_ext():
+    """The C helper that fills batch job records (fastpoly_b200/_fpx_jobs, built
+    with the library)."""
+    global _JOBS_EXT
+    if _JOBS_EXT is None:
+        try:
+            from . import _fpx_jobs
+        except ImportError as e:
+            raise ImportError("fastpoly_b200/_fpx_jobs is not built: run python -m fastpoly_b200.build") from e
+        _JOBS_EXT = _fpx_jobs
+    return _JOBS_EXT
+
+
 def _ptr(a: np.ndarray):
     return a.ctypes.data_as(_u32p) if a.size else None
 
@@ -498,85 +514,25 @@ class Context:
         exception the single-job call would raise for that job (not raised).
         """
         m = len(jobs)
-        keep = []
-        op, pp, ca, cla, cb, clb, ck, cn, cap1, cap2 = ([] for _ in range(10))
-        u32 = np.uint32
-        conv_op, pow_op, div_op = OP_CONV, OP_POW, OP_DIVMOD
-        cfb, addr = C.c_char.from_buffer, C.addressof
-
-        def ptr(x):  # a third of the cost of __array_interface__ (read-only arrays fall back)
-            try:
-                return addr(cfb(x))
-            except TypeError:
-                return x.__array_interface__["data"][0]
-
-        for jb in jobs:
-            o = _OPS[jb[0]]
-            op.append(o)
-            pp.append(jb[1])
-            a = jb[2]
-            if not (type(a) is np.ndarray and a.dtype == u32 and a.flags.c_contiguous):
-                a = _arr(a)
-                keep.append(a)
-            na = a.size
-            cla.append(na)
-            ca.append(ptr(a) if na else 0)
-            nb = 0
-            if o == conv_op or o == div_op:
-                bb = jb[3]
-                if not (type(bb) is np.ndarray and bb.dtype == u32 and bb.flags.c_contiguous):
-                    bb = _arr(bb)
-                    keep.append(bb)
-                nb = bb.size
-                clb.append(nb)
-                cb.append(ptr(bb) if nb else 0)
-            else:
-                clb.append(0)
-                cb.append(0)
-            if o == conv_op:
-                n = SIZE_MAX if len(jb) < 5 or jb[4] is None else int(jb[4])
-                cn.append(n)
-                ck.append(0)
-                cap = min(na, n) + min(nb, n) - 1 if na and nb and n else 0
-                cap1.append(max(min(cap, n), 1))
-                cap2.append(0)
-            elif o == pow_op:
-                ck.append(int(jb[3]))
-                cn.append(int(jb[4]))
-                cap1.append(max(int(jb[4]), 1))
-                cap2.append(0)
-            elif o == div_op:
-                ck.append(0)
-                cn.append(0)
-                cap1.append(max(na, 1))
-                cap2.append(max(nb, 1))
-            else:
-                ck.append(0)
-                cn.append(int(jb[3]))
-                cap1.append(max(int(jb[3]), 1))
-                cap2.append(0)
-        cols = {"a": ca, "la": cla, "b": cb, "lb": clb, "k": ck, "n": cn}
-        op = np.asarray(op, np.int32)
-        cap1 = np.asarray(cap1, np.int64)
-        cap2 = np.asarray(cap2, np.int64)
+        arr = np.zeros(max(m, 1), dtype=_JOB_DTYPE)
+        caps = np.empty(2 * max(m, 1), np.int64)
+        keep = _jobs_ext().fill(jobs, arr.ctypes.data, caps.ctypes.data, _OPS, _arr)
+        cap1, cap2 = caps[:m], caps[m: 2 * m]
         off1 = np.zeros(m, np.int64)
         if m:
             np.cumsum((cap1 + cap2)[:-1], out=off1[1:])
         off2 = off1 + cap1
         out = self._out_buffer(max(int((cap1 + cap2).sum()), 1))
         base = np.uint64(out.__array_interface__["data"][0])
-        arr = np.zeros(max(m, 1), dtype=_JOB_DTYPE)
         v = arr[:m]
-        v["op"], v["p"] = op, np.asarray(pp, np.uint32)
-        for f in ("a", "la", "b", "lb", "k", "n"):
-            v[f] = np.asarray(cols[f], np.uint64)
         v["out"] = base + np.uint64(4) * off1.astype(np.uint64)
         v["out2"] = np.where(cap2 > 0, base + np.uint64(4) * off2.astype(np.uint64), np.uint64(0))
         rc = self._L.fpx_batch_run(self._h, arr.ctypes.data, m, repr)
         if rc not in (OK, EDOMAIN, ESIZE, ELENGTH, EINVAL):
             self._check(rc, "batch")
+        del keep  # the converted inputs are no longer read
         st, ol, ol2 = v["status"].tolist(), v["out_len"].tolist(), v["out2_len"].tolist()
-        o1s, o2s, ops = off1.tolist(), off2.tolist(), op.tolist()
+        o1s, o2s, ops = off1.tolist(), off2.tolist(), v["op"].tolist()
         res = []
         for i in range(m):
             if st[i] != OK:

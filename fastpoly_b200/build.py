@@ -1,4 +1,5 @@
-"""Builds the in-tree CUDA library fastpoly_b200/libfpx_b200.so for sm_100a.
+"""Builds the in-tree CUDA library fastpoly_b200/libfpx_b200.so for sm_100a,
+and the CPython helper fastpoly_b200/_fpx_jobs (batch job records).
 
     python -m fastpoly_b200.build [--force]
 
@@ -12,6 +13,7 @@ import os
 import shutil
 import subprocess
 import sys
+import sysconfig
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
@@ -59,7 +61,25 @@ def _object_stale(src: str, obj: str, headers: list) -> bool:
     return os.path.getmtime(src) > t or any(os.path.getmtime(h) > t for h in headers if os.path.exists(h))
 
 
+PYJOBS_SRC = os.path.join(CSRC, "pyjobs.c")
+PYJOBS = os.path.join(HERE, "_fpx_jobs" + (sysconfig.get_config_var("EXT_SUFFIX") or ".so"))
+
+
+def build_pyjobs(force: bool = False, verbose: bool = False) -> str:
+    """The CPython extension that fills batch job records (plain C, no CUDA)."""
+    deps = [PYJOBS_SRC, os.path.join(INCLUDE, "fpx_b200.h")]
+    if not force and os.path.exists(PYJOBS) and all(os.path.getmtime(d) <= os.path.getmtime(PYJOBS) for d in deps):
+        return PYJOBS
+    cc = os.environ.get("CC", shutil.which("gcc") or "cc")
+    tmp = PYJOBS + ".tmp"
+    _run([cc, "-O2", "-fPIC", "-shared", "-Wall", "-I" + sysconfig.get_paths()["include"], "-I" + INCLUDE,
+          PYJOBS_SRC, "-o", tmp], verbose)
+    os.replace(tmp, PYJOBS)
+    return PYJOBS
+
+
 def build(force: bool = False, verbose: bool = False) -> str:
+    build_pyjobs(force, verbose)
     if not force and not _stale():
         return LIB
     os.makedirs(BUILD, exist_ok=True)

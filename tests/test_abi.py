@@ -125,3 +125,63 @@ def test_serve_plan_bytes_without_device():
     assert nb >= 4 * (2 * N) and nb < 4 * (6 * N)
     assert cb > 2.5 * nb
     assert lib.fpx_serve_plan_bytes(None) == 0
+
+
+def _records_in_python(jobs):
+    """The job records Context.batch builds, restated in Python: (op, p, la, lb,
+    k, n, cap1, cap2) per job."""
+    import numpy as np
+    rows = []
+    for jb in jobs:
+        op, p = F._OPS[jb[0]], int(jb[1])
+        na = np.asarray(jb[2]).size
+        nb = np.asarray(jb[3]).size if op in (F.OP_CONV, F.OP_DIVMOD) else 0
+        k, n, cap2 = 0, 0, 0
+        if op == F.OP_CONV:
+            n = F.SIZE_MAX if len(jb) < 5 or jb[4] is None else int(jb[4])
+            cap = min(na, n) + min(nb, n) - 1 if na and nb and n else 0
+            cap1 = max(min(cap, n), 1)
+        elif op == F.OP_POW:
+            k, n = int(jb[3]), int(jb[4])
+            cap1 = max(n, 1)
+        elif op == F.OP_DIVMOD:
+            cap1, cap2 = max(na, 1), max(nb, 1)
+        else:
+            n = int(jb[3])
+            cap1 = max(n, 1)
+        rows.append((op, p, na, nb, k, n, cap1, cap2))
+    return rows
+
+
+def test_batch_records_from_job_tuples():
+    """The C helper behind Context.batch writes the records the job tuples
+    describe, for every operation, argument form and array kind (uint32,
+    other dtypes, lists, read-only and non-contiguous arrays, empty operands)."""
+    import numpy as np
+    rng = np.random.default_rng(3)
+    a = rng.integers(0, 97, 50, dtype=np.uint32)
+    ro = a.copy()
+    ro.setflags(write=False)
+    jobs = [("conv", 97, a, a), ("conv", 97, a, a[:7], None), ("conv", 97, a, a, 30), ("conv", 97, a, [], None),
+            ("conv", 97, [1, 2, 3], a.astype(np.int64), 0), ("conv", 97, a[::2], ro),
+            ("inv", 998244353, a, 100), ("log", 998244353, ro, np.int64(9)), ("exp", 7340033, [0, 1], 5),
+            ("sqrt", 97, a.astype(np.int32), 3), ("pow", 97, a, (1 << 64) - 1, 40), ("pow", 97, a, 0, 0),
+            ("divmod", 97, a, a[:9]), ("divmod", 97, a[:3], a), ("inv", np.uint32(97), np.zeros(0, np.uint32), 4)]
+    m = len(jobs)
+    arr = np.zeros(m, dtype=F._JOB_DTYPE)
+    caps = np.empty(2 * m, np.int64)
+    keep = F._jobs_ext().fill(jobs, arr.ctypes.data, caps.ctypes.data, F._OPS, F._arr)
+    want = _records_in_python(jobs)
+    for i, (op, p, la, lb, k, n, c1, c2) in enumerate(want):
+        r = arr[i]
+        assert (int(r["op"]), int(r["p"]), int(r["la"]), int(r["lb"]), int(r["k"]), int(r["n"])) == \
+            (op, p, la, lb, k, n), (i, jobs[i][0])
+        assert (int(caps[i]), int(caps[m + i])) == (c1, c2), i
+        assert (int(r["a"]) == 0) == (la == 0) and (int(r["b"]) == 0) == (lb == 0), i
+    # uint32 C-contiguous inputs are read in place, everything else converted (and kept)
+    assert int(arr[0]["a"]) == a.ctypes.data and int(arr[7]["a"]) == ro.ctypes.data
+    assert len(keep) == 6 and all(k.dtype == np.uint32 and k.flags.c_contiguous for k in keep)
+    for bad, exc in [(("conv", 97, a), ValueError), (("nope", 97, a, 1), KeyError), (("inv", -1, a, 4), OverflowError),
+                     (("inv", 1 << 32, a, 4), OverflowError), (("pow", 97, a, 3), ValueError)]:
+        with pytest.raises(exc):
+            F._jobs_ext().fill([bad], arr.ctypes.data, caps.ctypes.data, F._OPS, F._arr)
