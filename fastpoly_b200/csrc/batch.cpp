@@ -179,10 +179,10 @@ class BatchRec {
       if (!g.c3) g.c3 = g.c1;
     }
     const auto ts = std::chrono::steady_clock::now();
-    Engine::Stage& st = e_.stage(batch_descriptor_bytes(plan_));
+    Engine::Stage st = e_.stage(batch_descriptor_bytes(plan_));
     const auto tl = std::chrono::steady_clock::now();
     e_.prof_begin();
-    e_.check(launch_batch(plan_, st.host, st.dev.get(), e_.stream(), st.ev), "batch");
+    e_.check(launch_batch(plan_, st.host, st.dev, e_.stream(), st.ev), "batch");
     e_.prof_end("batch");
     e_.host_phase("stage_wait", std::chrono::duration<double, std::milli>(tl - ts).count());
     e_.host_phase("launch_batch", std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - tl).count());
@@ -230,23 +230,88 @@ class BatchRec {
 
 // ------------------------------------------------------------ staging ring
 
-Engine::Stage& Engine::stage(size_t bytes) {
-  Stage& s = stages_[stage_next_];
-  stage_next_ = (stage_next_ + 1) % kStages;
-  if (!s.ev) check(cudaEventCreateWithFlags(&s.ev, cudaEventDisableTiming), "cudaEventCreate");
-  else check(cudaEventSynchronize(s.ev), "staging wait");  // the slot's previous copy has left
-  if (bytes > s.cap) {
-    const auto t0 = std::chrono::steady_clock::now();
-    const size_t cap = std::max<size_t>(bytes + bytes / 2, size_t(1) << 16);
-    if (s.host) cudaFreeHost(s.host);
-    s.host = nullptr;
-    s.cap = 0;
-    check(cudaMallocHost(&s.host, cap), "cudaMallocHost");
-    s.dev = Buf(&pool_, cap / 4 + 1);
-    s.cap = cap;
-    count_host_alloc(t0);
+bool Engine::stage_fits(size_t bytes, size_t& off) const {
+  const size_t cap = arena_.cap;
+  if (live_.empty()) {
+    off = 0;
+    return bytes <= cap;
   }
-  return s;
+  // free space: [head_, cap) and [0, tail) when head_ >= tail, else [head_, tail);
+  // an allocation never ends exactly at tail, so head_ == tail means empty
+  const size_t tail = live_.front().off;
+  if (head_ >= tail) {
+    if (cap - head_ >= bytes) {
+      off = head_;
+      return true;
+    }
+    off = 0;
+    return bytes < tail;
+  }
+  off = head_;
+  return bytes < tail - head_;
+}
+
+void Engine::stage_grow(size_t bytes) {
+  const auto t0 = std::chrono::steady_clock::now();
+  size_t cap = std::max(kMinArena, 2 * arena_.cap);
+  while (cap < 2 * bytes) cap *= 2;
+  StageArena a;
+  check(cudaMallocHost(reinterpret_cast<void**>(&a.host), cap), "cudaMallocHost");
+  try {
+    a.dev = Buf(&pool_, cap / 4);
+  } catch (...) {
+    cudaFreeHost(a.host);
+    throw;
+  }
+  a.cap = cap;
+  if (arena_.host) old_arenas_.push_back(std::move(arena_));
+  arena_ = std::move(a);
+  for (const StageRegion& r : live_) pending_.push_back(r.ev);
+  live_.clear();
+  head_ = 0;
+  count_host_alloc(t0);
+}
+
+Engine::Stage Engine::stage(size_t bytes) {
+  bytes = (bytes + 255) & ~size_t(255);
+  auto done = [&](cudaEvent_t e) {
+    const cudaError_t q = cudaEventQuery(e);
+    if (q == cudaErrorNotReady) return false;
+    check(q, "staging query");
+    return true;
+  };
+  while (!pending_.empty() && done(pending_.front())) {
+    stage_free_ev_.push_back(pending_.front());
+    pending_.pop_front();
+  }
+  while (!live_.empty() && done(live_.front().ev)) {
+    stage_free_ev_.push_back(live_.front().ev);
+    live_.pop_front();
+  }
+  if (live_.empty()) head_ = 0;
+  size_t off = 0;
+  while (!stage_fits(bytes, off)) {
+    if (live_.empty() || arena_.cap < kMaxArena) {
+      stage_grow(bytes);
+      continue;
+    }
+    // the arena is at its largest: wait for the oldest region's copy
+    check(cudaEventSynchronize(live_.front().ev), "staging wait");
+    stage_free_ev_.push_back(live_.front().ev);
+    live_.pop_front();
+    if (live_.empty()) head_ = 0;
+  }
+  cudaEvent_t ev;
+  if (!stage_free_ev_.empty()) {
+    ev = stage_free_ev_.back();
+    stage_free_ev_.pop_back();
+  } else {
+    check(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming), "cudaEventCreate");
+    stage_all_ev_.push_back(ev);
+  }
+  live_.push_back(StageRegion{off, ev});
+  head_ = off + bytes;
+  return Stage{arena_.host + off, static_cast<char*>(static_cast<void*>(arena_.dev.get())) + off, ev};
 }
 
 void Engine::free_stages() {
@@ -255,14 +320,21 @@ void Engine::free_stages() {
     if (q.ev) cudaEventDestroy(q.ev);
     q = Pin();
   }
-  for (Stage& s : stages_) {
-    if (s.host) cudaFreeHost(s.host);
-    if (s.ev) cudaEventDestroy(s.ev);
-    s.host = nullptr;
-    s.ev = nullptr;
-    s.cap = 0;
-    s.dev.reset();
+  // the engine's streams are drained: every staging copy has completed
+  live_.clear();
+  pending_.clear();
+  old_arenas_.push_back(std::move(arena_));
+  arena_ = StageArena();
+  for (StageArena& a : old_arenas_) {
+    if (a.host) cudaFreeHost(a.host);
+    a.host = nullptr;
+    a.dev.reset();
   }
+  old_arenas_.clear();
+  for (cudaEvent_t e : stage_all_ev_) cudaEventDestroy(e);
+  stage_all_ev_.clear();
+  stage_free_ev_.clear();
+  head_ = 0;
 }
 
 void Engine::count_batch(const BatchPlan& b) {
@@ -276,18 +348,18 @@ void Engine::count_batch(const BatchPlan& b) {
 }
 
 void Engine::gather_first(const std::vector<const uint32_t*>& ptrs, uint32_t* host_out) {
-  Stage& st = stage(ptrs.size() * 12 + 512);
+  Stage st = stage(ptrs.size() * 12 + 512);
   prof_begin();
-  check(launch_gather_first(ptrs, st.host, st.dev.get(), host_out, stream_), "gather");
+  check(launch_gather_first(ptrs, st.host, st.dev, host_out, stream_), "gather");
   prof_end("gather");  // counts the launch
   sync();
 }
 
 void Engine::convert_repr(const std::vector<ReprSeg>& segs) {
   if (segs.empty()) return;
-  Stage& st = stage(repr_batch_bytes(segs.size()));
+  Stage st = stage(repr_batch_bytes(segs.size()));
   prof_begin();
-  check(launch_repr_batch(segs, st.host, st.dev.get(), stream_, st.ev), "repr");
+  check(launch_repr_batch(segs, st.host, st.dev, stream_, st.ev), "repr");
   prof_end("repr");
   launches_ += (segs.size() + 65534) / 65535;
 }
@@ -349,7 +421,7 @@ namespace {
 enum Route : uint8_t { kNone, kConv, kInv, kLog, kExp, kSingle, kInvF, kExpF };
 }
 
-void Engine::batch(fpx_job* jobs, size_t count) {
+void Engine::batch(fpx_job* jobs, size_t count, const uint32_t* first_words) {
   std::vector<uint8_t> route(count, kNone);
   std::vector<const uint32_t*> firsts(count, nullptr);
   std::vector<size_t> conv_len(count, 0);
@@ -415,7 +487,12 @@ void Engine::batch(fpx_job* jobs, size_t count) {
   // ---- domain checks of inv / log / exp: one gather of every constant term
   if (need_first) {
     std::vector<uint32_t> a0(count, 0);
-    gather_first(firsts, a0.data());
+    if (first_words) {
+      for (size_t i = 0; i < count; ++i)
+        if (firsts[i]) a0[i] = first_words[i];
+    } else {
+      gather_first(firsts, a0.data());
+    }
     for (size_t i = 0; i < count; ++i) {
       fpx_job& j = jobs[i];
       const uint32_t p = j.p;
@@ -622,9 +699,9 @@ void Engine::batch(fpx_job* jobs, size_t count) {
       }
     }
     if (!preps.empty()) {
-      Stage& st = stage(batch_aux_bytes(preps.size()));
+      Stage st = stage(batch_aux_bytes(preps.size()));
       prof_begin();
-      check(launch_exp_prep_batch(preps, st.host, st.dev.get(), stream_, st.ev), "prep");
+      check(launch_exp_prep_batch(preps, st.host, st.dev, stream_, st.ev), "prep");
       prof_end("prep");
     }
     // the one-CTA Newton jobs depend on nothing the lockstep loop computes:
@@ -656,7 +733,7 @@ void Engine::batch(fpx_job* jobs, size_t count) {
       bool any_nat = false, any_crt = false;
       for (const NewtonJob& x : fused) (x.aux ? any_crt : any_nat) = true;
       const int newton_kernels = (int)any_nat + (int)any_crt;
-      Stage& st = stage(batch_newton_bytes(fused.size()));
+      Stage st = stage(batch_newton_bytes(fused.size()));
       fdesc = Buf(&pool_, batch_newton_bytes(fused.size()) / 4 + 1);
       if (side) {
         check(cudaEventRecord(side_fork_, stream_), "cudaEventRecord");
@@ -672,15 +749,15 @@ void Engine::batch(fpx_job* jobs, size_t count) {
       }
     }
     if (!seeds1.empty()) {
-      Stage& st = stage(batch_aux_bytes(seeds1.size()));
+      Stage st = stage(batch_aux_bytes(seeds1.size()));
       prof_begin();
-      check(launch_seeds_batch(seeds1, st.host, st.dev.get(), stream_, st.ev), "seed");
+      check(launch_seeds_batch(seeds1, st.host, st.dev, stream_, st.ev), "seed");
       prof_end("seed");
     }
     if (!seeds2.empty()) {
-      Stage& st = stage(batch_aux_bytes(seeds2.size()));
+      Stage st = stage(batch_aux_bytes(seeds2.size()));
       prof_begin();
-      check(launch_seeds_batch(seeds2, st.host, st.dev.get(), stream_, st.ev), "seed");
+      check(launch_seeds_batch(seeds2, st.host, st.dev, stream_, st.ev), "seed");
       prof_end("seed");
     }
 
@@ -918,6 +995,16 @@ void Engine::batch_host(fpx_job* jobs, size_t count, int repr) {
     in_off[1] = in_words;
     out_off[1] = out_words;
   }
+  // Constant terms for the domain checks of inv / log / exp, read from the
+  // caller's buffers (canonical limbs only; Montgomery limbs are converted on
+  // the device first, so those batches read them there).
+  std::vector<uint32_t> first;
+  if (repr != FPX_REPR_MONTGOMERY) {
+    first.assign(count, 0);
+    for (size_t i = 0; i < count; ++i)
+      if (wa[i] && (jobs[i].op == FPX_OP_INV || jobs[i].op == FPX_OP_LOG || jobs[i].op == FPX_OP_EXP))
+        first[i] = jobs[i].a[0];
+  }
   if (!copy_stream_) {
     check(cudaStreamCreateWithFlags(&copy_stream_, cudaStreamNonBlocking), "cudaStreamCreate");
     for (auto& e : chunk_ev_) check(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "cudaEventCreate");
@@ -956,7 +1043,7 @@ void Engine::batch_host(fpx_job* jobs, size_t count, int repr) {
     host_phase("copy_in", ms_since(t0));
     t0 = HClock::now();
     if (repr == FPX_REPR_MONTGOMERY) convert_repr(segs[c]);
-    batch(dj.data() + bounds[c], bounds[c + 1] - bounds[c]);
+    batch(dj.data() + bounds[c], bounds[c + 1] - bounds[c], first.empty() ? nullptr : first.data() + bounds[c]);
     if (repr == FPX_REPR_MONTGOMERY) {
       std::vector<ReprSeg> outs;
       for (size_t i = bounds[c]; i < bounds[c + 1]; ++i) {

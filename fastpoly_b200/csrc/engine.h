@@ -10,6 +10,7 @@
 #include <chrono>
 #include <cstdint>
 #include <functional>
+#include <deque>
 #include <map>
 #include <set>
 #include <tuple>
@@ -146,10 +147,14 @@ class Engine {
   // Many independent operations (device pointers) with shared launches:
   // products of all jobs in one launch set per transform size, the Newton loops
   // of inv / log / exp in lockstep.  Sets each job's status and lengths.
-  void batch(fpx_job* jobs, size_t count);
-  // The same with host buffers (blocking): inputs packed into one pinned
-  // buffer and copied at once, outputs brought back in one copy; repr as the
-  // C ABI's (canonical or Montgomery limbs).
+  // first_words (optional): a[0] of every job (0 when la == 0), canonical,
+  // from a host copy of the inputs; the domain checks then need no device read
+  // (which waits for all work queued before the batch).
+  void batch(fpx_job* jobs, size_t count, const uint32_t* first_words = nullptr);
+  // The same with host buffers (blocking): inputs packed through pinned
+  // staging slots on several host threads, in two chunks pipelined with the
+  // kernels when large, outputs brought back the same way; repr as the C ABI's
+  // (canonical or Montgomery limbs).
   void batch_host(fpx_job* jobs, size_t count, int repr);
   // In-place representation changes of many arrays in one launch.
   void convert_repr(const std::vector<ReprSeg>& segs);
@@ -270,15 +275,37 @@ class Engine {
   void log_into(uint32_t p, const uint32_t* a, size_t la, size_t n, uint32_t* out);
 
   // ---- batches (batch.cpp)
-  struct Stage {  // one slot of the descriptor staging ring
-    void* host = nullptr;  // pinned
-    size_t cap = 0;
-    Buf dev;
-    cudaEvent_t ev = nullptr;  // recorded after the slot's host->device copy
+  // Descriptor staging: one pinned host arena and its device mirror, carved
+  // in ring order.  A region is reused once the event recorded after its
+  // host->device copy has completed (device offsets are rewritten only by
+  // later copies on the engine's stream, after the kernels that read them).
+  // When the next region does not fit, the arena doubles (up to kMaxArena)
+  // rather than waiting, so recording a batch never waits for the GPU to
+  // catch up; outgrown arenas are kept until the engine goes, since copies
+  // from them may be in flight and freeing pinned memory synchronises the device.
+  struct Stage {
+    void* host;
+    void* dev;
+    cudaEvent_t ev;  // the caller records it after the region's copy
   };
-  static constexpr int kStages = 4;
-  Stage stages_[kStages];
-  int stage_next_ = 0;
+  struct StageArena {
+    char* host = nullptr;
+    Buf dev;
+    size_t cap = 0;
+  };
+  struct StageRegion {
+    size_t off;
+    cudaEvent_t ev;
+  };
+  static constexpr size_t kMinArena = size_t(1) << 20, kMaxArena = size_t(256) << 20;
+  StageArena arena_;
+  std::vector<StageArena> old_arenas_;
+  std::deque<StageRegion> live_;     // regions of arena_ in allocation order
+  std::deque<cudaEvent_t> pending_;  // events of regions of outgrown arenas
+  std::vector<cudaEvent_t> stage_free_ev_, stage_all_ev_;
+  size_t head_ = 0;
+  bool stage_fits(size_t bytes, size_t& off) const;
+  void stage_grow(size_t bytes);
   // Two pinned staging slots of batch_host: host copies into one slot overlap
   // the DMA of the other.
   struct Pin {
@@ -302,8 +329,8 @@ class Engine {
   // while the next chunk's kernels run, and the events that order them.
   cudaStream_t copy_stream_ = nullptr;
   cudaEvent_t chunk_ev_[2] = {nullptr, nullptr};
-  // Next ring slot, holding >= bytes, whose previous copy has completed.
-  Stage& stage(size_t bytes);
+  // A staging region of at least `bytes` whose previous copy has completed.
+  Stage stage(size_t bytes);
   void free_stages();
   void count_batch(const BatchPlan& b);
   // host_out[i] = *ptrs[i] (0 for null), one launch, then synchronises.
