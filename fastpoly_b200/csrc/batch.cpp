@@ -418,10 +418,11 @@ void Engine::ext_phase2(BatchRec& rec, const ExtJob& j) {
 namespace {
 // kInvF / kExpF: inverse / exp on a transform prime up to 2^13 terms, one CTA
 // per job in one launch (k_newton_b); kInv / kExp: the lockstep doubling loop.
-enum Route : uint8_t { kNone, kConv, kInv, kLog, kExp, kSingle, kInvF, kExpF };
+// kDerived: sqrt / pow / divmod, as phases of batched operations where they can.
+enum Route : uint8_t { kNone, kConv, kInv, kLog, kExp, kSingle, kInvF, kExpF, kDerived };
 }
 
-void Engine::batch(fpx_job* jobs, size_t count, const uint32_t* first_words) {
+void Engine::batch(fpx_job* jobs, size_t count, const uint32_t* first_words, const fpx_job* host, bool host_mont) {
   std::vector<uint8_t> route(count, kNone);
   std::vector<const uint32_t*> firsts(count, nullptr);
   std::vector<size_t> conv_len(count, 0);
@@ -473,11 +474,11 @@ void Engine::batch(fpx_job* jobs, size_t count, const uint32_t* first_words) {
         if (j.n == 0) break;
         if (!j.out) { j.status = FPX_EINVAL; break; }
         j.out_len = j.n;
-        route[i] = kSingle;
+        route[i] = kDerived;
         break;
       case FPX_OP_DIVMOD:  // out / out2 may be null: quotient / remainder not wanted
         if (j.lb && !j.b) { j.status = FPX_EINVAL; break; }
-        route[i] = kSingle;
+        route[i] = kDerived;
         break;
       default:
         j.status = FPX_EINVAL;
@@ -870,41 +871,352 @@ void Engine::batch(fpx_job* jobs, size_t count, const uint32_t* first_words) {
     }
   }
 
+  // ---- sqrt / pow / divmod through batched phases
+  std::vector<size_t> derived;
+  for (size_t i = 0; i < count; ++i)
+    if (route[i] == kDerived) derived.push_back(i);
+  if (!derived.empty()) batch_derived(jobs, derived, host, host_mont);
+
   // ---- jobs that share no launches run one after another
-  for (size_t i = 0; i < count; ++i) {
-    if (route[i] != kSingle) continue;
-    fpx_job& j = jobs[i];
-    try {
-      switch (j.op) {
-        case FPX_OP_CONV: j.out_len = conv(j.p, j.a, j.la, j.b, j.lb, j.n, j.out); break;
-        case FPX_OP_INV: inv(j.p, j.a, std::min(j.la, j.n), j.n, j.out); break;
-        case FPX_OP_LOG: log(j.p, j.a, std::min(j.la, j.n), j.n, j.out); break;
-        case FPX_OP_EXP: exp(j.p, j.a, std::min(j.la, j.n), j.n, j.out); break;
-        case FPX_OP_SQRT: sqrt(j.p, j.a, std::min(j.la, j.n), j.n, j.out); break;
-        case FPX_OP_POW: pow(j.p, j.a, j.la, j.k, j.n, j.out); break;
-        case FPX_OP_DIVMOD: {
-          size_t lq = 0, lr = 0;
-          divmod(j.p, j.a, j.la, j.b, j.lb, j.out, &lq, j.out2, &lr, j.out != nullptr, j.out2 != nullptr);
-          j.out_len = lq;
-          j.out2_len = lr;
-          break;
-        }
-        default: j.status = FPX_EINVAL;
+  for (size_t i = 0; i < count; ++i)
+    if (route[i] == kSingle) batch_single(jobs[i]);
+}
+
+void Engine::batch_single(fpx_job& j) {
+  try {
+    switch (j.op) {
+      case FPX_OP_CONV: j.out_len = conv(j.p, j.a, j.la, j.b, j.lb, j.n, j.out); break;
+      case FPX_OP_INV: inv(j.p, j.a, std::min(j.la, j.n), j.n, j.out); break;
+      case FPX_OP_LOG: log(j.p, j.a, std::min(j.la, j.n), j.n, j.out); break;
+      case FPX_OP_EXP: exp(j.p, j.a, std::min(j.la, j.n), j.n, j.out); break;
+      case FPX_OP_SQRT: sqrt(j.p, j.a, std::min(j.la, j.n), j.n, j.out); break;
+      case FPX_OP_POW: pow(j.p, j.a, j.la, j.k, j.n, j.out); break;
+      case FPX_OP_DIVMOD: {
+        size_t lq = 0, lr = 0;
+        divmod(j.p, j.a, j.la, j.b, j.lb, j.out, &lq, j.out2, &lr, j.out != nullptr, j.out2 != nullptr);
+        j.out_len = lq;
+        j.out2_len = lr;
+        break;
       }
-    } catch (const Error& e) {
-      if (e.code == FPX_ECUDA) throw;  // the stream is unusable: fail the whole batch
+      default: j.status = FPX_EINVAL;
+    }
+  } catch (const Error& e) {
+    if (e.code == FPX_ECUDA) throw;  // the stream is unusable: fail the whole batch
+    j.status = e.code;
+    j.out_len = 0;
+    j.out2_len = 0;
+  }
+}
+
+
+// ------------------------------------------------------- sqrt / pow / divmod
+
+namespace {
+// sqrt jobs above this many result terms keep the single path (one Newton
+// loop, about half the work of the log and exp below).
+constexpr size_t kDerivedSqrtMax = size_t(1) << 16;
+// Longer pow / divmod jobs keep the single path too: a batch holds few of them
+// (phases gain little), and their phase buffers, sized by the sum over the
+// batch, asked the pool for new multi-GB classes (a served mix spent twice as
+// long in cudaMalloc, single calls up to 110 ms, stalling every worker).
+constexpr size_t kDerivedMax = size_t(1) << 17;
+
+// FPX_BATCH_PHASED=0: every sqrt / pow / divmod job of a batch through the
+// single path, one after another.
+bool phased_on() {
+  static const bool on = [] {
+    const char* e = std::getenv("FPX_BATCH_PHASED");
+    return !(e && e[0] == '0');
+  }();
+  return on;
+}
+
+// Operand reads for the host decisions (valuation, constant terms, degrees):
+// the caller's host copy when batch_host has one, else the device.
+struct OperandReader {
+  Engine& e;
+  bool mont;
+  uint32_t p = 0, rinv = 1;  // 2^-32 mod p, for Montgomery host words
+  size_t first(const uint32_t* dev, const uint32_t* host, size_t n) {
+    if (!host) return e.find_nonzero(dev, n, false);
+    for (size_t i = 0; i < n; ++i)
+      if (host[i]) return i;
+    return n;
+  }
+  size_t last(const uint32_t* dev, const uint32_t* host, size_t n) {
+    if (!host) return e.find_nonzero(dev, n, true);
+    for (size_t i = n; i-- > 0;)
+      if (host[i]) return i;
+    return n;
+  }
+  uint32_t word(const uint32_t* dev, const uint32_t* host, size_t at, uint32_t mod) {
+    if (!host) return e.read_word(dev + at);
+    if (!mont) return host[at];
+    if (mod != p) {
+      p = mod;
+      rinv = invm((uint32_t)((uint64_t(1) << 32) % mod), mod);
+    }
+    return (uint32_t)((uint64_t)host[at] * rinv % mod);
+  }
+};
+
+// One sqrt / pow / divmod job run as phases.
+struct DerivedJob {
+  size_t i;
+  int op;
+  // sqrt / pow: dst[0, inner) = post * exp(mid * log(u * pre)), u = ulen words
+  const uint32_t* u = nullptr;
+  size_t ulen = 0, inner = 0;
+  uint32_t pre = 0, mid = 0, post = 0;
+  uint32_t* dst = nullptr;
+  uint32_t *nrm = nullptr, *l = nullptr;
+  // divmod (division.hpp:12-80): q = reverse(reverse(a) / reverse(b)), r = a - b q
+  size_t an = 0, bn = 0, dn = 0, nrb = 0, rn = 0, lp = 0;
+  uint32_t *ra = nullptr, *rb = nullptr, *ib = nullptr, *rq = nullptr, *qd = nullptr, *prod = nullptr;
+  bool failed = false;
+};
+}  // namespace
+
+void Engine::batch_derived(fpx_job* jobs, const std::vector<size_t>& idx, const fpx_job* host, bool host_mont) {
+  OperandReader rd{*this, host_mont};
+  std::vector<DerivedJob> dj;
+  std::vector<size_t> single;
+  // ---- host decisions: the cases the single path settles without products,
+  // or with binary powering, stay there; the rest become phases
+  for (size_t i : idx) {
+    fpx_job& j = jobs[i];
+    const uint32_t p = j.p;
+    const fpx_job* h = host ? host + i : nullptr;
+    DerivedJob d;
+    d.i = i;
+    d.op = j.op;
+    bool ok = false;
+    const bool phased = phased_on() && p != 2;
+    if (phased && j.op == FPX_OP_POW) {  // power.hpp:17-87, as Engine::pow
+      const size_t n = j.n, la = j.la;
+      const uint64_t k = j.k;
+      const size_t v = k > 1 ? rd.first(j.a, h ? h->a : nullptr, la) : la;
+      if (v < la && !(v != 0 && k > (n - 1) / v)) {
+        const size_t sh = (size_t)(v * k), inner = n - sh;
+        size_t ulen = std::min(la - v, inner);
+        ulen = rd.last(j.a + v, h ? h->a + v : nullptr, ulen) + 1;
+        if (ulen > 1 && k > 64 && inner <= p && inner <= kDerivedMax) {
+          const uint32_t c0 = rd.word(j.a, h ? h->a : nullptr, v, p);
+          d.u = j.a + v;
+          d.ulen = ulen;
+          d.inner = inner;
+          d.pre = invm(c0, p);
+          d.mid = (uint32_t)(k % p);
+          d.post = powm(c0, k, p);
+          d.dst = j.out + sh;
+          ok = true;
+        }
+      }
+    } else if (phased && j.op == FPX_OP_SQRT) {  // square_root.hpp, as exp(log(u / u0) / 2) * sqrt(u0)
+      const size_t n = j.n, la = std::min(j.la, j.n);
+      const size_t v = rd.first(j.a, h ? h->a : nullptr, la);
+      uint32_t root0 = 0;
+      if (v < la && !(v & 1)) {
+        const uint32_t u0 = rd.word(j.a, h ? h->a : nullptr, v, p);
+        const size_t half = v / 2;
+        if (half < n && n - half <= std::min<size_t>(p, kDerivedSqrtMax) && sqrt_mod(u0, p, &root0)) {
+          d.u = j.a + v;
+          d.ulen = la - v;
+          d.inner = n - half;
+          d.pre = invm(u0, p);
+          d.mid = (p + 1) / 2;
+          d.post = root0;
+          d.dst = j.out + half;
+          ok = true;
+        }
+      }
+    } else if (phased && j.op == FPX_OP_DIVMOD) {
+      const size_t al = rd.last(j.a, h ? h->a : nullptr, j.la), bl = rd.last(j.b, h ? h->b : nullptr, j.lb);
+      d.an = al < j.la ? al + 1 : 0;
+      d.bn = bl < j.lb ? bl + 1 : 0;
+      if (d.bn > 1 && d.an >= d.bn && d.an <= kDerivedMax) {
+        d.dn = d.an - d.bn + 1;
+        d.nrb = std::min(d.bn, d.dn);
+        d.rn = d.bn - 1;
+        d.lp = std::min(d.bn + d.dn - 1, d.rn);
+        ok = true;
+      }
+    }
+    if (ok) dj.push_back(d);
+    else single.push_back(i);
+  }
+  // a failure other than a CUDA error (the pool limit, say) fails the phased
+  // jobs only, as it fails one job on the single path
+  try {
+    // ---- scratch of every phased job: one pool block
+    auto r64 = [](size_t w) { return (w + 63) & ~size_t(63); };
+    size_t words = 0;
+    for (const DerivedJob& d : dj) {
+      const fpx_job& j = jobs[d.i];
+      if (d.op == FPX_OP_DIVMOD)
+        words += 3 * r64(d.dn) + r64(d.nrb) + (j.out ? 0 : r64(d.dn)) + (j.out2 ? r64(d.lp) : 0);
+      else
+        words += r64(d.ulen) + r64(d.inner);
+    }
+    Buf arena;
+    if (words) arena = Buf(&pool_, words);
+    uint32_t* q = arena.get();
+    auto take = [&](size_t w) {
+      uint32_t* r = q;
+      q += r64(w);
+      return r;
+    };
+    for (DerivedJob& d : dj) {
+      fpx_job& j = jobs[d.i];
+      if (d.op == FPX_OP_DIVMOD) {
+        d.ra = take(d.dn);
+        d.rb = take(d.nrb);
+        d.ib = take(d.dn);
+        d.rq = take(d.dn);
+        d.qd = j.out ? j.out : take(d.dn);
+        if (j.out2) d.prod = take(d.lp);
+      } else {
+        d.nrm = take(d.ulen);
+        d.l = take(d.inner);
+      }
+    }
+    auto launch = [&](const char* what, auto&& fn) {
+      prof_begin();
+      check(fn(), what);
+      prof_end(what);
+    };
+    // One phase: the internal jobs as one batch (their constant terms are known:
+    // 1 for log and inverse inputs, 0 for exp's), failures passed to their owners.
+    std::vector<fpx_job> in;
+    std::vector<size_t> owner;
+    std::vector<uint32_t> firsts;
+    auto add = [&](size_t d, int op, uint32_t p, const uint32_t* a, size_t la, const uint32_t* b, size_t lb, size_t n,
+                   uint32_t* out, uint32_t first) {
+      fpx_job x{};
+      x.op = op;
+      x.p = p;
+      x.a = a;
+      x.la = la;
+      x.b = b;
+      x.lb = lb;
+      x.n = n;
+      x.out = out;
+      in.push_back(x);
+      owner.push_back(d);
+      firsts.push_back(first);
+    };
+    auto run = [&]() {
+      if (!in.empty()) {
+        batch(in.data(), in.size(), firsts.data());
+        for (size_t t = 0; t < in.size(); ++t) {
+          DerivedJob& d = dj[owner[t]];
+          if (in[t].status != FPX_OK && !d.failed) {
+            d.failed = true;
+            jobs[d.i].status = in[t].status;
+          }
+        }
+      }
+      in.clear();
+      owner.clear();
+      firsts.clear();
+    };
+
+    // A: normalised operands (u / u0, u / c0) and reversed divmod operands
+    for (DerivedJob& d : dj) {
+      fpx_job& j = jobs[d.i];
+      if (d.op == FPX_OP_DIVMOD) {
+        launch("reverse", [&] { return launch_reverse(j.a + (d.an - d.dn), d.ra, d.dn, stream_); });
+        launch("reverse", [&] { return launch_reverse(j.b + (d.bn - d.nrb), d.rb, d.nrb, stream_); });
+      } else {
+        check(cudaMemsetAsync(j.out, 0, j.n * 4, stream_), "memset");
+        launch("normalise", [&] { return launch_scale(j.p, d.u, d.nrm, d.ulen, d.pre, stream_); });
+      }
+    }
+    // B: log of the normalised operands; inverse of the reversed divisors
+    for (size_t t = 0; t < dj.size(); ++t) {
+      DerivedJob& d = dj[t];
+      const uint32_t p = jobs[d.i].p;
+      if (d.op == FPX_OP_DIVMOD) add(t, FPX_OP_INV, p, d.rb, d.nrb, nullptr, 0, d.dn, d.ib, 1);
+      else add(t, FPX_OP_LOG, p, d.nrm, d.ulen, nullptr, 0, d.inner, d.l, 1);
+    }
+    run();
+    // C: the log times k (pow) or 1/2 (sqrt)
+    for (DerivedJob& d : dj)
+      if (d.op != FPX_OP_DIVMOD && !d.failed)
+        launch("scale", [&] { return launch_scale(jobs[d.i].p, d.l, d.l, d.inner, d.mid, stream_); });
+    // D: exp of it into the result window; the reversed quotient
+    for (size_t t = 0; t < dj.size(); ++t) {
+      DerivedJob& d = dj[t];
+      if (d.failed) continue;
+      const uint32_t p = jobs[d.i].p;
+      if (d.op == FPX_OP_DIVMOD) add(t, FPX_OP_CONV, p, d.ra, d.dn, d.ib, d.dn, d.dn, d.rq, 0);
+      else add(t, FPX_OP_EXP, p, d.l, d.inner, nullptr, 0, d.inner, d.dst, 0);
+    }
+    run();
+    // E: times c0^k (pow) or the constant term's root (sqrt); the quotient
+    for (DerivedJob& d : dj) {
+      if (d.failed) continue;
+      const fpx_job& j = jobs[d.i];
+      if (d.op == FPX_OP_DIVMOD)
+        launch("reverse", [&] { return launch_reverse(d.rq, d.qd, d.dn, stream_); });
+      else
+        launch("scale", [&] { return launch_scale(j.p, d.dst, d.dst, d.inner, d.post, stream_); });
+    }
+    // F: b q over the remainder's window, G: r = a - b q and its length
+    for (size_t t = 0; t < dj.size(); ++t) {
+      DerivedJob& d = dj[t];
+      const fpx_job& j = jobs[d.i];
+      if (d.op == FPX_OP_DIVMOD && !d.failed && j.out2) add(t, FPX_OP_CONV, j.p, j.b, d.bn, d.qd, d.dn, d.lp, d.prod, 0);
+    }
+    run();
+    std::vector<Segment> segs;
+    std::vector<size_t> seg_of;
+    for (size_t t = 0; t < dj.size(); ++t) {
+      DerivedJob& d = dj[t];
+      const fpx_job& j = jobs[d.i];
+      if (d.op != FPX_OP_DIVMOD || d.failed || !j.out2) continue;
+      launch("remainder", [&] { return launch_sub(j.p, j.a, d.prod, d.lp, j.out2, d.rn, stream_); });
+      segs.push_back(Segment{j.out2, d.rn});
+      seg_of.push_back(t);
+    }
+    std::vector<size_t> rlen(dj.size(), 0);
+    if (!segs.empty()) {
+      Stage st = stage(last_nonzero_batch_bytes(segs.size()));
+      launch("remainder length", [&] { return launch_last_nonzero_batch(segs, st.host, st.dev, stream_); });
+      sync();
+      const auto* res = reinterpret_cast<const unsigned long long*>(static_cast<const char*>(st.host) +
+                                                                    last_nonzero_results_offset(segs.size()));
+      for (size_t s2 = 0; s2 < segs.size(); ++s2) rlen[seg_of[s2]] = res[s2] < segs[s2].n ? (size_t)res[s2] + 1 : 0;
+    }
+    for (size_t t = 0; t < dj.size(); ++t) {
+      const DerivedJob& d = dj[t];
+      fpx_job& j = jobs[d.i];
+      if (d.failed) {
+        j.out_len = 0;
+        j.out2_len = 0;
+      } else if (d.op == FPX_OP_DIVMOD) {
+        j.out_len = j.out ? d.dn : 0;
+        j.out2_len = j.out2 ? rlen[t] : 0;
+      }
+    }
+  } catch (const Error& e) {
+    if (e.code == FPX_ECUDA) throw;
+    for (const DerivedJob& d : dj) {
+      fpx_job& j = jobs[d.i];
       j.status = e.code;
       j.out_len = 0;
       j.out2_len = 0;
     }
   }
+  // the rest: one after another
+  for (size_t i : single) batch_single(jobs[i]);
 }
-
 
 // ------------------------------------------------------- host-buffer batches
 
-// Packs every input into one pinned buffer (one host->device copy), runs the
-// batch on device copies, and brings every output back in one copy.
+// Packs the inputs into device copies through the pinned slots, runs the
+// batch on them (host decisions read from the caller's buffers), and brings
+// the outputs back the same way.
 void Engine::batch_host(fpx_job* jobs, size_t count, int repr) {
   // Words each job reads and writes (host side); the device copy of a job
   // points into one input and one output region.
@@ -1043,7 +1355,8 @@ void Engine::batch_host(fpx_job* jobs, size_t count, int repr) {
     host_phase("copy_in", ms_since(t0));
     t0 = HClock::now();
     if (repr == FPX_REPR_MONTGOMERY) convert_repr(segs[c]);
-    batch(dj.data() + bounds[c], bounds[c + 1] - bounds[c], first.empty() ? nullptr : first.data() + bounds[c]);
+    batch(dj.data() + bounds[c], bounds[c + 1] - bounds[c], first.empty() ? nullptr : first.data() + bounds[c],
+          jobs + bounds[c], repr == FPX_REPR_MONTGOMERY);
     if (repr == FPX_REPR_MONTGOMERY) {
       std::vector<ReprSeg> outs;
       for (size_t i = bounds[c]; i < bounds[c + 1]; ++i) {

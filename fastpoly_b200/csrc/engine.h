@@ -150,7 +150,11 @@ class Engine {
   // first_words (optional): a[0] of every job (0 when la == 0), canonical,
   // from a host copy of the inputs; the domain checks then need no device read
   // (which waits for all work queued before the batch).
-  void batch(fpx_job* jobs, size_t count, const uint32_t* first_words = nullptr);
+  // host (optional): the same jobs with the caller's host pointers (batch_host),
+  // read for the host decisions of sqrt / pow / divmod instead of the device;
+  // host_mont: those host words are Montgomery limbs.
+  void batch(fpx_job* jobs, size_t count, const uint32_t* first_words = nullptr, const fpx_job* host = nullptr,
+             bool host_mont = false);
   // The same with host buffers (blocking): inputs packed through pinned
   // staging slots on several host threads, in two chunks pipelined with the
   // kernels when large, outputs brought back the same way; repr as the C ABI's
@@ -333,14 +337,16 @@ class Engine {
   Stage stage(size_t bytes);
   void free_stages();
   void count_batch(const BatchPlan& b);
+  // One job of a batch through the single-operation path (errors to its status).
+  void batch_single(fpx_job& j);
+  // sqrt / pow / divmod jobs of a batch (indices idx) as phases of batched
+  // log / exp / inverse / product calls; the rest of them one after another.
+  void batch_derived(fpx_job* jobs, const std::vector<size_t>& idx, const fpx_job* host, bool host_mont);
   // host_out[i] = *ptrs[i] (0 for null), one launch, then synchronises.
   void gather_first(const std::vector<const uint32_t*>& ptrs, uint32_t* host_out);
   void ext_phase1(BatchRec& rec, const ExtJob& j);
   void ext_phase2(BatchRec& rec, const ExtJob& j);
 
-  // small device->host reads
-  uint32_t read_word(const uint32_t* d);
-  size_t find_nonzero(const uint32_t* a, size_t n, bool last);  // n if none
 
   void prof_begin();
   void prof_end(const char* what);
@@ -360,6 +366,9 @@ class Engine {
     a.second += ms;
   }
   bool profiling() const { return prof_on_; }
+  // small device->host reads (synchronous)
+  uint32_t read_word(const uint32_t* d);
+  size_t find_nonzero(const uint32_t* a, size_t n, bool last);  // n if none
   // Pinned host allocations of the staging buffers (count, host time: total
   // and longest); written by the thread that drives the engine.
   std::atomic<uint64_t> host_allocs{0}, host_alloc_ns{0}, host_alloc_ns_max{0};

@@ -2770,6 +2770,62 @@ cudaError_t launch_repr_batch(const std::vector<ReprSeg>& segs, void* host_stagi
 namespace fpx {
 // out_host[i] = *ptrs[i] (0 for null) for many device pointers: one H2D of the
 // pointer list, one kernel, one D2H; the caller synchronises the stream.
+namespace {
+constexpr int kScanThreads = 256, kScanPerThread = 4;
+// Block b: the last nonzero word of segment b, scanning windows of
+// kScanThreads * kScanPerThread words from the end (one window, as a rule: a
+// remainder's top words are zero only by chance).
+__global__ void __launch_bounds__(kScanThreads) k_last_nonzero_b(const Segment* __restrict__ segs,
+                                                                 unsigned long long* __restrict__ out) {
+  pdl_enter();
+  const Segment g = segs[blockIdx.x];
+  constexpr size_t W = (size_t)kScanThreads * kScanPerThread;
+  size_t hi = g.n;
+  unsigned long long found = g.n;
+  while (hi > 0) {
+    const size_t lo = hi > W ? hi - W : 0;
+    long long best = -1;
+#pragma unroll
+    for (int k = 0; k < kScanPerThread; ++k) {
+      const size_t i = lo + (size_t)k * kScanThreads + threadIdx.x;
+      if (i < hi && g.ptr[i] != 0u) best = (long long)i;
+    }
+    // the largest index found in this window, if any
+    __shared__ unsigned long long top;
+    if (threadIdx.x == 0) top = 0;
+    __syncthreads();
+    if (best >= 0) atomicMax(&top, (unsigned long long)best + 1);
+    __syncthreads();
+    const unsigned long long t = top;
+    __syncthreads();
+    if (t) {
+      found = t - 1;
+      break;
+    }
+    hi = lo;
+  }
+  if (threadIdx.x == 0) out[blockIdx.x] = found;
+}
+}  // namespace
+
+size_t last_nonzero_results_offset(size_t segs) { return (segs * sizeof(Segment) + 255) & ~size_t(255); }
+size_t last_nonzero_batch_bytes(size_t segs) { return last_nonzero_results_offset(segs) + segs * 8 + 256; }
+
+cudaError_t launch_last_nonzero_batch(const std::vector<Segment>& segs, void* host_staging, void* dev_buf,
+                                      cudaStream_t s) {
+  if (segs.empty()) return cudaSuccess;
+  const size_t bytes = segs.size() * sizeof(Segment), roff = last_nonzero_results_offset(segs.size());
+  std::memcpy(host_staging, segs.data(), bytes);
+  char* d = static_cast<char*>(dev_buf);
+  cudaError_t e = cudaMemcpyAsync(d, host_staging, bytes, cudaMemcpyHostToDevice, s);
+  if (e != cudaSuccess) return e;
+  auto* dres = reinterpret_cast<unsigned long long*>(d + roff);
+  (void)pdl_launch(k_last_nonzero_b, (unsigned)segs.size(), kScanThreads, 0, s,
+                   reinterpret_cast<const Segment*>(d), dres);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  return cudaMemcpyAsync(static_cast<char*>(host_staging) + roff, dres, segs.size() * 8, cudaMemcpyDeviceToHost, s);
+}
+
 cudaError_t launch_gather_first(const std::vector<const uint32_t*>& ptrs, void* host_staging, void* dev_buf,
                                 uint32_t* host_out, cudaStream_t s) {
   if (ptrs.empty()) return cudaSuccess;

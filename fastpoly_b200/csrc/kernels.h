@@ -314,4 +314,16 @@ cudaError_t launch_repr_batch(const std::vector<ReprSeg>& segs, void* host_stagi
 // host_out[i] = *ptrs[i]; dev_buf needs ptrs.size() * 12 + 256 bytes.
 cudaError_t launch_gather_first(const std::vector<const uint32_t*>& ptrs, void* host_staging, void* dev_buf,
                                 uint32_t* host_out, cudaStream_t s);
+// For each segment (ptr, n): the index of its last nonzero word, n if none,
+// one block per segment scanning back from the end.  The results land in the
+// pinned staging region itself (host_staging + last_nonzero_results_offset);
+// they are in place once the stream has passed the call.
+struct Segment {
+  const uint32_t* ptr;
+  size_t n;
+};
+size_t last_nonzero_batch_bytes(size_t segs);
+size_t last_nonzero_results_offset(size_t segs);
+cudaError_t launch_last_nonzero_batch(const std::vector<Segment>& segs, void* host_staging, void* dev_buf,
+                                      cudaStream_t s);
 }  // namespace fpx

@@ -157,8 +157,13 @@ int fpx_mod(fpx_ctx* ctx, uint32_t p, const uint32_t* a, size_t la, const uint32
  * functions, job by job.  The batch shares launches between jobs: all products
  * of a stage run as one launch set per transform size (mixed primes and CRT
  * lifts included), and the Newton loops of inv, log and exp advance in
- * lockstep.  sqrt, pow and divmod jobs, and transforms past 2^24 points, run
- * one after another inside the same call. */
+ * lockstep.  sqrt, pow and divmod jobs of up to 2^17 terms (sqrt: 2^16) run as
+ * phases of such batched calls (pow: log, then exp; sqrt: exp of half the log
+ * times the root of the constant term; divmod: inverse of the reversed
+ * divisor, then two products), with the remainders' lengths read back once
+ * per batch.  Longer ones, pow with exponents up to 64 (binary powering),
+ * characteristic 2, and transforms past 2^24 points run one after another
+ * inside the same call (FPX_BATCH_PHASED=0: every sqrt / pow / divmod job). */
 enum fpx_op {
   FPX_OP_CONV = 0,   /* out = conv(a, b, n)                     (convolution.hpp:145) */
   FPX_OP_INV = 1,    /* out = inv(a, n)                         (inverse.hpp:163) */
@@ -194,9 +199,11 @@ typedef struct fpx_job {
  * the whole batch). */
 int fpx_batch_submit(fpx_ctx* ctx, fpx_job* jobs, size_t count);
 int fpx_batch_wait(fpx_ctx* ctx);
-/* Host buffers (blocking): every input is packed into one pinned buffer and
- * copied to the device at once, the batch runs, and every output comes back in
- * one copy.  repr as for the single-job functions. */
+/* Host buffers (blocking): inputs are packed through pinned staging slots by
+ * several host threads while the DMA runs; a batch moving at least 64 MiB runs
+ * as two chunks, the second packed while the first computes and the first
+ * unpacked while the second computes.  Returns when every result is in the
+ * caller's buffers.  repr as for the single-job functions. */
 int fpx_batch_run(fpx_ctx* ctx, fpx_job* jobs, size_t count, int repr);
 
 /* ---- serving (no counterpart in the reference) --------------------------------

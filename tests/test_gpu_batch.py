@@ -292,3 +292,94 @@ def test_batch_smaller_arena_takes_cached_block(oracle):
             eq(first[i].cpu().numpy().view(np.uint32), oracle.conv(p, *host[i]), f"job {i}")
     finally:
         ctx.close()
+
+
+def _derived_jobs(rng):
+    """sqrt / pow / divmod jobs covering every host decision of the phased path."""
+    jobs = []
+    for p in (998244353, 1000000007, 167772161, 2147483647):
+        a = rnd(rng, p, 3000, nonzero0=True)
+        z = np.concatenate([np.zeros(6, np.uint32), a[:2000]])        # valuation 6
+        tz = np.concatenate([a[:700], np.zeros(300, np.uint32)])      # trailing zeros
+        sq = (rnd(rng, p, 1, nonzero0=True).astype(np.uint64) ** 2 % p).astype(np.uint32)
+        root_in = np.concatenate([sq, a[1:1500]])                     # a square constant term
+        jobs += [("sqrt", p, root_in, 1500), ("sqrt", p, np.concatenate([np.zeros(4, np.uint32), root_in]), 1800),
+                 ("sqrt", p, root_in[:40], 70000),                    # longer than the phased limit: single path
+                 ("pow", p, a[:800], (1 << 64) - 1, 2500), ("pow", p, z, 1000003, 2500), ("pow", p, tz, 999999, 2100),
+                 ("pow", p, a[:300], p * 5, 900),                      # k = 0 mod p
+                 ("pow", p, a[:300], 17, 900), ("pow", p, z, 10 ** 6, 30),   # binary powering; all-zero window
+                 ("divmod", p, a, a[:1200]), ("divmod", p, tz, np.concatenate([a[:90], np.zeros(5, np.uint32)])),
+                 ("divmod", p, a[:50], a[:400]), ("divmod", p, a, a[:1])]
+    return jobs
+
+
+def test_batch_sqrt_pow_divmod_phased(fpx, oracle):
+    """sqrt, pow and divmod jobs run as phases of batched log / exp / inverse /
+    product calls: the oracle's results, from host buffers in both limb forms."""
+    rng = np.random.default_rng(71)
+    jobs = _derived_jobs(rng)
+    res = fpx.batch(jobs)
+    for i, jb in enumerate(jobs):
+        _check(res[i], _oracle_job(oracle, jb), f"job {i} {jb[0]} p={jb[1]} len={len(jb[2])}")
+    # Montgomery limbs: the host decisions read converted words
+    sub = [jb for jb in jobs if jb[1] in (998244353, 1000000007)]
+    mj = []
+    for jb in sub:
+        p = jb[1]
+        m = lambda x: np.array([oracle.to_mont(p, int(v)) for v in x], np.uint32)
+        mj.append((jb[0], p, m(jb[2])) + ((m(jb[3]),) if jb[0] == "divmod" else jb[3:]))
+    mres = fpx.batch(mj, repr=F.MONTGOMERY)
+    for i, jb in enumerate(sub):
+        want = _oracle_job(oracle, jb)
+        p = jb[1]
+        m = lambda x: np.array([oracle.to_mont(p, int(v)) for v in x], np.uint32)
+        if isinstance(want, tuple):
+            want = (m(want[0]), m(want[1]))
+        elif not isinstance(want, Exception):
+            want = m(want)
+        _check(mres[i], want, f"mont job {i} {jb[0]} p={p}")
+
+
+def test_batch_sqrt_pow_divmod_device_pointers(fpx, oracle):
+    """The same jobs through fpx_batch_submit (the host decisions read the device)."""
+    import torch
+    rng = np.random.default_rng(72)
+    specs = [jb for jb in _derived_jobs(rng) if jb[1] in (998244353, 2147483647)]
+    jobs = (F.Job * len(specs))()
+    keep = []
+    for j, jb in zip(jobs, specs):
+        op, p, a = jb[0], jb[1], np.asarray(jb[2], np.uint32)
+        da = torch.from_numpy(a.view(np.int32).copy()).cuda()
+        keep.append(da)
+        j.op, j.p, j.a, j.la = F._OPS[op], p, da.data_ptr(), a.size
+        if op == "divmod":
+            b = np.asarray(jb[3], np.uint32)
+            db = torch.from_numpy(b.view(np.int32).copy()).cuda()
+            q, r = torch.zeros(a.size, dtype=torch.int32, device="cuda"), torch.zeros(b.size, dtype=torch.int32, device="cuda")
+            keep += [db, q, r]
+            j.b, j.lb, j.out, j.out2 = db.data_ptr(), b.size, q.data_ptr(), r.data_ptr()
+        else:
+            n = jb[-1]
+            o = torch.zeros(n, dtype=torch.int32, device="cuda")
+            keep.append(o)
+            j.n, j.out = n, o.data_ptr()
+            if op == "pow":
+                j.k = jb[3]
+    torch.cuda.synchronize()
+    fpx.batch_submit(jobs)
+    fpx.batch_wait()
+    for i, jb in enumerate(specs):
+        want = _oracle_job(oracle, jb)
+        j = jobs[i]
+        if isinstance(want, Exception):
+            assert j.status == F.EDOMAIN, (i, jb[0])
+            continue
+        assert j.status == F.OK, (i, jb[0], j.status)
+        if jb[0] == "divmod":
+            q = keep[[k for k, t in enumerate(keep) if t.data_ptr() == j.out][0]]
+            r = keep[[k for k, t in enumerate(keep) if t.data_ptr() == j.out2][0]]
+            eq(q.cpu().numpy().view(np.uint32)[: j.out_len], want[0], f"device job {i} q")
+            eq(r.cpu().numpy().view(np.uint32)[: j.out2_len], want[1], f"device job {i} r")
+        else:
+            o = keep[[k for k, t in enumerate(keep) if t.data_ptr() == j.out][0]]
+            eq(o.cpu().numpy().view(np.uint32)[: j.out_len], want, f"device job {i} {jb[0]}")
