@@ -161,6 +161,42 @@ class ClockSampler:
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def measure_link(mib: int = 64, reps: int = 8) -> dict:
+    """Pinned host <-> device copy bandwidth of this GPU's host link (GB/s): each
+    direction alone and both at once on two streams (torch copies, CUDA events)."""
+    import torch
+    n = mib << 18
+    h_in = torch.empty(n, dtype=torch.int32).pin_memory()
+    h_out = torch.empty(n, dtype=torch.int32).pin_memory()
+    d_in = torch.empty(n, dtype=torch.int32, device="cuda")
+    d_out = torch.zeros(n, dtype=torch.int32, device="cuda")
+    s1, s2 = torch.cuda.Stream(), torch.cuda.Stream()
+
+    def timed(h2d: bool, d2h: bool) -> float:
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(s1)
+        s2.wait_event(e0)
+        for _ in range(reps):
+            if h2d:
+                with torch.cuda.stream(s1):
+                    d_in.copy_(h_in, non_blocking=True)
+            if d2h:
+                with torch.cuda.stream(s2):
+                    h_out.copy_(d_out, non_blocking=True)
+        done = torch.cuda.Event()
+        done.record(s2)
+        s1.wait_event(done)
+        e1.record(s1)
+        torch.cuda.synchronize()
+        return reps * n * 4 / (e0.elapsed_time(e1) * 1e-3) / 1e9
+
+    timed(True, True)
+    h2d, d2h, both = timed(True, False), timed(False, True), timed(True, True)
+    return {"h2d_gbs": round(h2d, 1), "d2h_gbs": round(d2h, 1), "each_way_both_gbs": round(both, 1),
+            "how": f"pinned {mib} MiB copies x{reps}, torch, CUDA events; both: H2D and D2H on two streams"}
+
+
 def max_over_ranks(dist, values, device="cpu"):
     """Element-wise max of per-rank timings (every rank gets the result)."""
     if not dist:
@@ -411,6 +447,12 @@ def run_fpx(args):
                         "pageable": {"value": round(e2e_pageable, 1), "unit": "Mcoeff/s",
                                      "api": f"fpx_conv from pageable host memory, {callers} concurrent callers"}},
                 "gpu_launches": int(launches), "roofline": roof, "clocks": clk}
+        if world == 1:
+            # the host link bounds e2e: 32 MiB each way per conv
+            link = measure_link()
+            per_dir = max(2 * N_IN, N_OUT) * 4 * (e2e_value * 1e6 / N_OUT) / 1e9
+            line["e2e"]["link"] = dict(link, achieved_each_way_gbs=round(per_dir, 1),
+                                       frac=round(per_dir / link["each_way_both_gbs"], 3))
         if world == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_reference_sample(reps=3)
         if world == 1 and not args.headline_only:
