@@ -151,12 +151,99 @@ static Tw2 shoup_pair(uint32_t w, uint32_t p) { return Tw2{w, (uint32_t)(((uint6
 
 // --------------------------------------------------------------------- pool
 
+namespace {
+// The stream-ordered pool of a device, created on first use and kept for the
+// process: reserved memory is never handed back on synchronisation (release
+// threshold: all of it), and an allocation never waits for another stream's
+// work to reuse memory freed there (it takes completed frees or grows).
+cudaMemPool_t stream_pool(int device) {
+  static std::mutex mu;
+  static cudaMemPool_t pools[64];
+  static bool tried[64];
+  if (device < 0 || device >= 64) return nullptr;
+  std::lock_guard<std::mutex> g(mu);
+  if (!tried[device]) {
+    tried[device] = true;
+    cudaMemPoolProps props{};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = device;
+    cudaMemPool_t mp = nullptr;
+    if (cudaMemPoolCreate(&mp, &props) == cudaSuccess) {
+      uint64_t keep = UINT64_MAX;
+      int no = 0;
+      if (cudaMemPoolSetAttribute(mp, cudaMemPoolAttrReleaseThreshold, &keep) == cudaSuccess &&
+          cudaMemPoolSetAttribute(mp, cudaMemPoolReuseAllowInternalDependencies, &no) == cudaSuccess)
+        pools[device] = mp;
+      else
+        cudaMemPoolDestroy(mp);
+    }
+    cudaGetLastError();
+  }
+  return pools[device];
+}
+
+uint64_t pool_reserved(cudaMemPool_t mp) {
+  uint64_t v = 0;
+  if (cudaMemPoolGetAttribute(mp, cudaMemPoolAttrReservedMemCurrent, &v) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return (uint64_t)v;
+}
+}  // namespace
+
 Pool::~Pool() { release(); }
 
 uint32_t* Pool::get(size_t words, size_t* cls_out) {
   size_t bytes = words * sizeof(uint32_t);
   size_t cls = 1024;
   while (cls < bytes) cls <<= 1;
+  if (cls >= kStreamBytes) {
+    // large: from the device's stream-ordered pool, rounded to 2 MiB
+    cudaMemPool_t mp = nullptr;
+    const size_t size = (bytes + (size_t(2) << 20) - 1) & ~((size_t(2) << 20) - 1);
+    {
+      std::lock_guard<std::mutex> g(mu_);
+      if (!capturing_ && stream_) mp = stream_pool(device_);
+      if (mp) {
+        if (limit_ && in_use_bytes + size > limit_)
+          throw Error{FPX_ENOMEM, "device pool limit reached (" + std::to_string(limit_) + " bytes)"};
+        in_use_bytes += size;
+      }
+    }
+    if (mp) {
+      const auto t0 = std::chrono::steady_clock::now();
+      const uint64_t r0 = pool_reserved(mp);
+      void* p = nullptr;
+      cudaError_t e = cudaMallocFromPoolAsync(&p, size, mp, *stream_);
+      if (e != cudaSuccess) {
+        cudaGetLastError();
+        release();  // the free lists' cache, and the pool's unused reservation
+        e = cudaMallocFromPoolAsync(&p, size, mp, *stream_);
+      }
+      if (e != cudaSuccess) {
+        cudaGetLastError();
+        std::lock_guard<std::mutex> g(mu_);
+        in_use_bytes -= size;
+        throw Error{FPX_ENOMEM, "device allocation of " + std::to_string(size) + " bytes failed"};
+      }
+      const bool grew = pool_reserved(mp) > r0;
+      const uint64_t ns = static_cast<uint64_t>(
+          std::chrono::duration_cast<std::chrono::nanoseconds>(std::chrono::steady_clock::now() - t0).count());
+      std::lock_guard<std::mutex> g(mu_);
+      async_.insert(p);
+      if (grew) {
+        ++system_allocations;
+        alloc_ns += ns;
+        alloc_ns_max = std::max(alloc_ns_max, ns);
+      } else {
+        ++cache_hits;
+      }
+      *cls_out = size;
+      return static_cast<uint32_t*>(p);
+    }
+  }
   {
     std::lock_guard<std::mutex> g(mu_);
     if (capturing_) {
@@ -241,6 +328,16 @@ uint32_t* Pool::get(size_t words, size_t* cls_out) {
 
 void Pool::put(uint32_t* p, size_t cls) {
   std::lock_guard<std::mutex> g(mu_);
+  if (async_.erase(p)) {
+    // back to the stream-ordered pool after the stream's work on it
+    if (stream_) {
+      if (cudaFreeAsync(p, *stream_) != cudaSuccess) cudaGetLastError();
+    } else if (cudaFree(p) != cudaSuccess) {
+      cudaGetLastError();
+    }
+    in_use_bytes -= cls;
+    return;
+  }
   if (capturing_ && cap_owned_.count(p)) {
     cap_free_[cls].push_back(p);  // reused only inside the graph being captured
     return;
@@ -290,6 +387,11 @@ void Pool::release() {
   free_.clear();
   cached_bytes = 0;
   cached_blocks = 0;
+  // the device pool's unused reservation (every engine's: only memory no
+  // allocation holds is returned)
+  if (device_ >= 0)
+    if (cudaMemPool_t mp = stream_pool(device_))
+      if (cudaMemPoolTrimTo(mp, 0) != cudaSuccess) cudaGetLastError();
 }
 
 // ------------------------------------------------------------------- engine
@@ -304,6 +406,7 @@ Engine::Engine(int device, size_t pool_limit) : device_(device), pool_(pool_limi
   check(cudaSetDevice(device), "cudaSetDevice");
   check(cudaStreamCreateWithFlags(&own_stream_, cudaStreamNonBlocking), "cudaStreamCreate");
   stream_ = own_stream_;
+  pool_.bind(device, &stream_);
   check(kernels_init(), "kernel attributes");
   check(cudaMalloc(&scratch_ull_, 16), "cudaMalloc");
   check(cudaMallocHost(&host_ull_, 16), "cudaMallocHost");
@@ -342,6 +445,7 @@ Engine::~Engine() {
   if (scratch_ull_) cudaFree(scratch_ull_);
   if (host_ull_) cudaFreeHost(host_ull_);
   pool_.release();
+  pool_.unbind();  // blocks the members still hold are freed synchronously
   if (own_stream_) cudaStreamDestroy(own_stream_);
 }
 

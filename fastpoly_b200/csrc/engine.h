@@ -60,10 +60,28 @@ class Pool {
   size_t limit_ = 0;
   // Classes from this size up may be served by a cached block of a larger class.
   static constexpr size_t kFitBytes = size_t(64) << 20;
+  // Blocks of this size and more (outside graph capture) come from a
+  // stream-ordered memory pool that every engine on the device shares
+  // (cudaMallocFromPoolAsync / cudaFreeAsync on the engine's stream, memory
+  // kept reserved between uses): freed memory serves any later size, where
+  // per-class free lists kept asking for new multi-GB classes, and a
+  // cudaMalloc of several GB held every worker of a server for up to 240 ms.
+  static constexpr size_t kStreamBytes = size_t(64) << 20;
+  // The engine's device and its current stream (async blocks are allocated
+  // and freed in its order); unbind() before the stream goes: later frees of
+  // such blocks then synchronise.
+  void bind(int device, const cudaStream_t* stream) {
+    device_ = device;
+    stream_ = stream;
+  }
+  void unbind() { stream_ = nullptr; }
 
  private:
   std::map<size_t, std::vector<void*>> free_;
   std::mutex mu_;
+  int device_ = -1;
+  const cudaStream_t* stream_ = nullptr;
+  std::set<void*> async_;  // blocks from the stream-ordered pool
   bool capturing_ = false;
   std::map<uint32_t*, size_t> cap_owned_;
   std::map<size_t, std::vector<uint32_t*>> cap_free_;

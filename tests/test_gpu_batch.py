@@ -252,9 +252,9 @@ def test_batch_more_cluster_jobs_than_one_launch(fpx, oracle):
 
 
 def test_batch_smaller_arena_takes_cached_block(oracle):
-    """A batch whose scratch arena falls in a smaller size class than any cached
-    block takes a cached block of up to four times its size instead of a new
-    device allocation, with the same results."""
+    """A batch whose scratch arena is smaller than the previous one's reuses
+    memory the pool already holds (no new device allocation), with the same
+    results."""
     import torch
     ctx = F.Context(0)
     try:
