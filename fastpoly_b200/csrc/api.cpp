@@ -148,6 +148,7 @@ int fpx_release_pool(fpx_ctx* ctx) {
   return guarded(ctx, [&](fpx::Engine& e) {
     e.sync();
     e.drop_graphs();
+    e.drop_flush_arena();
     e.pool().release();
   });
 }

@@ -154,9 +154,15 @@ class BatchRec {
     size_t words = 0;
     for (size_t w : need_) words += round64(w);
     for (const CBuf& c : cbuf_) words += round64(c.words);
+    // (inside a graph capture the graph owns its blocks: one of its own)
     Buf arena;
-    if (words) arena = Buf(&e_.pool(), words);
-    uint32_t* q = arena.get();
+    uint32_t* q = nullptr;
+    if (words && e_.pool().capturing()) {
+      arena = Buf(&e_.pool(), words);
+      q = arena.get();
+    } else if (words) {
+      q = e_.flush_arena(words);
+    }
     for (size_t i = 0; i < plan_.xjobs.size(); ++i) {
       XJob& j = plan_.xjobs[i];
       if (!need_[i]) continue;
@@ -229,6 +235,16 @@ class BatchRec {
 };
 
 // ------------------------------------------------------------ staging ring
+
+uint32_t* Engine::flush_arena(size_t words) {
+  if (words > flush_arena_words_) {
+    flush_arena_.reset();  // back to the pool in stream order, after the flushes that used it
+    flush_arena_words_ = 0;
+    flush_arena_ = Buf(&pool_, words);
+    flush_arena_words_ = words;
+  }
+  return flush_arena_.get();
+}
 
 bool Engine::stage_fits(size_t bytes, size_t& off) const {
   const size_t cap = arena_.cap;

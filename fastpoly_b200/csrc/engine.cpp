@@ -439,6 +439,7 @@ Engine::~Engine() {
   primes_.clear();
   bigs_.clear();
   inv_tabs_.clear();
+  drop_flush_arena();
   free_stages();
   for (auto& r : prof_recs_) { cudaEventDestroy(r.b); cudaEventDestroy(r.e); }
   for (auto ev : ev_free_) cudaEventDestroy(ev);

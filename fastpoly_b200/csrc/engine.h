@@ -75,6 +75,10 @@ class Pool {
     stream_ = stream;
   }
   void unbind() { stream_ = nullptr; }
+  bool capturing() {
+    std::lock_guard<std::mutex> g(mu_);
+    return capturing_;
+  }
 
  private:
   std::map<size_t, std::vector<void*>> free_;
@@ -355,6 +359,13 @@ class Engine {
   Stage stage(size_t bytes);
   void free_stages();
   void count_batch(const BatchPlan& b);
+  // Scratch of one batch flush, kept between flushes (grown when a flush
+  // needs more): flushes run one after another on the engine's stream, so
+  // each may reuse the last one's memory, with no pool operation in the stream
+  // between their launches.
+  uint32_t* flush_arena(size_t words);
+  Buf flush_arena_;
+  size_t flush_arena_words_ = 0;
   // One job of a batch through the single-operation path (errors to its status).
   void batch_single(fpx_job& j);
   // sqrt / pow / divmod jobs of a batch (indices idx) as phases of batched
@@ -384,6 +395,10 @@ class Engine {
     a.second += ms;
   }
   bool profiling() const { return prof_on_; }
+  void drop_flush_arena() {
+    flush_arena_.reset();
+    flush_arena_words_ = 0;
+  }
   // small device->host reads (synchronous)
   uint32_t read_word(const uint32_t* d);
   size_t find_nonzero(const uint32_t* a, size_t n, bool last);  // n if none
