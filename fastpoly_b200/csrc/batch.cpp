@@ -1283,34 +1283,44 @@ void Engine::batch_host(fpx_job* jobs, size_t count, int repr) {
   uint32_t* dout = din + in_words;
   std::vector<fpx_job> dj(jobs, jobs + count);
   // Two chunks of about equal input words when the batch moves at least
-  // 64 MiB: the host packs the second while the GPU runs the first, and unpacks
-  // the first (copied back on the copy stream) while the GPU runs the second.
-  size_t cut = count;
-  if (count >= 2 && in_words * 4 >= (size_t(64) << 20)) {
+  // 64 MiB: the host packs chunk c + 1 while the GPU runs chunk c, and unpacks
+  // chunk c - 1 (copied back on the copy stream) meanwhile.  Four chunks
+  // measured slower on the config-4 mix (147-158 k against 186-202 k polys/s):
+  // every chunk runs its own launch set per size and Newton doubling step, so
+  // the GPU's share grows with the chunk count and the host waits on it.
+  constexpr size_t kChunkBytes = size_t(32) << 20;
+  constexpr size_t kMaxChunks = 2;
+  std::vector<size_t> bounds{0};
+  const size_t want = in_words * 4 >= 2 * kChunkBytes ? std::min(kMaxChunks, in_words * 4 / kChunkBytes) : 1;
+  if (count >= 2 && want > 1) {
     size_t acc = 0;
-    for (cut = 0; cut + 1 < count && acc < in_words / 2; ++cut) acc += wa[cut] + wb[cut];
+    for (size_t i = 0; i + 1 < count && bounds.size() < want; ++i) {
+      acc += wa[i] + wb[i];
+      if (acc * want >= in_words * bounds.size()) bounds.push_back(i + 1);  // one boundary per job at most
+    }
   }
-  const size_t bounds[3] = {0, cut, count};
-  const int nchunks = cut < count && cut > 0 ? 2 : 1;
-  std::vector<ReprSeg> segs[2];
-  std::vector<HostSpan> ins[2];
-  size_t in_off[3] = {0, 0, in_words}, out_off[3] = {0, 0, out_words};
+  bounds.push_back(count);
+  const int nchunks = (int)bounds.size() - 1;
+  std::vector<std::vector<ReprSeg>> segs(nchunks);
+  std::vector<std::vector<HostSpan>> ins(nchunks);
+  std::vector<size_t> in_off(nchunks + 1, in_words), out_off(nchunks + 1, out_words);
   size_t qi = 0, qo = 0;
+  int ck = -1;
   for (size_t i = 0; i < count; ++i) {
-    const int c = nchunks == 2 && i >= cut ? 1 : 0;
-    if (nchunks == 2 && i == cut) {
-      in_off[1] = qi;
-      out_off[1] = qo;
+    while (ck + 1 < nchunks && i == bounds[ck + 1]) {
+      ++ck;
+      in_off[ck] = qi;
+      out_off[ck] = qo;
     }
     const fpx_job& j = jobs[i];
     fpx_job& d = dj[i];
-    if (wa[i]) ins[c].push_back(HostSpan{j.a, nullptr, wa[i]});
+    if (wa[i]) ins[ck].push_back(HostSpan{j.a, nullptr, wa[i]});
     d.a = j.a ? din + qi : nullptr;
-    if (wa[i]) segs[c].push_back(ReprSeg{j.p, din + qi, wa[i], 0});
+    if (wa[i]) segs[ck].push_back(ReprSeg{j.p, din + qi, wa[i], 0});
     qi += wa[i];
-    if (wb[i]) ins[c].push_back(HostSpan{j.b, nullptr, wb[i]});
+    if (wb[i]) ins[ck].push_back(HostSpan{j.b, nullptr, wb[i]});
     d.b = j.b ? din + qi : nullptr;
-    if (wb[i]) segs[c].push_back(ReprSeg{j.p, din + qi, wb[i], 0});
+    if (wb[i]) segs[ck].push_back(ReprSeg{j.p, din + qi, wb[i], 0});
     qi += wb[i];
     d.la = j.a ? wa[i] : j.la;  // a null pointer keeps its length: the batch reports it
     d.lb = j.b ? wb[i] : j.lb;
@@ -1318,10 +1328,6 @@ void Engine::batch_host(fpx_job* jobs, size_t count, int repr) {
     qo += wo[i];
     d.out2 = j.out2 ? dout + qo : nullptr;
     qo += wo2[i];
-  }
-  if (nchunks == 1) {
-    in_off[1] = in_words;
-    out_off[1] = out_words;
   }
   // Constant terms for the domain checks of inv / log / exp, read from the
   // caller's buffers (canonical limbs only; Montgomery limbs are converted on
@@ -1333,9 +1339,11 @@ void Engine::batch_host(fpx_job* jobs, size_t count, int repr) {
       if (wa[i] && (jobs[i].op == FPX_OP_INV || jobs[i].op == FPX_OP_LOG || jobs[i].op == FPX_OP_EXP))
         first[i] = jobs[i].a[0];
   }
-  if (!copy_stream_) {
-    check(cudaStreamCreateWithFlags(&copy_stream_, cudaStreamNonBlocking), "cudaStreamCreate");
-    for (auto& e : chunk_ev_) check(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "cudaEventCreate");
+  if (!copy_stream_) check(cudaStreamCreateWithFlags(&copy_stream_, cudaStreamNonBlocking), "cudaStreamCreate");
+  while (chunk_ev_.size() < (size_t)nchunks) {
+    cudaEvent_t e;
+    check(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "cudaEventCreate");
+    chunk_ev_.push_back(e);
   }
   using HClock = std::chrono::steady_clock;
   auto ms_since = [](HClock::time_point t) { return std::chrono::duration<double, std::milli>(HClock::now() - t).count(); };

@@ -354,7 +354,7 @@ class Engine {
   // Stream of batch_host's copies back, so that a chunk's results come back
   // while the next chunk's kernels run, and the events that order them.
   cudaStream_t copy_stream_ = nullptr;
-  cudaEvent_t chunk_ev_[2] = {nullptr, nullptr};
+  std::vector<cudaEvent_t> chunk_ev_;
   // A staging region of at least `bytes` whose previous copy has completed.
   Stage stage(size_t bytes);
   void free_stages();
