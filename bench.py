@@ -260,7 +260,9 @@ def run_reference(args):
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "Mcoeff/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "threads": threads, "step": f"{threads} concurrent conv calls"},
+            "config": {"workload": WORKLOAD, "p": P, "n_in": N_IN, "n_out": N_OUT, "transform_points": N_FFT,
+                       "parallelism": f"{threads} host threads", "threads": threads,
+                       "step": f"{threads} concurrent conv calls"},
             "cpu_baseline": {"value": value, "unit": "Mcoeff/s", "cores": threads, "kind": "reference",
                              "sample": f"{threads} concurrent fpx::poly::conv(2^22 x 2^22) calls per step ({ref.backend})"},
             "e2e": {"value": value, "unit": "Mcoeff/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
