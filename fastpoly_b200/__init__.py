@@ -73,6 +73,8 @@ def load_library(path: str = LIB_PATH):
     L.fpx_last_error_message.restype = C.c_char_p
     L.fpx_pool_stats.argtypes = [vp, vp]
     L.fpx_release_pool.argtypes = [vp]
+    L.fpx_host_alloc.argtypes = [sz, C.POINTER(vp)]
+    L.fpx_host_free.argtypes = [vp]
     L.fpx_ctx_set_crt_block.argtypes = [vp, sz]
     L.fpx_ntt_max_log.argtypes = [u32]
     L.fpx_profile.argtypes = [vp, i32]
@@ -303,6 +305,19 @@ def _dptr(t) -> int:
 
 # Batch output buffers of at least this many words are reused across calls.
 _OUT_KEEP_WORDS = 1 << 20
+
+
+def _pinned_words(lib, words: int):
+    """A uint32 array in page-locked host memory (fpx_host_alloc), freed when the
+    array and every view of it are gone; None if none can be had."""
+    import weakref
+    ptr = C.c_void_p()
+    if lib.fpx_host_alloc(words * 4, C.byref(ptr)) != OK or not ptr.value:
+        return None
+    raw = (C.c_char * (words * 4)).from_address(ptr.value)
+    arr = np.frombuffer(raw, np.uint32)
+    weakref.finalize(arr, lib.fpx_host_free, ptr.value)
+    return arr
 
 
 class Context:
@@ -544,29 +559,34 @@ class Context:
         return res
 
     def _out_buffer(self, words: int) -> np.ndarray:
-        """Output buffer of a batch.  Large ones are kept and handed out again once
-        no result of the call that had them is referenced any more: a fresh buffer
-        costs a page fault per 4 KiB page on first write (several ms for the
-        hundreds of MB a large batch returns), and is mapped with transparent huge
-        pages requested."""
+        """Output buffer of a batch.  Large ones are page-locked (fpx_host_alloc:
+        the batch's results are copied straight into them, with no host-side
+        unpacking), kept (at most two) and handed out again once no result of the
+        call that had them is referenced any more.  When both kept buffers are
+        still referenced, the call gets an ordinary buffer (transparent huge pages
+        requested): pinning hundreds of MB costs more than the page faults."""
         if words < _OUT_KEEP_WORDS:
             return np.empty(words, np.uint32)
         for b in self._outbufs:
             # references: the list, the loop variable, the argument (a result view adds one)
             if b.size >= words and sys.getrefcount(b) == 3:
                 return b[:words]
-        m = mmap.mmap(-1, words * 4)
-        if hasattr(m, "madvise") and hasattr(mmap, "MADV_HUGEPAGE"):
-            try:
-                m.madvise(mmap.MADV_HUGEPAGE)
-            except OSError:
-                pass
-        buf = np.frombuffer(m, np.uint32)
         free = [i for i, b in enumerate(self._outbufs) if sys.getrefcount(b) == 3]
-        if len(self._outbufs) < 2:
-            self._outbufs.append(buf)
-        elif free:
-            self._outbufs[free[0]] = buf
+        keep = len(self._outbufs) < 2 or bool(free)
+        buf = _pinned_words(self._L, words) if keep else None
+        if buf is None:
+            m = mmap.mmap(-1, words * 4)
+            if hasattr(m, "madvise") and hasattr(mmap, "MADV_HUGEPAGE"):
+                try:
+                    m.madvise(mmap.MADV_HUGEPAGE)
+                except OSError:
+                    pass
+            buf = np.frombuffer(m, np.uint32)
+        if keep:
+            if len(self._outbufs) < 2:
+                self._outbufs.append(buf)
+            else:
+                self._outbufs[free[0]] = buf
         return buf
 
     def batch_submit(self, jobs) -> int:

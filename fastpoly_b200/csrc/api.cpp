@@ -144,6 +144,27 @@ int fpx_pool_stats(fpx_ctx* ctx, fpx_pool_stats_t* out) {
   return FPX_OK;
 }
 
+int fpx_host_alloc(size_t bytes, void** out) {
+  if (!out) return FPX_EINVAL;
+  *out = nullptr;
+  if (bytes == 0) return FPX_EINVAL;
+  if (cudaHostAlloc(out, bytes, cudaHostAllocPortable) != cudaSuccess) {
+    cudaGetLastError();
+    *out = nullptr;
+    return FPX_ENOMEM;
+  }
+  return FPX_OK;
+}
+
+int fpx_host_free(void* p) {
+  if (!p) return FPX_EINVAL;
+  if (cudaFreeHost(p) != cudaSuccess) {
+    cudaGetLastError();
+    return FPX_EINVAL;
+  }
+  return FPX_OK;
+}
+
 int fpx_release_pool(fpx_ctx* ctx) {
   return guarded(ctx, [&](fpx::Engine& e) {
     e.sync();

@@ -1348,6 +1348,16 @@ void Engine::batch_host(fpx_job* jobs, size_t count, int repr) {
   using HClock = std::chrono::steady_clock;
   auto ms_since = [](HClock::time_point t) { return std::chrono::duration<double, std::milli>(HClock::now() - t).count(); };
 
+  // Copies into page-locked result buffers queued but not waited for: waited
+  // for before the call returns, also when an error unwinds it (they read the
+  // device buffer, which goes back to the pool after this guard).
+  struct QueuedCopies {
+    cudaStream_t s;
+    bool queued = false;
+    ~QueuedCopies() {
+      if (queued) cudaStreamSynchronize(s);
+    }
+  } copies{copy_stream_};
   // Results of chunk c: statuses and lengths to the caller's records, then
   // every output region in device order (result words to the caller's buffer,
   // the rest skipped), copied on the copy stream once the chunk's work is done.
@@ -1369,7 +1379,7 @@ void Engine::batch_host(fpx_job* jobs, size_t count, int repr) {
     }
     check(cudaStreamWaitEvent(copy_stream_, chunk_ev_[c], 0), "cudaStreamWaitEvent");
     const auto t0 = HClock::now();
-    copy_out(dout + out_off[c], outs, copy_stream_);
+    if (!copy_out(dout + out_off[c], outs, copy_stream_, false)) copies.queued = true;
     host_phase("copy_out", ms_since(t0));
   };
 
@@ -1396,6 +1406,10 @@ void Engine::batch_host(fpx_job* jobs, size_t count, int repr) {
     if (c > 0) drain(c - 1);
   }
   drain(nchunks - 1);
+  if (copies.queued) {
+    copies.queued = false;
+    check(cudaStreamSynchronize(copy_stream_), "D2H wait");
+  }
 }
 
 // --------------------------------------------------------- pinned staging
@@ -1580,10 +1594,40 @@ void Engine::copy_in(const std::vector<HostSpan>& spans, uint32_t* dst) {
   }
 }
 
-void Engine::copy_out(const uint32_t* src, const std::vector<HostSpan>& spans, cudaStream_t s) {
+bool Engine::copy_out(const uint32_t* src, const std::vector<HostSpan>& spans, cudaStream_t s, bool wait) {
   if (!s) s = stream_;
   size_t total = 0;
   for (const HostSpan& s : spans) total += s.words;
+  // Destinations that form a few long runs of page-locked memory (a batch's
+  // results in one fpx_host_alloc buffer, laid out in device order): one
+  // device-to-host copy per run, straight into place.
+  {
+    struct Run {
+      size_t off, words;
+      uint32_t* dst;
+    };
+    std::vector<Run> runs;
+    size_t off = 0;
+    for (const HostSpan& sp : spans) {
+      if (sp.dst && !runs.empty() && runs.back().off + runs.back().words == off &&
+          runs.back().dst + runs.back().words == sp.dst)
+        runs.back().words += sp.words;
+      else if (sp.dst)
+        runs.push_back(Run{off, sp.words, sp.dst});
+      off += sp.words;
+    }
+    constexpr size_t kMaxDirectRuns = 64;
+    bool direct = !runs.empty() && runs.size() <= kMaxDirectRuns && total * 4 >= kStagedBytes;
+    for (size_t r = 0; direct && r < runs.size(); ++r) direct = pinned(runs[r].dst);
+    if (direct) {
+      const auto tp = std::chrono::steady_clock::now();
+      for (const Run& r : runs)
+        check(cudaMemcpyAsync(r.dst, src + r.off, r.words * 4, cudaMemcpyDeviceToHost, s), "D2H");
+      if (wait) check(cudaStreamSynchronize(s), "D2H wait");
+      host_phase("direct_out", std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - tp).count());
+      return wait;
+    }
+  }
   const size_t chunks = (total + kPinWords - 1) / kPinWords;
   size_t si = 0, so = 0;
   std::vector<CopyPiece> pieces;
@@ -1619,6 +1663,7 @@ void Engine::copy_out(const uint32_t* src, const std::vector<HostSpan>& spans, c
     if (c + 2 < chunks) issue(c + 2);
   }
   // every chunk's copy was waited for before its words were unpacked
+  return true;
 }
 
 }  // namespace fpx

@@ -349,8 +349,11 @@ class Engine {
   void copy_in(const std::vector<HostSpan>& spans, uint32_t* dst);
   // Device region [src, src + sum(words)) -> host spans (null ones skipped),
   // the copies on stream s (nullptr: the engine's stream); returns with every
-  // word in place.
-  void copy_out(const uint32_t* src, const std::vector<HostSpan>& spans, cudaStream_t s = nullptr);
+  // word in place, except that with wait == false copies straight into
+  // page-locked destinations are only queued (returns false then: the caller
+  // synchronises s before reading them).
+  bool copy_out(const uint32_t* src, const std::vector<HostSpan>& spans, cudaStream_t s = nullptr,
+                bool wait = true);
   // Stream of batch_host's copies back, so that a chunk's results come back
   // while the next chunk's kernels run, and the events that order them.
   cudaStream_t copy_stream_ = nullptr;

@@ -66,6 +66,12 @@ const char* fpx_last_error_message(fpx_ctx* ctx);
 /* scratch_memory_stats() / release_scratch_memory() (memory.hpp:21-26, 252-258) */
 int fpx_pool_stats(fpx_ctx* ctx, fpx_pool_stats_t* out);
 int fpx_release_pool(fpx_ctx* ctx);
+/* Page-locked host memory (no counterpart in the reference): copies between
+ * it and the device need no staging, and fpx_batch_run writes a batch's
+ * results straight into it where they lie in it in long contiguous runs.
+ * fpx_host_free takes only pointers fpx_host_alloc returned. */
+int fpx_host_alloc(size_t bytes, void** out);
+int fpx_host_free(void* p);
 /* Terms per block of products that go through the block-pair three-prime CRT
  * path (the reference's crt_convolution<M, Block> template parameter,
  * crt_convolution.hpp:188, default 2^23 = 0 here): a power of two in

@@ -84,6 +84,7 @@ def test_batch_output_buffer_reuse():
     import numpy as np
     ctx = F.Context.__new__(F.Context)  # the buffer logic needs no device
     ctx._outbufs = []
+    ctx._L = F.load_library()  # no GPU: page-locked memory is refused, ordinary buffers kept instead
     words = 3 << 20
     first = ctx._out_buffer(words)
     result = first[5:10]
