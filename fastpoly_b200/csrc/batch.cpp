@@ -746,6 +746,14 @@ void Engine::batch(fpx_job* jobs, size_t count, const uint32_t* first_words, con
       }
     } side_join{*this};
     if (!fused.empty()) {
+      // Longest first: the CTAs (one per SM, for their shared memory) start in
+      // launch order, so the short jobs fill in behind the long ones instead of
+      // a wave ending on a few long ones (config-4 batch 6.03 -> 5.74 ms; on
+      // the main stream instead of the side stream it measured the same).
+      // Outputs are per job: the order is free.
+      std::stable_sort(fused.begin(), fused.end(), [](const NewtonJob& x, const NewtonJob& y) {
+        return x.K * (x.kind == 1 ? 3 : 1) > y.K * (y.kind == 1 ? 3 : 1);  // exp: about three inverses' work
+      });
       // one launch for the one-CTA jobs, one for the cluster jobs
       bool any_nat = false, any_crt = false;
       for (const NewtonJob& x : fused) (x.aux ? any_crt : any_nat) = true;
