@@ -349,6 +349,37 @@ struct GarnerC {
 
 __device__ __forceinline__ uint32_t redc_any(uint32_t x, uint32_t m) { return min(x, x - m); }
 
+// One coefficient from its residues r1, r2, r3 (mod P1, P2, P3; the first
+// `primes` of them), reduced into the target field.
+__device__ __forceinline__ uint32_t garner_one(const GarnerC& g, int primes, uint32_t x1, uint32_t r2, uint32_t r3) {
+  uint32_t v = x1 - __umulhi(x1, g.t_q1) * g.t;
+  v = redc_any(v, g.t);
+  if (primes >= 2) {
+    uint32_t x2 = redc_any(shoup(r2 + g.P2 - x1, g.inv12, g.P2), g.P2);
+    uint32_t v2 = redc_any(shoup(x2, g.p1_t, g.t), g.t);
+    v = redc_any(v + v2, g.t);
+    if (primes == 3) {
+      const uint32_t y = redc_any(shoup(x2, g.p1_in3, g.P3), g.P3);
+      const uint32_t x12 = redc_any(x1 + y, g.P3);  // x1 + P1*x2 mod P3
+      const uint32_t x3 = redc_any(shoup(r3 + g.P3 - x12, g.inv123, g.P3), g.P3);
+      const uint32_t v3 = redc_any(shoup(x3, g.p12_t, g.t), g.t);
+      v = redc_any(v + v3, g.t);
+    }
+  }
+  return v;
+}
+// The epilogue of output i: the Montgomery table factor, negation, accumulation, store.
+__device__ __forceinline__ void garner_put(const GarnerC& g, uint32_t v, uint32_t* out, size_t i, int accumulate,
+                                           const uint32_t* post_mont, int negate, uint32_t tpinv) {
+  if (post_mont) {  // Montgomery table product in the target field (odd target)
+    const Fp ft{g.t, 2 * g.t, tpinv};
+    v = red(mont(v, __ldg(post_mont + i), ft), g.t);
+  }
+  if (negate && v) v = g.t - v;
+  if (accumulate) v = redc_any(v + out[i], g.t);
+  out[i] = v;
+}
+
 __device__ __forceinline__ void garner_body(const GarnerC& g, int primes, const uint32_t* c1, const uint32_t* c2,
                                             const uint32_t* c3, uint32_t* out, size_t n, int accumulate,
                                             const uint32_t* post_mont = nullptr, int negate = 0,
@@ -358,28 +389,8 @@ __device__ __forceinline__ void garner_body(const GarnerC& g, int primes, const 
   const size_t end = whole ? n : (first + span < n ? first + span : n);
   const size_t step = whole ? (size_t)gridDim.x * blockDim.x : blockDim.x;
   for (size_t i = (whole ? blockIdx.x * (size_t)blockDim.x : first) + threadIdx.x; i < end; i += step) {
-    const uint32_t x1 = c1[i];
-    uint32_t v = x1 - __umulhi(x1, g.t_q1) * g.t;
-    v = redc_any(v, g.t);
-    if (primes >= 2) {
-      uint32_t x2 = redc_any(shoup(c2[i] + g.P2 - x1, g.inv12, g.P2), g.P2);
-      uint32_t v2 = redc_any(shoup(x2, g.p1_t, g.t), g.t);
-      v = redc_any(v + v2, g.t);
-      if (primes == 3) {
-        const uint32_t y = redc_any(shoup(x2, g.p1_in3, g.P3), g.P3);
-        const uint32_t x12 = redc_any(x1 + y, g.P3);  // x1 + P1*x2 mod P3
-        const uint32_t x3 = redc_any(shoup(c3[i] + g.P3 - x12, g.inv123, g.P3), g.P3);
-        const uint32_t v3 = redc_any(shoup(x3, g.p12_t, g.t), g.t);
-        v = redc_any(v + v3, g.t);
-      }
-    }
-    if (post_mont) {  // Montgomery table product in the target field (odd target)
-      const Fp ft{g.t, 2 * g.t, tpinv};
-      v = red(mont(v, __ldg(post_mont + i), ft), g.t);
-    }
-    if (negate && v) v = g.t - v;
-    if (accumulate) v = redc_any(v + out[i], g.t);
-    out[i] = v;
+    const uint32_t v = garner_one(g, primes, c1[i], primes >= 2 ? c2[i] : 0u, primes == 3 ? c3[i] : 0u);
+    garner_put(g, v, out, i, accumulate, post_mont, negate, tpinv);
   }
 }
 
@@ -2387,12 +2398,39 @@ __global__ void k_seed_b(const SeedJobB* __restrict__ jobs) {
   seed_body(j.kind, j.p, j.a, j.la, j.out, j.n, j.r0);
 }
 
+// Four consecutive outputs per thread: 16-byte residue loads and four
+// independent Garner chains (the residue buffers are 16-byte aligned, and
+// every block starts at a multiple of kOutSpan); stores stay 32-bit, the
+// caller's output having any alignment.  Unaligned residues: one per thread.
 __global__ void k_garner_b(const GarnerJobB* __restrict__ jobs, const OutBlock* __restrict__ map) {
   pdl_enter();
   const OutBlock m = map[blockIdx.x];
   const GarnerJobB& j = jobs[m.job];
-  garner_body(j.g, j.primes, j.c1, j.c2, j.c3, j.out, j.n, j.accumulate, j.post_mont, j.negate, j.tpinv, m.first,
-              kOutSpan);
+  const uintptr_t al = reinterpret_cast<uintptr_t>(j.c1) | reinterpret_cast<uintptr_t>(j.c2) |
+                       reinterpret_cast<uintptr_t>(j.c3);
+  if (al & 15u) {
+    garner_body(j.g, j.primes, j.c1, j.c2, j.c3, j.out, j.n, j.accumulate, j.post_mont, j.negate, j.tpinv, m.first,
+                kOutSpan);
+    return;
+  }
+  const size_t end = m.first + kOutSpan < j.n ? m.first + kOutSpan : j.n;
+  for (size_t i = m.first + 4 * (size_t)threadIdx.x; i < end; i += 4 * (size_t)blockDim.x) {
+    if (i + 4 <= end) {
+      const uint4 a = *reinterpret_cast<const uint4*>(j.c1 + i);
+      const uint4 b = j.primes >= 2 ? *reinterpret_cast<const uint4*>(j.c2 + i) : make_uint4(0u, 0u, 0u, 0u);
+      const uint4 c = j.primes == 3 ? *reinterpret_cast<const uint4*>(j.c3 + i) : make_uint4(0u, 0u, 0u, 0u);
+      const uint32_t v0 = garner_one(j.g, j.primes, a.x, b.x, c.x), v1 = garner_one(j.g, j.primes, a.y, b.y, c.y);
+      const uint32_t v2 = garner_one(j.g, j.primes, a.z, b.z, c.z), v3 = garner_one(j.g, j.primes, a.w, b.w, c.w);
+      garner_put(j.g, v0, j.out, i, j.accumulate, j.post_mont, j.negate, j.tpinv);
+      garner_put(j.g, v1, j.out, i + 1, j.accumulate, j.post_mont, j.negate, j.tpinv);
+      garner_put(j.g, v2, j.out, i + 2, j.accumulate, j.post_mont, j.negate, j.tpinv);
+      garner_put(j.g, v3, j.out, i + 3, j.accumulate, j.post_mont, j.negate, j.tpinv);
+    } else {
+      for (size_t t = i; t < end; ++t)
+        garner_put(j.g, garner_one(j.g, j.primes, j.c1[t], j.primes >= 2 ? j.c2[t] : 0u, j.primes == 3 ? j.c3[t] : 0u),
+                   j.out, t, j.accumulate, j.post_mont, j.negate, j.tpinv);
+    }
+  }
 }
 
 using BatchFn = void (*)(const BigJobB*);
