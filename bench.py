@@ -100,6 +100,18 @@ def inputs(seed: int):
     return a, b
 
 
+def direct_coeffs(a, b, p: int, ks) -> list:
+    """Coefficients ks of the product a * b mod p by direct sums (numpy, each
+    product reduced before the sum): an oracle-free check of the measured path."""
+    a64, b64 = a.astype(np.uint64), b.astype(np.uint64)
+    out = []
+    for k in ks:
+        lo, hi = max(0, k - (len(b) - 1)), min(k, len(a) - 1)
+        t = (a64[lo:hi + 1] * b64[k - hi:k - lo + 1][::-1]) % np.uint64(p)
+        out.append(int(t.sum(dtype=np.uint64) % np.uint64(p)))
+    return out
+
+
 def measured_peak_hbm():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -296,13 +308,14 @@ def run_fpx(args):
     def step():
         return ctx.conv_device(P, da, N_IN, db, N_IN, None, dout)
 
-    # correctness spot-check of the measured path (first/last coefficients vs a
-    # direct sum), cheap and independent of the oracle
+    # correctness spot-check of the measured path: 24 coefficients (first,
+    # last, the middle one with the longest sum, random others) against direct
+    # sums, independent of the oracle
     step()
     torch.cuda.synchronize()
-    got = dout[:4].cpu().numpy().view(np.uint32)
-    want0 = int(a[0]) * int(b[0]) % P
-    assert int(got[0]) == want0, "conv spot-check failed"
+    got = dout.cpu().numpy().view(np.uint32)
+    ks = [0, N_OUT - 1, N_IN - 1] + [int(k) for k in np.random.default_rng(9).integers(0, N_OUT, 21)]
+    assert [int(got[k]) for k in ks] == direct_coeffs(a, b, P, ks), "conv spot-check failed"
 
     for _ in range(args.warmup):
         flush.zero_()
