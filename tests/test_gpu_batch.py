@@ -383,3 +383,32 @@ def test_batch_sqrt_pow_divmod_device_pointers(fpx, oracle):
         else:
             o = keep[[k for k, t in enumerate(keep) if t.data_ptr() == j.out][0]]
             eq(o.cpu().numpy().view(np.uint32)[: j.out_len], want, f"device job {i} {jb[0]}")
+
+
+def test_batch_output_buffers_not_reused_while_held(fpx, oracle):
+    """Large batches return views into page-locked output buffers the context
+    keeps: a later call never writes into a buffer whose results are still
+    held, and hands a buffer out again once they are dropped."""
+    rng = np.random.default_rng(81)
+    p = 998244353
+
+    def mix(seed):
+        r = np.random.default_rng(seed)
+        return [("conv", p, rnd(r, p, 1 << 17), rnd(r, p, 1 << 17)) for _ in range(8)]  # 2^21 output words
+
+    jobs1, jobs2, jobs3 = mix(1), mix(2), mix(3)
+    r1 = fpx.batch(jobs1)
+    keep1 = [x.copy() for x in r1]
+    r2 = fpx.batch(jobs2)
+    r3 = fpx.batch(jobs3)  # both kept buffers held: a fresh one
+    for i in range(8):
+        eq(r1[i], keep1[i], f"first call's result {i} changed")
+    for i in (0, 7):
+        eq(r2[i], oracle.conv(p, jobs2[i][2], jobs2[i][3]), f"second call {i}")
+        eq(r3[i], oracle.conv(p, jobs3[i][2], jobs3[i][3]), f"third call {i}")
+    addr1 = r1[0].__array_interface__["data"][0]  # the first job's result starts its buffer
+    del r1
+    r4 = fpx.batch(jobs1)  # the first buffer is free again
+    assert r4[0].__array_interface__["data"][0] == addr1
+    for i in range(8):
+        eq(r4[i], keep1[i], f"repeat {i}")
