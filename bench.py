@@ -315,7 +315,8 @@ def run_fpx(args):
     torch.cuda.synchronize()
     got = dout.cpu().numpy().view(np.uint32)
     ks = [0, N_OUT - 1, N_IN - 1] + [int(k) for k in np.random.default_rng(9).integers(0, N_OUT, 21)]
-    assert [int(got[k]) for k in ks] == direct_coeffs(a, b, P, ks), "conv spot-check failed"
+    want_ks = direct_coeffs(a, b, P, ks)
+    assert [int(got[k]) for k in ks] == want_ks, "conv spot-check failed"
 
     for _ in range(args.warmup):
         flush.zero_()
@@ -399,7 +400,7 @@ def run_fpx(args):
     e2e_pageable_s = run_callers(pageable)
     clk = clocks.stop()
     for _, _, _, po in pinned + pageable:
-        assert int(po[0]) == want0
+        assert [int(po[k]) for k in ks] == want_ks, "end-to-end result check failed"
     for c in ctxs[1:]:
         c.close()
 
