@@ -137,6 +137,12 @@ struct fpx_server {
     if (!own && lane == 0) return 0;
     std::deque<Request*>& q = own ? queue[lane] : queue[0];
     if (large_waiting && !(own && lane == 1)) return 0;
+    // One micro-batch takes at most its lane's share of the budget (the budget
+    // over the lane's workers), so that a backlog does not turn into one
+    // budget-sized micro-batch that every other request waits behind; a
+    // single request above the share still goes, alone.
+    const int lane_workers = lane == 0 ? small_workers : (int)engines.size() - small_workers;
+    const size_t share = cfg.hbm_budget_bytes / (size_t)std::max(1, lane_workers);
     size_t bytes = 0;
     while (!q.empty() && mine.size() < cfg.max_batch_jobs) {
       Request* r = q.front();
@@ -146,6 +152,7 @@ struct fpx_server {
         if (own && lane == 1 && mine.empty()) large_waiting = true;
         break;
       }
+      if (!mine.empty() && bytes + r->bytes > share) break;
       if (r->bytes > cfg.hbm_budget_bytes) ++stats.oversize_requests;
       bytes += r->bytes;
       mine.push_back(r);

@@ -241,7 +241,8 @@ typedef struct fpx_serve_config {
 typedef struct fpx_serve_stats {
   uint64_t submitted, completed, batches;
   uint64_t max_batch_jobs_seen;     /* largest micro-batch formed */
-  uint64_t max_batch_bytes_seen;    /* largest planned device bytes admitted in one micro-batch */
+  uint64_t max_batch_bytes_seen;    /* largest planned device bytes admitted in one micro-batch (at most the
+                                       budget over the lane's workers, unless one request alone is larger) */
   uint64_t oversize_requests;       /* requests that alone exceeded the budget (ran alone) */
   uint64_t max_in_flight_bytes;     /* largest planned device bytes of all micro-batches on the GPU at once */
   uint64_t device_pool_bytes;       /* device bytes the workers' scratch pools hold now (cached + in use) */
