@@ -527,6 +527,10 @@ class Context:
         ("pow", p, a, k, n) or ("divmod", p, a, b).  Returns one entry per job: the
         result array ((q, r) for divmod; views into one output buffer), or the
         exception the single-job call would raise for that job (not raised).
+        Large output buffers (page-locked, so results arrive by DMA in place) are
+        kept by the context and used again by a later call only once no result
+        of the call that had them is referenced: keep a result (or a copy), not
+        a raw pointer into it.
         """
         m = len(jobs)
         arr = np.zeros(max(m, 1), dtype=_JOB_DTYPE)
