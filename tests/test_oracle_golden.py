@@ -138,3 +138,30 @@ def test_domain_errors(oracle):
         oracle.divmod(p, [1, 2], [0, 0])
     assert oracle.inv(p, [], 0).size == 0
     assert oracle.conv(p, [], [1]).size == 0
+
+
+def _scale(p, x, c):
+    return (np.asarray(x, np.uint64) * np.uint64(c) % np.uint64(p)).astype(np.uint32)
+
+
+@pytest.mark.parametrize("p", [998244353, 1000000007, 167772161, 7340033])
+def test_identities_of_phased_batch_jobs(oracle, p):
+    """The formulas batches use for sqrt and pow, checked on the oracle: for p
+    odd and n <= p, sqrt(u) = r0 * exp(log(u / u0) / 2) with r0 the reference's
+    root of u0 (a power series has one square root with a given constant term),
+    and pow(u, k) = c0^k exp((k mod p) log(u / c0)) (power.hpp:76-86)."""
+    rng = np.random.default_rng(p % 1000)
+    for n in (1, 2, 17, 300, 1000):
+        u0 = int(rng.integers(1, p)) ** 2 % p
+        u = rng.integers(0, p, n + 5, dtype=np.uint64).astype(np.uint32)
+        u[0] = u0
+        r0 = oracle.sqrt_mod(u0, p)
+        half = (p + 1) // 2
+        lg = oracle.log(p, _scale(p, u, pow(u0, p - 2, p)), n)
+        via = _scale(p, oracle.exp(p, _scale(p, lg, half), n), r0)
+        assert np.array_equal(via, oracle.sqrt(p, u[:n], n)), (p, n)
+        k = int(rng.integers(65, 2 ** 63))
+        c0 = int(u[0])
+        via_pow = _scale(p, oracle.exp(p, _scale(p, oracle.log(p, _scale(p, u, pow(c0, p - 2, p)), n), k % p), n),
+                         pow(c0, k, p))
+        assert np.array_equal(via_pow, oracle.pow(p, u, k, n)), (p, n, k)
