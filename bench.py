@@ -1058,7 +1058,7 @@ def main():
     ap.add_argument("--requests", type=int, default=3000, help="serve: requests per load level")
     ap.add_argument("--serve-max-log", type=int, default=22, help="serve: largest size 2^k")
     ap.add_argument("--workers", type=int, default=0,
-                    help="serve: worker threads (half large-lane, the rest small-lane; 0 = the library's 4)")
+                    help="serve: worker threads (half large-lane, the rest small-lane; 0 = the library's 6)")
     ap.add_argument("--clients", type=int, default=32, help="serve: callers of the closed-loop saturation run")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--headline-only", action="store_true",

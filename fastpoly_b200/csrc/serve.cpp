@@ -235,7 +235,7 @@ int fpx_serve_start(int device, const fpx_serve_config* cfg, fpx_server** out) {
     s->cfg.hbm_budget_bytes = std::min(free_b / 4, size_t(32) << 30);
   }
   if (s->cfg.max_batch_jobs == 0) s->cfg.max_batch_jobs = 4096;
-  if (s->cfg.workers <= 0) s->cfg.workers = 4;
+  if (s->cfg.workers <= 0) s->cfg.workers = 6;
   if (s->cfg.workers < 2) s->cfg.workers = 2;
   // half the workers (at least one) for the large lane, the rest for the small lane
   s->small_workers = s->cfg.workers - std::max(1, s->cfg.workers / 2);

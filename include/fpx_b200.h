@@ -234,7 +234,7 @@ typedef struct fpx_serve_config {
                               0 = a quarter of the device memory free at start, at most 32 GiB */
   size_t max_batch_jobs;   /* 0 = 4096 */
   int workers;             /* worker threads (at least 2): half for the large lane, the rest for the small
-                              lane; 0 = 4 */
+                              lane; 0 = 6 */
   int repr;                /* FPX_REPR_CANONICAL or FPX_REPR_MONTGOMERY for every request */
 } fpx_serve_config;
 
