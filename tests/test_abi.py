@@ -186,3 +186,20 @@ def test_batch_records_from_job_tuples():
                      (("inv", 1 << 32, a, 4), OverflowError), (("pow", 97, a, 3), ValueError)]:
         with pytest.raises(exc):
             F._jobs_ext().fill([bad], arr.ctypes.data, caps.ctypes.data, F._OPS, F._arr)
+
+
+def test_host_alloc_arguments_without_gpu():
+    """fpx_host_alloc / fpx_host_free reject bad arguments; without a GPU the
+    page-locked allocation itself is refused (no host fallback is made up)."""
+    lib = F.load_library()
+    p = ctypes.c_void_p(123)
+    assert lib.fpx_host_alloc(0, ctypes.byref(p)) == F.EINVAL and not p.value
+    assert lib.fpx_host_alloc(16, None) == F.EINVAL
+    assert lib.fpx_host_free(None) == F.EINVAL
+    try:
+        import torch
+        if torch.cuda.is_available():
+            return  # with a GPU the allocation is made (the batch tests use it)
+    except ImportError:
+        pass
+    assert lib.fpx_host_alloc(1 << 20, ctypes.byref(p)) == F.ENOMEM and not p.value
